@@ -1,0 +1,69 @@
+#!/usr/bin/env bash
+# Builds the reference solver's own C++ sources (read in place under REF_DIR)
+# against the Eigen API stand-in in shim/, together with harness.cpp, into
+# oracle/_ref/.  Test infrastructure: the CPU oracle and CPU baseline only.
+#
+#   ref_f32       as shipped (float), the reference's flags (-O3 -mavx2 -mfma
+#                 -fopenmp, build.bat:36): the timed CPU baseline
+#   ref_f32_pin   float, -ffp-contract=off: bit-exact pin of the C restatement
+#   ref_f64_pin   the same sources re-typed to double by a textual substitution
+#                 (float->double, MatrixXf->MatrixXd, VectorXf->VectorXd, 'f'
+#                 literal suffixes dropped), -ffp-contract=off: the FP64 oracle
+#
+# The re-typed copy lives only in a temporary directory; nothing from REF_DIR
+# is written into the repository.
+set -euo pipefail
+HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
+REF_DIR="${REF_DIR:-/root/reference}"
+OUT="${OUT:-$HERE/../_ref}"
+CXX="${CXX:-g++}"
+# the image's g++ driver does not search the system gcc directory for
+# libgomp.spec; point it there explicitly when that directory exists
+GOMP_B=()
+[ -f /usr/lib/gcc/x86_64-linux-gnu/13/libgomp.spec ] && GOMP_B=(-B/usr/lib/gcc/x86_64-linux-gnu/13/)
+if [ ! -f "$REF_DIR/SIMPLE.cpp" ]; then
+    echo "build_ref.sh: no reference sources at $REF_DIR" >&2
+    exit 3
+fi
+mkdir -p "$OUT"
+TMP="$(mktemp -d /tmp/cp_refbuild.XXXXXX)"
+trap 'rm -rf "$TMP"' EXIT
+
+SRCS_REL="SIMPLE.cpp $(cd "$REF_DIR" && ls Utilities/*.cpp Utilities/solvers/cpu/*.cpp | tr '\n' ' ')"
+
+build() {  # build <name> <srcroot> <real> <flags...>
+    local name="$1" root="$2" real="$3"; shift 3
+    local obj="$TMP/obj_$name"
+    mkdir -p "$obj"
+    local objs=()
+    for s in $SRCS_REL; do
+        local o="$obj/$(echo "$s" | tr '/' '_').o"
+        local extra=()
+        [ "$s" = "SIMPLE.cpp" ] && extra=(-Dmain=ref_main_unused)
+        "$CXX" "${GOMP_B[@]}" -std=c++17 "$@" -fopenmp -w "${extra[@]}" -I"$HERE/shim" -I"$root" -I"$root/Utilities" \
+            -c "$root/$s" -o "$o" &
+        objs+=("$o")
+    done
+    "$CXX" "${GOMP_B[@]}" -std=c++17 "$@" -fopenmp -w -DREF_REAL="$real" -I"$HERE/shim" -I"$root" -I"$root/Utilities" \
+        -c "$HERE/harness.cpp" -o "$obj/harness.o" &
+    wait
+    "$CXX" "${GOMP_B[@]}" "$@" -fopenmp "${objs[@]}" "$obj/harness.o" -o "$OUT/$name"
+    echo "built $OUT/$name"
+}
+
+# float, as shipped
+build ref_f32 "$REF_DIR" float -O3 -mavx2 -mfma -ftree-vectorize
+build ref_f32_pin "$REF_DIR" float -O2 -ffp-contract=off
+
+# double re-typed copy
+SRC64="$TMP/src64"
+mkdir -p "$SRC64"
+(cd "$REF_DIR" && find . -maxdepth 1 -name 'SIMPLE.*' -print0; \
+ cd "$REF_DIR" && find Utilities -maxdepth 1 \( -name '*.cpp' -o -name '*.h' \) -print0; \
+ cd "$REF_DIR" && find Utilities/solvers -name '*.cpp' -print0 -o -name '*.h' -print0) \
+ | (cd "$REF_DIR" && xargs -0 cp --parents -t "$SRC64")
+find "$SRC64" \( -name '*.cpp' -o -name '*.h' \) -print0 | xargs -0 sed -i -E \
+    -e 's/\bfloat\b/double/g' \
+    -e 's/MatrixXf/MatrixXd/g' -e 's/VectorXf/VectorXd/g' \
+    -e 's/\b([0-9][0-9]*\.?[0-9]*([eE][-+]?[0-9]+)?)[fF]\b/\1/g'
+build ref_f64_pin "$SRC64" double -O2 -ffp-contract=off
