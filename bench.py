@@ -1,0 +1,340 @@
+#!/usr/bin/env python
+"""Time-to-converge of the B200 SIMPLE solver on the 2048 x 1024 density
+workload: mixed precision vs FP64 on the GPU, with the reference's CPU path
+timed beside it.
+
+One "step" is one full solve from the initial state to the outer iteration
+after which the full-system pressure drop stays within 1e-5 (relative) of
+the converged FP64 value dP*.  dP* and the iteration counts k64 / kmix are
+found first by untimed calibration runs (FP64 and mixed, each run until the
+pressure drop is stationary).  The timed steps then run exactly kmix (mixed)
+and k64 (FP64) outer iterations from a reset state; value = mixed seconds.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun (N > 1) every rank solves its own replica (seed + rank): the
+path does not shard, so the replicas run independently with no collective
+on the data path; the line reports the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "coldplate-solver_b200"))
+
+METRIC = "time-to-converge 2048×1024 (ΔP rel err ≤1e-5): mixed vs FP64 GPU; adjoint/fwd"
+DP_TOL = 1e-5
+# outer iterations of the FP64 solve of the default workload, measured by
+# the calibration run of this script on a B200 (used only by the reference
+# arm, which has no GPU run to count them from)
+DEFAULT_K64 = None
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--ny", type=int, default=1024)
+    ap.add_argument("--nx", type=int, default=2048)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--max-iter", type=int, default=60000)
+    ap.add_argument("--cpu-sample-iters", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------ helpers
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                if out:
+                    self.rows.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+
+    def summary(self) -> dict:
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4) if len(r) > 5 + k and r[5 + k] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def flush_l2(torch):
+    """Write 512 MB (> 126 MB L2) between timed solves."""
+    buf = torch.empty(64 * 1024 * 1024, dtype=torch.float64, device="cuda")
+    buf.fill_(1.0)
+    torch.cuda.synchronize()
+    del buf
+
+
+def first_stable_iter(dp: np.ndarray, dp_star: float, tol: float = DP_TOL) -> int:
+    """1-based count of iterations after which |dP_k - dP*| <= tol |dP*| for all k."""
+    bad = np.nonzero(np.abs(dp - dp_star) > tol * abs(dp_star))[0]
+    return int(bad[-1] + 2) if bad.size else 1
+
+
+def calibrate(Simple, case, prec: str, max_iter: int):
+    """Untimed run until the full pressure drop is stationary (relative
+    change over 200 iterations below 1e-9, or residual epsilon 1e-12)."""
+    prm = case.params(precision=prec, maxIterations=max_iter, epsilon=1e-12, historyCapacity=max_iter,
+                      chunk=200)
+    with Simple(cellType=case.cellType, **prm) as g:
+        done = 0
+        while done < max_iter:
+            rep = g.step(1000)
+            done = rep["iter"]
+            h = g.history()
+            dp = h["fullTotal"]
+            if rep["done"]:
+                break
+            if len(dp) > 400 and abs(dp[-1] - dp[-201]) <= 1e-9 * abs(dp[-1]):
+                break
+        h = g.history()
+    return h
+
+
+# ------------------------------------------------------------------ CPU baseline
+def cpu_baseline(case, n_iter: int, k_converge: int) -> dict | None:
+    """The reference's own CPU path (oracle/_ref/ref_f32, built from its
+    sources) on this workload, all host threads, a bounded sample of outer
+    iterations; time-to-converge extrapolated with the FP64 iteration count."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import REF_DIR, write_case
+    cores = os.cpu_count() or 1
+    exe = os.path.join(REF_DIR, "ref_f32")
+    prm = case.params(maxIterations=n_iter, epsilon=1e-30)
+    if os.path.exists(exe):
+        from oracle import ref_overrides
+        with tempfile.TemporaryDirectory() as d:
+            write_case(d, case.cellType, case.hy, case.hx, case.U, case.Ht)
+            out = subprocess.run([exe, d, d, *ref_overrides(prm, threads=cores), "time_only=1"],
+                                 capture_output=True, text=True, timeout=3600).stdout
+        secs = [float(l.split()[2]) for l in out.splitlines() if l.startswith("ITER")]
+        kind, used = "reference", cores
+    else:
+        from oracle import Oracle
+        o = Oracle("f32", prm, cellType=case.cellType, hy=case.hy, hx=case.hx, U=case.U, Ht=case.Ht)
+        secs = []
+        for _ in range(n_iter):
+            t = time.perf_counter()
+            o.run(1)
+            secs.append(time.perf_counter() - t)
+        kind, used = "port", 1
+    if not secs:
+        return None
+    s_per_it = float(np.mean(secs[1:] if len(secs) > 1 else secs))
+    return {"value": s_per_it * k_converge, "unit": "s", "cores": used, "kind": kind,
+            "sample": f"{len(secs)} outer iterations of the same workload, {s_per_it:.3f} s each, "
+                      f"extrapolated to {k_converge} iterations",
+            "s_per_outer_iteration": s_per_it}
+
+
+# ------------------------------------------------------------------ reference arm
+def reference_arm(args, case, rank: int):
+    if rank != 0:
+        return
+    k = DEFAULT_K64
+    if k is None:
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "outer-iteration count of this workload not yet measured on a B200"}))
+        return
+    times = []
+    for s in range(args.warmup + args.steps):
+        cb = cpu_baseline(case, max(1, args.cpu_sample_iters), k)
+        if cb is None:
+            print(json.dumps({"impl": "reference", "unavailable": "reference CPU build missing"}))
+            return
+        if s >= args.warmup:
+            times.append(cb)
+    v = float(np.mean([t["value"] for t in times]))
+    line = {"metric": METRIC, "value": v, "unit": "s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"density_field {args.nx}x{args.ny} seed {args.seed}"},
+            "impl": "reference",
+            "cpu_baseline": {k2: times[-1][k2] for k2 in ("kind", "cores", "sample")} | {"value": v, "unit": "s"},
+            "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+# ------------------------------------------------------------------ our arm
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    from coldplate_b200 import cases
+    case = cases.density_field(args.ny, args.nx, seed=args.seed + rank)
+    if args.impl == "reference":
+        return reference_arm(args, case, rank)
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    from coldplate_b200 import Simple, build
+    build.build()
+
+    # ---- calibration (untimed): dP*, k64, kmix
+    h64 = calibrate(Simple, case, "fp64", args.max_iter)
+    dp_star = float(h64["fullTotal"][-1])
+    k64 = first_stable_iter(h64["fullTotal"], dp_star)
+    hmx = calibrate(Simple, case, "mixed", args.max_iter)
+    kmix = first_stable_iter(hmx["fullTotal"], dp_star)
+    dp_mix_final = float(hmx["fullTotal"][-1])
+
+    # ---- timed solves (device time, CUDA events inside cp_step)
+    def timed_solves(prec: str, k: int, n_warm: int, n_steps: int):
+        prm = case.params(precision=prec, maxIterations=k + 10, epsilon=1e-30, historyCapacity=k + 10,
+                          chunk=max(32, min(k, 512)))
+        out = []
+        with Simple(cellType=case.cellType, **prm) as g:
+            for s in range(n_warm + n_steps):
+                g.reset()
+                flush_l2(torch)
+                if dist:
+                    dist.barrier()
+                torch.cuda.synchronize()
+                rep = g.step(k)
+                torch.cuda.synchronize()
+                if s >= n_warm:
+                    out.append(rep["device_ms"] / 1e3)
+            dp_end = g.history()["fullTotal"][k - 1]
+        return out, dp_end
+
+    with ClockSampler(local) as clk:
+        t_mix, dp_mix_k = timed_solves("mixed", kmix, args.warmup, args.steps)
+        t_64, dp_64_k = timed_solves("fp64", k64, 1, 1)
+    clocks = clk.summary()
+    t_mixed = max(t_mix)
+    if dist:
+        tt = torch.tensor([t_mixed], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_mixed = float(tt.item())
+
+    # ---- per-kernel device times and the roofline of the dominant kernel
+    prm = case.params(precision="mixed", maxIterations=100000, epsilon=1e-30, historyCapacity=100000)
+    with Simple(cellType=case.cellType, **prm) as g:
+        g.step(50)
+        kt = g.kernel_times(20)
+    nP = (args.ny) * (args.nx - 1)
+    w_mix = 4
+    pcg_ms = kt["ms"]["pcg"] / max(kt["launches"]["pcg"], 1)
+    pcg_iters = kt["pcgIterations"] / max(kt["launches"]["pcg"], 1)
+    pcg_bytes = pcg_iters * 8 * w_mix * nP          # 8 w per unknown per PCG iteration
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    achieved = pcg_bytes / (pcg_ms * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": None, "kernel": "k_pcg<float>",
+                "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"}
+
+    # ---- end to end through the public API with host buffers
+    e2e_t = []
+    gamma_host = torch.from_numpy(1.0 - case.cellType).pin_memory().numpy()
+    prm = case.params(precision="mixed", maxIterations=kmix + 10, epsilon=1e-30, historyCapacity=kmix + 10,
+                      chunk=max(32, min(kmix, 512)))
+    with Simple(cellType=case.cellType, **prm) as g:
+        for s in range(1 + args.steps):
+            flush_l2(torch)
+            t0 = time.perf_counter()
+            g.reset()
+            g.set_gamma(gamma_host)
+            g.step(kmix)
+            p = g.get("p")
+            u = g.get("u")
+            v = g.get("v")
+            dp = g.history()["fullTotal"][-1]
+            t1 = time.perf_counter()
+            if s >= 1:
+                e2e_t.append(t1 - t0)
+    h2d = gamma_host.nbytes
+    d2h = p.nbytes + u.nbytes + v.nbytes + 8
+
+    if rank == 0:
+        cb = None if args.no_cpu_baseline else cpu_baseline(case, args.cpu_sample_iters, k64)
+        iters_per_launch = 8
+        line = {
+            "metric": METRIC, "value": t_mixed, "unit": "s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_mixed * 1e3, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 inner / f64 fields+reductions",
+            "data": "synthetic",
+            "config": {"workload": f"density_field {args.nx}x{args.ny} seed {args.seed} (SOU, 2.5-D, "
+                                   f"Brinkman alpha_max 1e9, q 0.1, U_in {case.U} m/s)",
+                       "flush": "512 MB L2 flush before every timed solve",
+                       "parallelism": "replicas" if world > 1 else "single GPU"},
+            "t_fp64_s": max(t_64), "t_mixed_s": t_mixed, "mixed_over_fp64": t_mixed / max(t_64),
+            "k_fp64": k64, "k_mixed": kmix, "dp_star_pa": dp_star,
+            "dp_rel_err_mixed_final": abs(dp_mix_final - dp_star) / abs(dp_star),
+            "dp_rel_err_mixed_at_k": abs(dp_mix_k - dp_star) / abs(dp_star),
+            "dp_rel_err_fp64_at_k": abs(dp_64_k - dp_star) / abs(dp_star),
+            "calibration_iters": {"fp64": int(len(h64["fullTotal"])), "mixed": int(len(hmx["fullTotal"]))},
+            "kernel_ms_per_outer_iteration": {k2: v2 / max(kt["iterations"], 1) for k2, v2 in kt["ms"].items()},
+            "pcg_iterations_per_outer": pcg_iters,
+            "jacobi_sweeps_per_outer": kt["jacobiSweeps"] / max(kt["iterations"], 1),
+            "roofline": roofline,
+            "cpu_baseline": cb,
+            "e2e": {"value": float(np.mean(e2e_t)), "unit": "s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h)},
+            "clocks": clocks,
+            "gpu_launches": int((args.steps) * kmix * iters_per_launch),
+        }
+        print(json.dumps(line))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,180 @@
+"""Python mirror of the reference's SIMPLE solver interface over the C ABI.
+
+``Simple`` follows class SIMPLE (SIMPLE.h:55-614): the parameters keep their
+SIMPLE.h names (pressureSolverType, momentumSolverType, maxPressureIter,
+uvAlpha, ...), the fields keep their staggered shapes (u (M+1) x N,
+v M x (N+1), p (M+1) x (N+1)), and the entry points are the ones
+iterations.cpp and SIMPLE.cpp call:
+
+    runIterations()            SIMPLE.cpp:310      (whole loop, device-side stop rules)
+    calculateStep()            iterations.cpp:82   (one outer iteration)
+    solveUMomentumImplicit()   momentum_solver.cpp:362
+    solveVMomentumImplicit()   momentum_solver.cpp:366
+    solvePressureSystem()      pressure_solver.cpp:462
+
+Every call runs the CUDA kernels in libcoldplate.so; there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from . import _native as nat
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def make_params(**knobs) -> nat.CpParams:
+    """cp_params with the SIMPLE.h defaults, then the given overrides."""
+    p = nat.default_params()
+    names = {n for n, _ in nat.PARAM_FIELDS}
+    for k, v in knobs.items():
+        if k not in names:
+            raise KeyError(f"unknown parameter {k!r}")
+        if k == "precision" and isinstance(v, str):
+            v = {"fp64": nat.PREC_FP64, "mixed": nat.PREC_MIXED}[v]
+        setattr(p, k, v)
+    return p
+
+
+class Simple:
+    """One field on the GPU.  ``knobs`` are cp_params / SIMPLE.h names."""
+
+    def __init__(self, *, cellType=None, gamma=None, params: nat.CpParams | None = None, **knobs):
+        self._lib = nat.lib()
+        self.params = params if params is not None else make_params(**knobs)
+        if params is not None and knobs:
+            for k, v in knobs.items():
+                setattr(self.params, k, v)
+        h = ctypes.c_void_p()
+        nat.check(self._lib.cp_create(ctypes.byref(self.params), ctypes.byref(h)))
+        self._h = h
+        self.M, self.N = self.params.Ny + 1, self.params.Nx + 1
+        self.pressureIterations = 0
+        if cellType is not None:
+            self.set_cell_type(cellType)
+        elif gamma is not None:
+            self.set_gamma(gamma)
+
+    # -------------------------------------------------------------- set-up
+    @classmethod
+    def from_case(cls, case_dir: str, **knobs) -> "Simple":
+        """Load ExportFiles/fluid_params.txt and geometry_fluid.txt like the
+        reference constructor (SIMPLE.cpp:18-29)."""
+        p = make_params(**knobs)
+        nat.check(nat.lib().cp_read_fluid_params(
+            os.path.join(case_dir, "ExportFiles", "fluid_params.txt").encode(), ctypes.byref(p)))
+        s = cls(params=p)
+        nat.check(s._lib.cp_read_geometry(s._h, os.path.join(case_dir, "ExportFiles", "geometry_fluid.txt").encode()))
+        return s
+
+    def set_cell_type(self, cellType) -> None:
+        a = np.ascontiguousarray(cellType, dtype=np.float64)
+        nat.check(self._lib.cp_set_cell_type(self._h, _dptr(a), a.shape[0], a.shape[1], a.shape[1], 1))
+
+    def set_gamma(self, gamma) -> None:
+        a = np.ascontiguousarray(gamma, dtype=np.float64)
+        nat.check(self._lib.cp_set_gamma(self._h, _dptr(a), a.shape[0], a.shape[1], a.shape[1], 1))
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None and self._h.value:
+            self._lib.cp_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -------------------------------------------------------------- fields
+    def shape(self, name: str) -> tuple[int, int]:
+        M, N = self.M, self.N
+        return {"u": (M + 1, N), "v": (M, N + 1), "p": (M + 1, N + 1), "uStar": (M + 1, N),
+                "vStar": (M, N + 1), "pStar": (M + 1, N + 1), "dE": (M + 1, N), "dN": (M, N + 1),
+                "gamma": (M, N), "alpha": (M, N), "cellType": (M, N)}[name]
+
+    def get(self, name: str) -> np.ndarray:
+        r, c = self.shape(name)
+        out = np.empty((r, c), dtype=np.float64)
+        nat.check(self._lib.cp_get_field(self._h, nat.FIELDS[name], _dptr(out), r, c, c, 1))
+        return out
+
+    def set(self, name: str, arr) -> None:
+        r, c = self.shape(name)
+        a = np.ascontiguousarray(arr, dtype=np.float64)
+        if a.shape != (r, c):
+            raise ValueError(f"{name}: shape {a.shape}, expected {(r, c)}")
+        nat.check(self._lib.cp_set_field(self._h, nat.FIELDS[name], _dptr(a), r, c, c, 1))
+
+    def __getattr__(self, name):
+        if name in nat.FIELDS:
+            return self.get(name)
+        raise AttributeError(name)
+
+    # -------------------------------------------------------------- loop
+    def step(self, n: int = 1) -> dict:
+        rep = nat.CpIterReport()
+        nat.check(self._lib.cp_step(self._h, int(n), ctypes.byref(rep)))
+        self.pressureIterations = rep.pressureIterations
+        return rep.as_dict()
+
+    def calculateStep(self) -> float:
+        """One outer iteration; returns max(residU, residV, residMass)."""
+        return self.step(1)["error"]
+
+    def runIterations(self) -> dict:
+        rep = nat.CpIterReport()
+        nat.check(self._lib.cp_run(self._h, ctypes.byref(rep)))
+        self.pressureIterations = rep.pressureIterations
+        return rep.as_dict()
+
+    def reset_loop(self) -> None:
+        nat.check(self._lib.cp_reset_loop(self._h))
+
+    def reset(self) -> None:
+        """Back to the initial state (zero fields, empty history), no allocation."""
+        nat.check(self._lib.cp_reset(self._h))
+
+    def kernel_times(self, n: int) -> dict:
+        """Run n outer iterations with a CUDA-event bracket around every launch."""
+        t = nat.CpKernelTiming()
+        nat.check(self._lib.cp_kernel_times(self._h, int(n), ctypes.byref(t)))
+        return {"ms": dict(zip(nat.KERNEL_KINDS, list(t.ms))),
+                "launches": dict(zip(nat.KERNEL_KINDS, list(t.launches))),
+                "jacobiSweeps": t.jacobiSweeps, "pcgIterations": t.pcgIterations, "iterations": t.iterations}
+
+    def history(self) -> dict:
+        ncol = self._lib.cp_history_columns()
+        cap = max(self.params.historyCapacity or self.params.maxIterations, 1)
+        buf = np.zeros((cap, ncol), dtype=np.float64)
+        n = ctypes.c_int()
+        nat.check(self._lib.cp_get_history(self._h, _dptr(buf), cap, ctypes.byref(n)))
+        rows = buf[: n.value]
+        return {name: rows[:, k] for k, name in enumerate(nat.HIST_COLS)}
+
+    # -------------------------------------------------------------- dispatch boundary
+    def solveUMomentumImplicit(self) -> tuple[int, float]:
+        r, it = ctypes.c_double(), ctypes.c_int()
+        nat.check(self._lib.cp_momentum_u(self._h, ctypes.byref(r), ctypes.byref(it)))
+        return it.value, r.value
+
+    def solveVMomentumImplicit(self) -> tuple[int, float]:
+        r, it = ctypes.c_double(), ctypes.c_int()
+        nat.check(self._lib.cp_momentum_v(self._h, ctypes.byref(r), ctypes.byref(it)))
+        return it.value, r.value
+
+    def solvePressureSystem(self) -> tuple[int, float]:
+        it, r = ctypes.c_int(), ctypes.c_double()
+        nat.check(self._lib.cp_pressure(self._h, ctypes.byref(it), ctypes.byref(r)))
+        return it.value, r.value

@@ -1,0 +1,819 @@
+// Host driver of the B200-native SIMPLE solver and the C ABI declared in
+// include/cp_simple.h.
+//
+// A cp_ctx owns every device buffer of one field for its lifetime (the
+// reference's GPU backends instead copy the whole CSR system host->device on
+// every call, momentum_solver.cu:156-171, pressure_solver.cu:136-146).  One
+// outer iteration is a fixed sequence of launches on the context's stream;
+// it is captured once into a CUDA graph and replayed in chunks, and the host
+// only reads the device status word between chunks.  The stop rules run on
+// the device (k_finalize), so replaying past convergence does no work.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "cp_kernels.cuh"
+
+using namespace cp;
+
+namespace {
+
+thread_local std::string g_err;
+
+cp_status fail(cp_status s, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return s;
+}
+
+#define CK(call)                                                                                   \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess)                                                                     \
+            return fail(CP_ERR_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_),       \
+                        __FILE__, __LINE__);                                                       \
+    } while (0)
+
+constexpr int kThreads = 256;
+
+}  // namespace
+
+struct cp_ctx {
+    cp_params prm{};
+    KParams k{};
+    Dims d{};
+    int dev = 0, numSMs = 0;
+    cudaStream_t stream = nullptr;
+    size_t nElem = 0;
+    int es = 8;  // bytes of the inner-system type
+    // fields (double)
+    double *u = nullptr, *v = nullptr, *p = nullptr, *uStar = nullptr, *vStar = nullptr, *pStar = nullptr;
+    double *dE = nullptr, *dN = nullptr, *gamma = nullptr, *alpha = nullptr;
+    std::vector<double> cellTypeHost;  // M x N padded, as the reference keeps it
+    // inner systems (double or float)
+    void* mom[12] = {};
+    void* xb[4] = {};
+    void* pcg[9] = {};
+    double *partJ = nullptr, *partM = nullptr, *partP = nullptr;
+    unsigned *barJ = nullptr, *barP = nullptr;
+    Status* st = nullptr;
+    Status* stHost = nullptr;
+    double* hist = nullptr;
+    int histCap = 0;
+    double* dpWin = nullptr;
+    int gJac = 0, gPcg = 0, gElem = 0, nbMass = 0;
+    cudaGraphExec_t graph = nullptr;
+    bool graphTried = false;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::vector<void*> allocs;
+};
+
+namespace {
+
+template <typename T>
+cp_status dalloc(cp_ctx* c, T** ptr, size_t count) {
+    void* q = nullptr;
+    CK(cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(T)));
+    CK(cudaMemsetAsync(q, 0, std::max<size_t>(count, 1) * sizeof(T), c->stream));
+    c->allocs.push_back(q);
+    *ptr = static_cast<T*>(q);
+    return CP_OK;
+}
+
+cp_status dalloc_bytes(cp_ctx* c, void** ptr, size_t bytes) {
+    CK(cudaMalloc(ptr, std::max<size_t>(bytes, 1)));
+    CK(cudaMemsetAsync(*ptr, 0, std::max<size_t>(bytes, 1), c->stream));
+    c->allocs.push_back(*ptr);
+    return CP_OK;
+}
+
+bool finite(double x) { return std::isfinite(x); }
+
+cp_status validate(const cp_params* p) {
+    if (!p) return fail(CP_ERR_BAD_PARAM, "params is NULL");
+    if (p->Ny < 2 || p->Nx < 3) return fail(CP_ERR_BAD_PARAM, "grid %d x %d too small (need Ny >= 2, Nx >= 3)", p->Ny, p->Nx);
+    if ((long long)(p->Ny + 3) * (long long)(p->Nx + 33) > (1ll << 31))
+        return fail(CP_ERR_BAD_PARAM, "grid %d x %d exceeds the 2^31-element index range", p->Ny, p->Nx);
+    const double pos[] = {p->hy, p->hx, p->rho, p->eta, p->uvAlpha, p->pAlpha};
+    const char* posn[] = {"hy", "hx", "rho", "eta", "uvAlpha", "pAlpha"};
+    for (int q = 0; q < 6; ++q)
+        if (!finite(pos[q]) || pos[q] <= 0.0) return fail(CP_ERR_BAD_PARAM, "%s must be finite and > 0", posn[q]);
+    const double fin[] = {p->targetVel, p->epsilon, p->pTol, p->momentumTol, p->brinkmanKMin, p->brinkmanQ,
+                          p->Ht_channel, p->twoPointFiveDConvectionFactor, p->twoPointFiveDSinkMultiplier,
+                          p->xPlaneCoreInlet, p->xPlaneCoreOutlet};
+    for (double x : fin)
+        if (!finite(x)) return fail(CP_ERR_NONFINITE, "non-finite parameter");
+    if (p->maxIterations < 0 || p->maxPressureIter < 0 || p->maxMomentumIter < 0)
+        return fail(CP_ERR_BAD_PARAM, "iteration limits must be >= 0");
+    if (p->pressureSolverType != 1 && p->pressureSolverType != 4)
+        return fail(CP_ERR_UNSUPPORTED,
+                    "pressureSolverType %d not available: types 1 (PCG) and 4 (GPU) run the native PCG",
+                    p->pressureSolverType);
+    if (p->momentumSolverType != 1)
+        return fail(CP_ERR_UNSUPPORTED, "momentumSolverType %d not available: only 1 (implicit Jacobi)",
+                    p->momentumSolverType);
+    if (p->enablePseudoTimeStepping || p->enableSER || p->enableLineSearch || p->enableCflRamp)
+        return fail(CP_ERR_UNSUPPORTED, "pseudo-transient continuation is not available");
+    if (p->enableResidualViscosity) return fail(CP_ERR_UNSUPPORTED, "residual artificial viscosity is not available");
+    if (p->usePressureDropSlopeGate) return fail(CP_ERR_UNSUPPORTED, "pressure-drop slope gate is not available");
+    if (p->convectionScheme != 0 && p->convectionScheme != 1)
+        return fail(CP_ERR_BAD_PARAM, "convectionScheme must be 0 (FOU) or 1 (SOU)");
+    if (p->precision != CP_PREC_FP64 && p->precision != CP_PREC_MIXED)
+        return fail(CP_ERR_BAD_PARAM, "precision must be CP_PREC_FP64 or CP_PREC_MIXED");
+    if (p->usePressureDropConvergence && p->dpConvergenceWindow <= 0)
+        return fail(CP_ERR_BAD_PARAM, "dpConvergenceWindow must be > 0");
+    return CP_OK;
+}
+
+void fill_kparams(cp_ctx* c) {
+    const cp_params& p = c->prm;
+    KParams& k = c->k;
+    k.d = c->d;
+    k.hx = p.hx; k.hy = p.hy; k.rho = p.rho; k.eta = p.eta;
+    k.uvAlpha = p.uvAlpha; k.pAlpha = p.pAlpha;
+    k.targetVel = p.targetVel;
+    k.rampOn = p.enableInletRamp; k.rampSteps = p.rampSteps;
+    // 2.5-D needs Ht > 0 (SIMPLE.cpp:67-73); sink 12 mu / Ht^2 (momentum_solver.cpp:187-189)
+    const bool twoD5 = p.enableTwoPointFiveD && p.Ht_channel > 0.0;
+    k.convScale = twoD5 ? p.twoPointFiveDConvectionFactor : 1.0;
+    const double sink = twoD5 ? p.twoPointFiveDSinkMultiplier * (12.0 * p.eta / (p.Ht_channel * p.Ht_channel)) : 0.0;
+    k.sinkDiag = sink * (p.hx * p.hy);
+    k.sou = p.convectionScheme == 1;
+    k.pTol = p.pTol; k.momTol = p.momentumTol;
+    k.maxP = p.maxPressureIter; k.maxMom = p.maxMomentumIter;
+    k.xCoreIn = p.xPlaneCoreInlet; k.xCoreOut = p.xPlaneCoreOutlet;
+    k.eps = p.epsilon; k.maxIterations = p.maxIterations;
+    k.normalized = p.enableNormalizedResiduals;
+    k.velFloor = p.residNormFloorVel; k.massFloor = p.residNormFloorMass;
+    k.dpConv = p.usePressureDropConvergence; k.dpWindow = p.dpConvergenceWindow; k.dpRampSteps = p.rampSteps;
+    k.dpPercent = p.dpConvergencePercent;
+    const int M = c->d.M, N = c->d.N;
+    k.nU = (M - 1) * (N - 2);
+    k.nV = (M - 2) * (N - 1);
+    k.nP = (M - 1) * (N - 2);
+}
+
+// density -> gamma (1 - clamp(cellType)) with the padded row/column copied,
+// alpha by RAMP (SIMPLE.cpp:667-676, 707-729, 766-772); all M x N, double.
+void build_density(const cp_ctx* c, const std::vector<double>& cellTypePadded, std::vector<double>& gamma,
+                   std::vector<double>& alpha) {
+    const int M = c->d.M, N = c->d.N, pr = M - 1, pc = N - 1;
+    gamma.assign((size_t)M * N, 1.0);
+    alpha.assign((size_t)M * N, 0.0);
+    for (int i = 0; i < pr; ++i)
+        for (int j = 0; j < pc; ++j) {
+            const double val = cellTypePadded[(size_t)i * N + j];
+            const double vc = std::max(0.0, std::min(1.0, val));
+            gamma[(size_t)i * N + j] = 1.0 - vc;
+        }
+    for (int i = 0; i < pr; ++i) gamma[(size_t)i * N + pc] = gamma[(size_t)i * N + pc - 1];
+    for (int j = 0; j < N; ++j) gamma[(size_t)pr * N + j] = gamma[(size_t)(pr - 1) * N + std::min(j, pc - 1)];
+    const double amax = c->prm.eta / std::max(c->prm.brinkmanKMin, 1e-20);
+    const double q = c->prm.brinkmanQ;
+    for (size_t k = 0; k < (size_t)M * N; ++k) {
+        const double g = gamma[k];
+        alpha[k] = amax * (1.0 - g) / (1.0 + q * g + 1e-10);
+    }
+}
+
+cp_status upload_cells(cp_ctx* c, const std::vector<double>& g, const std::vector<double>& a) {
+    const int M = c->d.M, N = c->d.N;
+    CK(cudaMemcpy2DAsync(c->gamma, (size_t)c->d.P * 8, g.data(), (size_t)N * 8, (size_t)N * 8, M,
+                         cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpy2DAsync(c->alpha, (size_t)c->d.P * 8, a.data(), (size_t)N * 8, (size_t)N * 8, M,
+                         cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return CP_OK;
+}
+
+bool field_shape(const cp_ctx* c, cp_field f, double** dptr, int* rows, int* cols) {
+    const int M = c->d.M, N = c->d.N;
+    switch (f) {
+        case CP_FIELD_U: *dptr = c->u; *rows = M + 1; *cols = N; return true;
+        case CP_FIELD_V: *dptr = c->v; *rows = M; *cols = N + 1; return true;
+        case CP_FIELD_P: *dptr = c->p; *rows = M + 1; *cols = N + 1; return true;
+        case CP_FIELD_USTAR: *dptr = c->uStar; *rows = M + 1; *cols = N; return true;
+        case CP_FIELD_VSTAR: *dptr = c->vStar; *rows = M; *cols = N + 1; return true;
+        case CP_FIELD_PSTAR: *dptr = c->pStar; *rows = M + 1; *cols = N + 1; return true;
+        case CP_FIELD_DE: *dptr = c->dE; *rows = M + 1; *cols = N; return true;
+        case CP_FIELD_DN: *dptr = c->dN; *rows = M; *cols = N + 1; return true;
+        case CP_FIELD_GAMMA: *dptr = c->gamma; *rows = M; *cols = N; return true;
+        case CP_FIELD_ALPHA: *dptr = c->alpha; *rows = M; *cols = N; return true;
+        case CP_FIELD_CELLTYPE: *dptr = nullptr; *rows = M; *cols = N; return true;
+    }
+    return false;
+}
+
+// ---------------------------------------------------------------- launches
+// Optional CUDA-event bracket around each launch (cp_kernel_times).
+struct EvRec {
+    static constexpr int kMax = 24;
+    cudaEvent_t ev[2 * kMax] = {};
+    int kind[kMax] = {};
+    int n = 0;
+    void begin(cudaStream_t s, int k) {
+        if (n < kMax) { kind[n] = k; cudaEventRecord(ev[2 * n], s); }
+    }
+    void end(cudaStream_t s) {
+        if (n < kMax) { cudaEventRecord(ev[2 * n + 1], s); ++n; }
+    }
+};
+#define REC_BEGIN(r, k) do { if (r) (r)->begin(c->stream, (k)); } while (0)
+#define REC_END(r) do { if (r) (r)->end(c->stream); } while (0)
+
+template <typename Kern, typename... Args>
+cudaError_t launch_coop(Kern kern, int grid, cudaStream_t s, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(kThreads);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kern, args...);
+}
+
+template <typename TC>
+MomSys<TC> mom_sys(cp_ctx* c, int comp) {
+    MomSys<TC> s;
+    TC** a = reinterpret_cast<TC**>(c->mom + comp * 6);
+    s.aP = a[0]; s.aE = a[1]; s.aW = a[2]; s.aN = a[3]; s.aS = a[4]; s.b = a[5];
+    return s;
+}
+
+template <typename TV>
+PcgBufs<TV> pcg_bufs(cp_ctx* c) {
+    PcgBufs<TV> b;
+    TV** a = reinterpret_cast<TV**>(c->pcg);
+    b.fE = a[0]; b.fN = a[1]; b.d = a[2]; b.x = a[3]; b.r = a[4]; b.pa = a[5]; b.pb = a[6]; b.Ap = a[7];
+    b.rhs = a[8];
+    return b;
+}
+
+template <typename TC, bool Mixed>
+cp_status enqueue_momentum(cp_ctx* c, int doU, int doV, int applyBC, EvRec* rec = nullptr) {
+    Fields f{c->u, c->v, c->p, c->alpha, c->gamma};
+    MomSys<TC> U = mom_sys<TC>(c, 0), V = mom_sys<TC>(c, 1);
+    REC_BEGIN(rec, CP_K_ASSEMBLE);
+    k_assemble<TC, Mixed><<<c->gElem, kThreads, 0, c->stream>>>(c->k, c->st, f, U, V, c->dE, c->dN, doU, doV);
+    REC_END(rec);
+    CK(cudaGetLastError());
+    CK(cudaMemsetAsync(c->barJ, 0, sizeof(unsigned), c->stream));
+    JacobiOut out{c->uStar, c->vStar};
+    REC_BEGIN(rec, CP_K_JACOBI);
+    CK(launch_coop(k_jacobi<TC, Mixed>, c->gJac, c->stream, c->k, c->st, U, V, (const double*)c->u,
+                   (const double*)c->v, (TC*)c->xb[0], (TC*)c->xb[1], (TC*)c->xb[2], (TC*)c->xb[3], out,
+                   (const double*)c->gamma, c->partJ, c->barJ, doU, doV, applyBC));
+    REC_END(rec);
+    return CP_OK;
+}
+
+template <typename TV>
+cp_status enqueue_pressure(cp_ctx* c, EvRec* rec = nullptr) {
+    PcgBufs<TV> B = pcg_bufs<TV>(c);
+    REC_BEGIN(rec, CP_K_MASS);
+    k_mass<TV><<<c->nbMass, kThreads, 0, c->stream>>>(c->k, c->st, c->u, c->v, c->uStar, c->vStar, B.rhs, c->partM);
+    REC_END(rec);
+    CK(cudaGetLastError());
+    CK(cudaMemsetAsync(c->barP, 0, sizeof(unsigned), c->stream));
+    REC_BEGIN(rec, CP_K_PCG);
+    CK(launch_coop(k_pcg<TV>, c->gPcg, c->stream, c->k, c->st, (const double*)c->dE, (const double*)c->dN, B,
+                   c->pStar, c->partP, c->barP));
+    REC_END(rec);
+    return CP_OK;
+}
+
+template <typename TC, bool Mixed>
+cp_status enqueue_iteration(cp_ctx* c, EvRec* rec = nullptr) {
+    REC_BEGIN(rec, CP_K_BC);
+    k_bc<<<c->gElem, kThreads, 0, c->stream>>>(c->k, c->st, c->u, c->v, c->p, c->gamma, 1);
+    REC_END(rec);
+    CK(cudaGetLastError());
+    cp_status s = enqueue_momentum<TC, Mixed>(c, 1, 1, 1, rec);
+    if (s != CP_OK) return s;
+    s = enqueue_pressure<TC>(c, rec);
+    if (s != CP_OK) return s;
+    REC_BEGIN(rec, CP_K_CORRECT);
+    k_correct<<<c->gElem, kThreads, 0, c->stream>>>(c->k, c->st, c->u, c->v, c->p, c->uStar, c->vStar, c->pStar,
+                                                    c->dE, c->dN);
+    REC_END(rec);
+    CK(cudaGetLastError());
+    REC_BEGIN(rec, CP_K_BC);
+    k_bc<<<c->gElem, kThreads, 0, c->stream>>>(c->k, c->st, c->u, c->v, c->p, c->gamma, 0);
+    REC_END(rec);
+    CK(cudaGetLastError());
+    FinalizeArgs fa{c->u, c->v, c->p, c->gamma, c->partM, c->nbMass, c->hist, c->histCap, c->dpWin};
+    REC_BEGIN(rec, CP_K_FINALIZE);
+    k_finalize<<<1, 1024, 0, c->stream>>>(c->k, c->st, fa);
+    REC_END(rec);
+    CK(cudaGetLastError());
+    return CP_OK;
+}
+
+cp_status enqueue_iteration_any(cp_ctx* c, EvRec* rec = nullptr) {
+    return c->prm.precision == CP_PREC_MIXED ? enqueue_iteration<float, true>(c, rec)
+                                             : enqueue_iteration<double, false>(c, rec);
+}
+
+cp_status build_graph(cp_ctx* c) {
+    c->graphTried = true;
+    cudaGraph_t g = nullptr;
+    if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        cudaGetLastError();
+        return CP_OK;
+    }
+    cp_status s = enqueue_iteration_any(c);
+    cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+    if (s != CP_OK || e != cudaSuccess || !g) {
+        cudaGetLastError();
+        if (g) cudaGraphDestroy(g);
+        g_err.clear();
+        return CP_OK;  // fall back to direct launches
+    }
+    cudaGraphExec_t ex = nullptr;
+    e = cudaGraphInstantiate(&ex, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return CP_OK;
+    }
+    c->graph = ex;
+    return CP_OK;
+}
+
+cp_status read_status(cp_ctx* c) {
+    CK(cudaMemcpyAsync(c->stHost, c->st, sizeof(Status), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return CP_OK;
+}
+
+void fill_report(cp_ctx* c, cp_iter_report* out) {
+    if (!out) return;
+    memset(out, 0, sizeof(*out));
+    const Status& s = *c->stHost;
+    out->iter = s.iter;
+    out->done = s.done;
+    out->stop_reason = s.reason;
+    const int last = s.iter - 1;
+    if (last >= 0 && last < c->histCap) {
+        double row[kHistCols];
+        if (cudaMemcpy(row, c->hist + (size_t)last * kHistCols, sizeof row, cudaMemcpyDeviceToHost) == cudaSuccess) {
+            out->error = row[H_ERROR];
+            out->residU_RMS = row[H_RMS_U]; out->residV_RMS = row[H_RMS_V]; out->residMass_RMS = row[H_RMS_MASS];
+            out->residU_max = row[H_MAX_U]; out->residV_max = row[H_MAX_V]; out->residMass_max = row[H_MAX_MASS];
+            out->pressureIterations = (int)row[H_ITERS_P];
+            out->momentumItersU = (int)row[H_ITERS_U]; out->momentumItersV = (int)row[H_ITERS_V];
+            out->coreTotalDrop = row[H_CORE_TOTAL]; out->fullTotalDrop = row[H_FULL_TOTAL];
+            out->coreStaticDrop = row[H_CORE_STATIC]; out->fullStaticDrop = row[H_FULL_STATIC];
+            out->inletMassFlux = row[H_IN_FLUX]; out->outletMassFlux = row[H_OUT_FLUX];
+            out->residU = row[H_RES_U]; out->residV = row[H_RES_V]; out->residMass = row[H_RES_MASS];
+        }
+    }
+}
+
+cp_status device_error(cp_ctx* c) {
+    if (c->stHost->err != 0)
+        return fail((cp_status)c->stHost->err, "device reported %s at iteration %d",
+                    cp_status_string((cp_status)c->stHost->err), c->stHost->iter);
+    return CP_OK;
+}
+
+cp_status run_iterations(cp_ctx* c, long long n, bool untilDone, cp_iter_report* out) {
+    if (!c->graphTried) {
+        cp_status s = build_graph(c);
+        if (s != CP_OK) return s;
+    }
+    CK(cudaEventRecord(c->ev0, c->stream));
+    long long done = 0;
+    const int chunk = std::max(1, c->prm.chunk);
+    for (;;) {
+        const long long todo = untilDone ? chunk : std::min<long long>(chunk, n - done);
+        if (todo <= 0) break;
+        for (long long q = 0; q < todo; ++q) {
+            if (c->graph) CK(cudaGraphLaunch(c->graph, c->stream));
+            else {
+                cp_status s = enqueue_iteration_any(c);
+                if (s != CP_OK) return s;
+            }
+        }
+        done += todo;
+        cp_status s = read_status(c);
+        if (s != CP_OK) return s;
+        if (c->stHost->done) break;
+        if (!untilDone && done >= n) break;
+    }
+    CK(cudaEventRecord(c->ev1, c->stream));
+    CK(cudaEventSynchronize(c->ev1));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    fill_report(c, out);
+    if (out) out->device_ms = ms;
+    return device_error(c);
+}
+
+cp_status strided_to_dense(const double* host, long rows, long cols, long rs, long cs, int R, int C,
+                           std::vector<double>& dense) {
+    if (!host) return fail(CP_ERR_BAD_PARAM, "host pointer is NULL");
+    if (rows != R || cols != C) return fail(CP_ERR_BAD_PARAM, "shape %ld x %ld, expected %d x %d", rows, cols, R, C);
+    dense.resize((size_t)R * C);
+    for (long i = 0; i < rows; ++i)
+        for (long j = 0; j < cols; ++j) {
+            const double x = host[i * rs + j * cs];
+            if (!std::isfinite(x)) return fail(CP_ERR_NONFINITE, "non-finite input at (%ld, %ld)", i, j);
+            dense[(size_t)i * C + j] = x;
+        }
+    return CP_OK;
+}
+
+}  // namespace
+
+// ======================================================================== C ABI
+extern "C" {
+
+const char* cp_status_string(cp_status s) {
+    switch (s) {
+        case CP_OK: return "CP_OK";
+        case CP_ERR_BAD_PARAM: return "CP_ERR_BAD_PARAM";
+        case CP_ERR_UNSUPPORTED: return "CP_ERR_UNSUPPORTED";
+        case CP_ERR_NONFINITE: return "CP_ERR_NONFINITE";
+        case CP_ERR_DIVERGED: return "CP_ERR_DIVERGED";
+        case CP_ERR_TIMEOUT: return "CP_ERR_TIMEOUT";
+        case CP_ERR_CUDA: return "CP_ERR_CUDA";
+        case CP_ERR_STATE: return "CP_ERR_STATE";
+    }
+    return "CP_ERR_UNKNOWN";
+}
+
+const char* cp_last_error_string(void) { return g_err.c_str(); }
+
+void cp_params_default(cp_params* p) {
+    if (!p) return;
+    memset(p, 0, sizeof(*p));
+    p->epsilon = 1e-7;
+    p->maxIterations = 1000;
+    p->saveStateInterval = 1000;
+    p->reuseInitialFields = 0;
+    p->xPlaneCoreInlet = 0.01;
+    p->xPlaneCoreOutlet = 0.05;
+    p->usePressureDropConvergence = 1;
+    p->dpConvergenceWindow = 500;
+    p->dpConvergencePercent = 1.0;
+    p->usePressureDropSlopeGate = 0;
+    p->dpSlopeWindowIters = 1000;
+    p->dpSlopeMaxDelta = 10.0;
+    p->numThreads = 8;
+    p->pressureSolverType = 4;
+    p->parallelizeDirectSolver = 1;
+    p->maxPressureIter = 30;
+    p->pTol = 1e-6;
+    p->sorOmega = 0.0;
+    p->momentumSolverType = 1;
+    p->momentumTol = 1e-6;
+    p->maxMomentumIter = 400;
+    p->momentumSorOmega = 1.0;
+    p->convectionScheme = 0;
+    p->enableTwoPointFiveD = 0;
+    p->twoPointFiveDConvectionFactor = 1.2;
+    p->twoPointFiveDSinkMultiplier = 1.0;
+    p->Ht_channel = 0.0;
+    p->brinkmanKMin = 1e-14;
+    p->brinkmanQ = 1.0;
+    p->timeStepMultiplier = 0.01;
+    p->enablePseudoTimeStepping = 0;
+    p->pseudoCFL = 0.1;
+    p->minPseudoSpeed = 0.05;
+    p->useLocalPseudoTime = 1;
+    p->pseudoControllerMode = 2;
+    p->enableSER = 0;
+    p->enableLineSearch = 0;
+    p->enableCflRamp = 0;
+    p->rho = 997.0;
+    p->eta = 0.00089;
+    p->targetVel = 0.0;
+    p->enableInletRamp = 0;
+    p->rampSteps = 1000;
+    p->uvAlpha = 0.7;
+    p->pAlpha = 0.3;
+    p->enableResidualViscosity = 0;
+    p->enableNormalizedResiduals = 0;
+    p->residNormFloorVel = 1e-6;
+    p->residNormFloorMass = 1e-12;
+    p->precision = CP_PREC_FP64;
+    p->refineRounds = 0;
+    p->historyCapacity = 0;   // 0: maxIterations rows
+    p->chunk = 32;
+}
+
+cp_status cp_read_fluid_params(const char* path, cp_params* p) {
+    if (!path || !p) return fail(CP_ERR_BAD_PARAM, "NULL argument");
+    FILE* f = fopen(path, "r");
+    if (!f) return fail(CP_ERR_BAD_PARAM, "cannot open %s", path);
+    int Ny = 0, Nx = 0, nin = 0, nout = 0;
+    double hy = 0, hx = 0, U = 0, Ht = 0;
+    const int got = fscanf(f, "%d %d %lf %lf %lf %d %d", &Ny, &Nx, &hy, &hx, &U, &nin, &nout);
+    if (got != 7) {
+        fclose(f);
+        return fail(CP_ERR_BAD_PARAM, "%s: expected 'Ny Nx hy hx U N_in N_out [Ht]'", path);
+    }
+    if (fscanf(f, "%lf", &Ht) != 1) Ht = p->Ht_channel;
+    fclose(f);
+    if (Ny <= 0 || Nx <= 0 || hy <= 0 || hx <= 0)
+        return fail(CP_ERR_BAD_PARAM, "%s: non-positive grid size or spacing", path);
+    p->Ny = Ny; p->Nx = Nx; p->hy = hy; p->hx = hx; p->targetVel = U;
+    p->N_in_buffer = nin; p->N_out_buffer = nout; p->Ht_channel = Ht;
+    return CP_OK;
+}
+
+cp_status cp_create(const cp_params* prm, cp_ctx** out) {
+    if (!out) return fail(CP_ERR_BAD_PARAM, "out is NULL");
+    *out = nullptr;
+    cp_status s = validate(prm);
+    if (s != CP_OK) return s;
+    cp_ctx* c = new cp_ctx();
+    c->prm = *prm;
+    if (c->prm.enableTwoPointFiveD && c->prm.Ht_channel <= 0.0) c->prm.enableTwoPointFiveD = 0;
+    const int M = prm->Ny + 1, N = prm->Nx + 1;
+    c->d.M = M;
+    c->d.N = N;
+    c->d.P = ((N + 1 + 31) / 32) * 32;
+    c->nElem = (size_t)(M + 2) * c->d.P;
+    c->es = prm->precision == CP_PREC_MIXED ? 4 : 8;
+    auto bail = [&](cp_status e) { cp_destroy(c); return e; };
+    if (cudaGetDevice(&c->dev) != cudaSuccess) return bail(fail(CP_ERR_CUDA, "no CUDA device"));
+    if (cudaDeviceGetAttribute(&c->numSMs, cudaDevAttrMultiProcessorCount, c->dev) != cudaSuccess)
+        return bail(fail(CP_ERR_CUDA, "cudaDeviceGetAttribute failed"));
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return bail(fail(CP_ERR_CUDA, "cudaStreamCreate failed"));
+    if (cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess)
+        return bail(fail(CP_ERR_CUDA, "cudaEventCreate failed"));
+    fill_kparams(c);
+    double** fields[] = {&c->u, &c->v, &c->p, &c->uStar, &c->vStar, &c->pStar, &c->dE, &c->dN, &c->gamma, &c->alpha};
+    for (double** f : fields)
+        if ((s = dalloc(c, f, c->nElem)) != CP_OK) return bail(s);
+    for (auto& m : c->mom)
+        if ((s = dalloc_bytes(c, &m, c->nElem * c->es)) != CP_OK) return bail(s);
+    for (auto& x : c->xb)
+        if ((s = dalloc_bytes(c, &x, c->nElem * c->es)) != CP_OK) return bail(s);
+    for (auto& x : c->pcg)
+        if ((s = dalloc_bytes(c, &x, c->nElem * c->es)) != CP_OK) return bail(s);
+    // cooperative grids: every block must be resident
+    int nbJ = 0, nbP = 0;
+    if (c->prm.precision == CP_PREC_MIXED) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nbJ, k_jacobi<float, true>, kThreads, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nbP, k_pcg<float>, kThreads, 0);
+    } else {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nbJ, k_jacobi<double, false>, kThreads, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nbP, k_pcg<double>, kThreads, 0);
+    }
+    if (nbJ < 1 || nbP < 1) return bail(fail(CP_ERR_CUDA, "cooperative kernels do not fit on an SM"));
+    c->gJac = c->numSMs * std::min(nbJ, 4);
+    c->gPcg = c->numSMs * std::min(nbP, 4);
+    c->gElem = c->numSMs * 4;
+    c->nbMass = c->numSMs * 4;
+    if (c->gJac > kMaxBlocks || c->gPcg > kMaxBlocks || c->nbMass > kMaxBlocks)
+        return bail(fail(CP_ERR_CUDA, "too many SMs for the partial-sum buffers"));
+    if ((s = dalloc(c, &c->partJ, (size_t)4 * c->gJac)) != CP_OK) return bail(s);
+    if ((s = dalloc(c, &c->partM, (size_t)4 * c->nbMass)) != CP_OK) return bail(s);
+    if ((s = dalloc(c, &c->partP, (size_t)3 * c->gPcg)) != CP_OK) return bail(s);
+    if ((s = dalloc(c, &c->barJ, 1)) != CP_OK) return bail(s);
+    if ((s = dalloc(c, &c->barP, 1)) != CP_OK) return bail(s);
+    if ((s = dalloc(c, &c->st, 1)) != CP_OK) return bail(s);
+    c->histCap = prm->historyCapacity > 0 ? prm->historyCapacity : std::max(prm->maxIterations, 1);
+    if ((s = dalloc(c, &c->hist, (size_t)c->histCap * kHistCols)) != CP_OK) return bail(s);
+    if ((s = dalloc(c, &c->dpWin, (size_t)std::max(prm->dpConvergenceWindow, 1))) != CP_OK) return bail(s);
+    if (cudaMallocHost(&c->stHost, sizeof(Status)) != cudaSuccess) return bail(fail(CP_ERR_CUDA, "cudaMallocHost failed"));
+    memset(c->stHost, 0, sizeof(Status));
+    // all fluid until a geometry is set (SIMPLE.cpp:267-269)
+    c->cellTypeHost.assign((size_t)M * N, 0.0);
+    std::vector<double> g, a;
+    build_density(c, c->cellTypeHost, g, a);
+    if ((s = upload_cells(c, g, a)) != CP_OK) return bail(s);
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) return bail(fail(CP_ERR_CUDA, "initialisation failed"));
+    *out = c;
+    return CP_OK;
+}
+
+cp_status cp_destroy(cp_ctx* c) {
+    if (!c) return CP_OK;
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->graph) cudaGraphExecDestroy(c->graph);
+    for (void* q : c->allocs) cudaFree(q);
+    if (c->stHost) cudaFreeHost(c->stHost);
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return CP_OK;
+}
+
+cp_status cp_set_cell_type(cp_ctx* c, const double* ct, long rows, long cols, long rs, long cs) {
+    if (!c) return fail(CP_ERR_BAD_PARAM, "ctx is NULL");
+    const int M = c->d.M, N = c->d.N, pr = M - 1, pc = N - 1;
+    std::vector<double> dense;
+    cp_status s = strided_to_dense(ct, rows, cols, rs, cs, pr, pc, dense);
+    if (s != CP_OK) return s;
+    std::vector<double>& P = c->cellTypeHost;
+    P.assign((size_t)M * N, 0.0);
+    for (int i = 0; i < pr; ++i)
+        for (int j = 0; j < pc; ++j) P[(size_t)i * N + j] = dense[(size_t)i * pc + j];
+    // pad the extra row/column by copy (SIMPLE.cpp:667-676)
+    for (int i = 0; i < pr; ++i) P[(size_t)i * N + pc] = P[(size_t)i * N + pc - 1];
+    for (int j = 0; j < N; ++j) P[(size_t)pr * N + j] = P[(size_t)(pr - 1) * N + std::min(j, pc - 1)];
+    std::vector<double> g, a;
+    build_density(c, P, g, a);
+    return upload_cells(c, g, a);
+}
+
+cp_status cp_set_gamma(cp_ctx* c, const double* gm, long rows, long cols, long rs, long cs) {
+    if (!c) return fail(CP_ERR_BAD_PARAM, "ctx is NULL");
+    const int pr = c->d.M - 1, pc = c->d.N - 1;
+    std::vector<double> dense;
+    cp_status s = strided_to_dense(gm, rows, cols, rs, cs, pr, pc, dense);
+    if (s != CP_OK) return s;
+    for (double& x : dense) x = 1.0 - x;  // gamma -> cellType
+    return cp_set_cell_type(c, dense.data(), pr, pc, pc, 1);
+}
+
+cp_status cp_read_geometry(cp_ctx* c, const char* path) {
+    if (!c || !path) return fail(CP_ERR_BAD_PARAM, "NULL argument");
+    const int pr = c->d.M - 1, pc = c->d.N - 1;
+    std::vector<double> ct((size_t)pr * pc, 0.0);
+    FILE* f = fopen(path, "r");
+    if (f) {  // missing file: all fluid (SIMPLE.cpp:645-649); short file: rest fluid
+        for (size_t q = 0; q < ct.size(); ++q)
+            if (fscanf(f, "%lf", &ct[q]) != 1) break;
+        fclose(f);
+    }
+    return cp_set_cell_type(c, ct.data(), pr, pc, pc, 1);
+}
+
+cp_status cp_get_field(cp_ctx* c, cp_field which, double* host, long rows, long cols, long rs, long cs) {
+    if (!c || !host) return fail(CP_ERR_BAD_PARAM, "NULL argument");
+    double* dp = nullptr;
+    int R = 0, C = 0;
+    if (!field_shape(c, which, &dp, &R, &C)) return fail(CP_ERR_BAD_PARAM, "unknown field %d", (int)which);
+    if (rows != R || cols != C) return fail(CP_ERR_BAD_PARAM, "shape %ld x %ld, expected %d x %d", rows, cols, R, C);
+    std::vector<double> dense((size_t)R * C);
+    if (which == CP_FIELD_CELLTYPE) {
+        dense = c->cellTypeHost;
+    } else {
+        CK(cudaMemcpy2DAsync(dense.data(), (size_t)C * 8, dp, (size_t)c->d.P * 8, (size_t)C * 8, R,
+                             cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+    }
+    for (long i = 0; i < rows; ++i)
+        for (long j = 0; j < cols; ++j) host[i * rs + j * cs] = dense[(size_t)i * C + j];
+    return CP_OK;
+}
+
+cp_status cp_set_field(cp_ctx* c, cp_field which, const double* host, long rows, long cols, long rs, long cs) {
+    if (!c) return fail(CP_ERR_BAD_PARAM, "ctx is NULL");
+    if (which == CP_FIELD_GAMMA || which == CP_FIELD_ALPHA || which == CP_FIELD_CELLTYPE)
+        return fail(CP_ERR_BAD_PARAM, "use cp_set_cell_type / cp_set_gamma for the geometry");
+    double* dp = nullptr;
+    int R = 0, C = 0;
+    if (!field_shape(c, which, &dp, &R, &C)) return fail(CP_ERR_BAD_PARAM, "unknown field %d", (int)which);
+    std::vector<double> dense;
+    cp_status s = strided_to_dense(host, rows, cols, rs, cs, R, C, dense);
+    if (s != CP_OK) return s;
+    CK(cudaMemcpy2DAsync(dp, (size_t)c->d.P * 8, dense.data(), (size_t)C * 8, (size_t)C * 8, R,
+                         cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return CP_OK;
+}
+
+cp_status cp_step(cp_ctx* c, int n_outer, cp_iter_report* out) {
+    if (!c) return fail(CP_ERR_BAD_PARAM, "ctx is NULL");
+    if (n_outer < 0) return fail(CP_ERR_BAD_PARAM, "n_outer < 0");
+    cp_status s = read_status(c);
+    if (s != CP_OK) return s;
+    if (c->stHost->done) {
+        fill_report(c, out);
+        return c->stHost->err ? device_error(c) : CP_OK;
+    }
+    return run_iterations(c, n_outer, false, out);
+}
+
+cp_status cp_run(cp_ctx* c, cp_iter_report* out) {
+    if (!c) return fail(CP_ERR_BAD_PARAM, "ctx is NULL");
+    cp_status s = read_status(c);
+    if (s != CP_OK) return s;
+    if (c->stHost->done) {
+        fill_report(c, out);
+        return c->stHost->err ? device_error(c) : CP_OK;
+    }
+    return run_iterations(c, 0, true, out);
+}
+
+cp_status cp_reset_loop(cp_ctx* c) {
+    if (!c) return fail(CP_ERR_BAD_PARAM, "ctx is NULL");
+    CK(cudaMemsetAsync(c->st, 0, sizeof(Status), c->stream));
+    CK(cudaMemsetAsync(c->dpWin, 0, sizeof(double) * std::max(c->prm.dpConvergenceWindow, 1), c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return CP_OK;
+}
+
+cp_status cp_reset(cp_ctx* c) {
+    if (!c) return fail(CP_ERR_BAD_PARAM, "ctx is NULL");
+    double* f[] = {c->u, c->v, c->p, c->uStar, c->vStar, c->pStar, c->dE, c->dN};
+    for (double* q : f) CK(cudaMemsetAsync(q, 0, c->nElem * sizeof(double), c->stream));
+    CK(cudaMemsetAsync(c->hist, 0, (size_t)c->histCap * kHistCols * sizeof(double), c->stream));
+    return cp_reset_loop(c);
+}
+
+cp_status cp_kernel_times(cp_ctx* c, int n_outer, cp_kernel_timing* out) {
+    if (!c || !out) return fail(CP_ERR_BAD_PARAM, "NULL argument");
+    memset(out, 0, sizeof(*out));
+    EvRec rec;
+    for (auto& e : rec.ev) CK(cudaEventCreate(&e));
+    cp_status s = CP_OK;
+    for (int it = 0; it < n_outer && s == CP_OK; ++it) {
+        if ((s = read_status(c)) != CP_OK) break;
+        if (c->stHost->done) break;
+        rec.n = 0;
+        if ((s = enqueue_iteration_any(c, &rec)) != CP_OK) break;
+        if ((s = read_status(c)) != CP_OK) break;
+        for (int q = 0; q < rec.n; ++q) {
+            float ms = 0.f;
+            if (cudaEventElapsedTime(&ms, rec.ev[2 * q], rec.ev[2 * q + 1]) == cudaSuccess) {
+                out->ms[rec.kind[q]] += ms;
+                out->launches[rec.kind[q]] += 1;
+            }
+        }
+        out->jacobiSweeps += c->stHost->itersU + c->stHost->itersV;
+        out->pcgIterations += c->stHost->itersP;
+        out->iterations += 1;
+        if ((s = device_error(c)) != CP_OK) break;
+    }
+    for (auto& e : rec.ev) cudaEventDestroy(e);
+    return s;
+}
+
+static cp_status momentum_one(cp_ctx* c, int isU, double* resid, int* iters) {
+    if (!c) return fail(CP_ERR_BAD_PARAM, "ctx is NULL");
+    cp_status s = read_status(c);
+    if (s != CP_OK) return s;
+    if (c->stHost->done) return fail(CP_ERR_STATE, "loop already stopped; call cp_reset_loop first");
+    // reset the max-change accumulators, then assemble + solve one component
+    CK(cudaMemsetAsync(&c->st->maxDU, 0, 2 * sizeof(unsigned long long), c->stream));
+    s = c->prm.precision == CP_PREC_MIXED ? enqueue_momentum<float, true>(c, isU, !isU, 0)
+                                          : enqueue_momentum<double, false>(c, isU, !isU, 0);
+    if (s != CP_OK) return s;
+    if ((s = read_status(c)) != CP_OK) return s;
+    const unsigned long long bits = isU ? c->stHost->maxDU : c->stHost->maxDV;
+    double r;
+    memcpy(&r, &bits, sizeof r);
+    if (resid) *resid = r;
+    if (iters) *iters = isU ? c->stHost->itersU : c->stHost->itersV;
+    return device_error(c);
+}
+
+cp_status cp_momentum_u(cp_ctx* c, double* resid, int* iters) { return momentum_one(c, 1, resid, iters); }
+cp_status cp_momentum_v(cp_ctx* c, double* resid, int* iters) { return momentum_one(c, 0, resid, iters); }
+
+cp_status cp_pressure(cp_ctx* c, int* iters, double* residMass) {
+    if (!c) return fail(CP_ERR_BAD_PARAM, "ctx is NULL");
+    cp_status s = read_status(c);
+    if (s != CP_OK) return s;
+    if (c->stHost->done) return fail(CP_ERR_STATE, "loop already stopped; call cp_reset_loop first");
+    CK(cudaMemsetAsync(c->pStar, 0, c->nElem * sizeof(double), c->stream));
+    s = c->prm.precision == CP_PREC_MIXED ? enqueue_pressure<float>(c) : enqueue_pressure<double>(c);
+    if (s != CP_OK) return s;
+    std::vector<double> part((size_t)4 * c->nbMass);
+    CK(cudaMemcpyAsync(part.data(), c->partM, part.size() * 8, cudaMemcpyDeviceToHost, c->stream));
+    if ((s = read_status(c)) != CP_OK) return s;
+    double mx = 0.0;
+    for (int b = 0; b < c->nbMass; ++b) mx = std::max(mx, part[(size_t)b * 4 + 3]);
+    if (residMass) *residMass = mx;
+    if (iters) *iters = c->stHost->itersP;
+    return device_error(c);
+}
+
+int cp_history_columns(void) { return kHistCols; }
+
+cp_status cp_get_history(cp_ctx* c, double* rows, int max_rows, int* n_rows) {
+    if (!c || !rows) return fail(CP_ERR_BAD_PARAM, "NULL argument");
+    cp_status s = read_status(c);
+    if (s != CP_OK) return s;
+    const int n = std::min(std::min(c->stHost->iter, c->histCap), std::max(max_rows, 0));
+    if (n > 0)
+        CK(cudaMemcpy(rows, c->hist, (size_t)n * kHistCols * sizeof(double), cudaMemcpyDeviceToHost));
+    if (n_rows) *n_rows = n;
+    return CP_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,244 @@
+/*
+ * cp_simple.h - C ABI of the B200-native SIMPLE solver (libcoldplate.so).
+ *
+ * Drop-in boundary for the reference's 2-D staggered-grid SIMPLE iteration
+ * (Carloossgg/coldplate-solver).  All state lives on the GPU inside a
+ * cp_ctx; host arrays cross this interface only as plain pointers with
+ * explicit (rows, cols, row_stride, col_stride) in elements, so Eigen's
+ * column-major MatrixXf/MatrixXd (row_stride 1, col_stride rows) and numpy's
+ * row-major arrays both pass without copies on the caller's side.
+ *
+ * Index conventions are the reference's: physical cells Ny x Nx,
+ * M = Ny + 1, N = Nx + 1 (SIMPLE.cpp:53-54); u is (M+1) x N, v is M x (N+1),
+ * p is (M+1) x (N+1) (SIMPLE.cpp:252-273).
+ *
+ * Every call returns a cp_status; cp_last_error_string() describes the last
+ * failure of the calling thread.  Contexts are independent: one per host
+ * thread (or stream) may run concurrently.
+ */
+#ifndef CP_SIMPLE_H
+#define CP_SIMPLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum cp_status {
+    CP_OK = 0,
+    CP_ERR_BAD_PARAM = 1,    /* invalid argument or parameter value          */
+    CP_ERR_UNSUPPORTED = 2,  /* a reference option this build does not run  */
+    CP_ERR_NONFINITE = 3,    /* NaN/Inf in inputs or produced by the solve   */
+    CP_ERR_DIVERGED = 4,     /* residual growth beyond the divergence limit  */
+    CP_ERR_TIMEOUT = 5,      /* a bounded device-side wait gave up           */
+    CP_ERR_CUDA = 6,         /* a CUDA runtime call failed                   */
+    CP_ERR_STATE = 7         /* call not valid in the context's state        */
+} cp_status;
+
+/* Arithmetic of the inner solves.  CP_PREC_FP64: everything in double (the
+ * reference algorithm re-typed).  CP_PREC_MIXED: momentum Jacobi sweeps and
+ * the PCG matvec/preconditioner in float on corrections of double state;
+ * residuals, global dot products, the mass imbalance and all fields stay
+ * double, so the converged fixed point is the FP64 one. */
+typedef enum cp_precision { CP_PREC_FP64 = 0, CP_PREC_MIXED = 1 } cp_precision;
+
+typedef enum cp_stop_reason {
+    CP_RUNNING = 0,
+    CP_STOP_RESIDUAL = 1,    /* error <= epsilon (SIMPLE.cpp:378)            */
+    CP_STOP_MAX_ITER = 2,    /* maxIterations reached                        */
+    CP_STOP_DP_WINDOW = 3,   /* pressure-drop window (SIMPLE.cpp:449-491)    */
+    CP_STOP_ERROR = 4        /* a device-side error stopped the loop         */
+} cp_stop_reason;
+
+typedef enum cp_field {
+    CP_FIELD_U = 0, CP_FIELD_V, CP_FIELD_P, CP_FIELD_USTAR, CP_FIELD_VSTAR, CP_FIELD_PSTAR,
+    CP_FIELD_DE, CP_FIELD_DN, CP_FIELD_GAMMA, CP_FIELD_ALPHA, CP_FIELD_CELLTYPE
+} cp_field;
+
+/*
+ * Parameter set: the public knobs of class SIMPLE (SIMPLE.h:68-448) with the
+ * same names and defaults (floats widened to double, bools as int), plus the
+ * inputs the reference reads from ExportFiles/fluid_params.txt
+ * (SIMPLE.cpp:41-59).  cp_params_default() fills the SIMPLE.h defaults.
+ * Options that this build does not run must keep their default "off" value;
+ * cp_create() returns CP_ERR_UNSUPPORTED otherwise.
+ */
+typedef struct cp_params {
+    /* fluid_params.txt: "Ny Nx hy hx U N_in N_out [Ht]" */
+    int Ny, Nx;                    /* physical cells (file order: rows, cols) */
+    double hy, hx;                 /* cell size [m]                            */
+    double targetVel;              /* inlet velocity U [m/s]                   */
+    int N_in_buffer, N_out_buffer; /* thermal crop buffers (bookkeeping only)  */
+    double Ht_channel;             /* out-of-plane height [m] (optional)       */
+
+    /* convergence control (SIMPLE.h:68-69) */
+    double epsilon;
+    int maxIterations;
+    /* output / restart (SIMPLE.h:77-78); host-side only */
+    int saveStateInterval;
+    int reuseInitialFields;
+    /* sampling planes (SIMPLE.h:88-89) */
+    double xPlaneCoreInlet, xPlaneCoreOutlet;
+    /* pressure-drop convergence (SIMPLE.h:98-103) */
+    int usePressureDropConvergence;
+    int dpConvergenceWindow;
+    double dpConvergencePercent;
+    int usePressureDropSlopeGate;
+    int dpSlopeWindowIters;
+    double dpSlopeMaxDelta;
+    /* OpenMP threads of the CPU code (SIMPLE.h:111); ignored */
+    int numThreads;
+    /* pressure solver (SIMPLE.h:145-156): types 1 (PCG) and 4 (the GPU type)
+     * run the native matrix-free PCG; 0, 2, 3 are CP_ERR_UNSUPPORTED */
+    int pressureSolverType;
+    int parallelizeDirectSolver;
+    int maxPressureIter;
+    double pTol;
+    double sorOmega;
+    /* momentum solver (SIMPLE.h:172-183): only type 1 (implicit Jacobi) */
+    int momentumSolverType;
+    double momentumTol;
+    int maxMomentumIter;
+    double momentumSorOmega;        /* printed by the reference, never used */
+    /* convection (SIMPLE.h:193): 0 FOU, 1 SOU deferred correction */
+    int convectionScheme;
+    /* 2.5-D model (SIMPLE.h:205-208) */
+    int enableTwoPointFiveD;
+    double twoPointFiveDConvectionFactor;
+    double twoPointFiveDSinkMultiplier;
+    /* Brinkman penalisation (SIMPLE.h:242-244); alpha_max = eta / K_min */
+    double brinkmanKMin;
+    double brinkmanQ;
+    /* pseudo-transient continuation (SIMPLE.h:260-345): must stay off */
+    double timeStepMultiplier;
+    int enablePseudoTimeStepping;
+    double pseudoCFL;
+    double minPseudoSpeed;
+    int useLocalPseudoTime;
+    int pseudoControllerMode;
+    int enableSER;
+    int enableLineSearch;
+    int enableCflRamp;
+    /* fluid properties (SIMPLE.h:374-375) */
+    double rho, eta;
+    /* inlet ramp (SIMPLE.h:385-386) */
+    int enableInletRamp;
+    int rampSteps;
+    /* under-relaxation (SIMPLE.h:397-398) */
+    double uvAlpha, pAlpha;
+    /* residual artificial viscosity (SIMPLE.h:406-411): must stay off */
+    int enableResidualViscosity;
+    /* residual reporting (SIMPLE.h:424, 447-448) */
+    int enableNormalizedResiduals;
+    double residNormFloorVel, residNormFloorMass;
+
+    /* ---- additions of this implementation ---- */
+    int precision;                  /* cp_precision                           */
+    int refineRounds;               /* mixed: extra FP32 PCG correction rounds
+                                       driven by the FP64 refinement residual */
+    int historyCapacity;            /* rows of per-iteration history kept     */
+    int chunk;                      /* outer iterations between host polls    */
+} cp_params;
+
+/* Per-iteration record (one row of the history, see cp_get_history). */
+typedef struct cp_iter_report {
+    int iter;                 /* completed outer iterations                   */
+    int done;                 /* 1 once the loop stopped                      */
+    int stop_reason;          /* cp_stop_reason                               */
+    int pressureIterations;   /* PCG iterations of the last outer iteration   */
+    int momentumItersU, momentumItersV;
+    double error;             /* max(residU, residV, residMass) as reported   */
+    double residU, residV, residMass;          /* reported (raw or normalised) */
+    double residU_RMS, residV_RMS, residMass_RMS;
+    double residU_max, residV_max, residMass_max;
+    double coreTotalDrop, fullTotalDrop;       /* total-pressure drop [Pa]     */
+    double coreStaticDrop, fullStaticDrop;
+    double inletMassFlux, outletMassFlux;      /* [kg/s per m depth]           */
+    double device_ms;         /* device time of the call (CUDA events)         */
+} cp_iter_report;
+
+typedef struct cp_ctx cp_ctx;
+
+/* Fills the SIMPLE.h defaults (pressureSolverType 4, maxPressureIter 30, ...). */
+void cp_params_default(cp_params* p);
+
+/* Reads "Ny Nx hy hx U N_in N_out [Ht]" like SIMPLE::loadParameters
+ * (SIMPLE.cpp:31-66) into the grid fields of *p. */
+cp_status cp_read_fluid_params(const char* path, cp_params* p);
+
+/* Allocates the device state for p (validated first). Fields start at zero
+ * and gamma at 1 (all fluid), like SIMPLE::initializeMemory. */
+cp_status cp_create(const cp_params* p, cp_ctx** out);
+cp_status cp_destroy(cp_ctx* ctx);
+
+/* Geometry.  cellType: Ny x Nx, 0 fluid .. 1 solid (geometry_fluid.txt,
+ * SIMPLE.cpp:633-690, converted as SIMPLE.cpp:695-777).  gamma: Ny x Nx
+ * density, 1 fluid .. 0 solid (set directly, e.g. by an optimiser). */
+cp_status cp_set_cell_type(cp_ctx* ctx, const double* cellType, long rows, long cols,
+                           long row_stride, long col_stride);
+cp_status cp_set_gamma(cp_ctx* ctx, const double* gamma, long rows, long cols,
+                       long row_stride, long col_stride);
+cp_status cp_read_geometry(cp_ctx* ctx, const char* path);
+
+/* Field transfer in the reference shapes (see cp_field). */
+cp_status cp_get_field(cp_ctx* ctx, cp_field which, double* host, long rows, long cols,
+                       long row_stride, long col_stride);
+cp_status cp_set_field(cp_ctx* ctx, cp_field which, const double* host, long rows, long cols,
+                       long row_stride, long col_stride);
+
+/* Whole outer iterations: SIMPLE::calculateStep (iterations.cpp:82) plus the
+ * pressure sampling and stop rules of SIMPLE::runIterations
+ * (SIMPLE.cpp:378-491).  cp_step runs at most n_outer iterations (fewer if the
+ * loop stops); cp_run runs until a stop rule fires.  `out` (may be NULL)
+ * receives the last iteration's record. */
+cp_status cp_step(cp_ctx* ctx, int n_outer, cp_iter_report* out);
+cp_status cp_run(cp_ctx* ctx, cp_iter_report* out);
+/* Clears the stop state so that cp_step/cp_run continue from the fields. */
+cp_status cp_reset_loop(cp_ctx* ctx);
+/* Back to the state after construction: u, v, p, u*, v*, p', dE, dN zero,
+ * loop state and history cleared; geometry and parameters kept.  No
+ * allocation, so repeated solves of one geometry reuse the device buffers. */
+cp_status cp_reset(cp_ctx* ctx);
+
+/* Solver-dispatch boundary of the reference (SIMPLE.h:876-880, 546):
+ *   cp_momentum_u  ~ int solveUMomentumImplicit(SIMPLE&, float& residU)
+ *   cp_momentum_v  ~ int solveVMomentumImplicit(SIMPLE&, float& residV)
+ *   cp_pressure    ~ bool SIMPLE::solvePressureSystem(int&, float&)
+ * They act on the device-resident u, v, p (cp_set_field) and write uStar /
+ * vStar, dE / dN and pStar like the reference; *iters gets the Jacobi or PCG
+ * iteration count, *resid the max |u* - u| and *residMass the max mass
+ * imbalance. */
+cp_status cp_momentum_u(cp_ctx* ctx, double* resid, int* iters);
+cp_status cp_momentum_v(cp_ctx* ctx, double* resid, int* iters);
+cp_status cp_pressure(cp_ctx* ctx, int* iters, double* residMass);
+
+/* Per-iteration history rows (cp_iter_report layout without device_ms, as
+ * doubles: see cp_history_columns()).  Returns the number of rows copied. */
+int cp_history_columns(void);
+cp_status cp_get_history(cp_ctx* ctx, double* rows, int max_rows, int* n_rows);
+
+/* Per-kernel device time (CUDA events around each launch) over n_outer
+ * iterations run without graph capture; the native counterpart of the
+ * reference's GlobalTimer / ScopedTimer phases (Utilities/Timer.h:12-82).
+ * Kernel kinds: see cp_kernel_kind.  The iterations advance the solution
+ * like cp_step. */
+typedef enum cp_kernel_kind {
+    CP_K_BC = 0, CP_K_ASSEMBLE, CP_K_JACOBI, CP_K_MASS, CP_K_PCG, CP_K_CORRECT, CP_K_FINALIZE,
+    CP_K_COUNT
+} cp_kernel_kind;
+typedef struct cp_kernel_timing {
+    double ms[CP_K_COUNT];      /* summed device time per kind            */
+    int launches[CP_K_COUNT];   /* launches per kind                      */
+    long long jacobiSweeps;     /* sweeps (U + V) run by the Jacobi kernel */
+    long long pcgIterations;    /* PCG iterations run                      */
+    int iterations;             /* outer iterations timed                  */
+} cp_kernel_timing;
+cp_status cp_kernel_times(cp_ctx* ctx, int n_outer, cp_kernel_timing* out);
+
+const char* cp_status_string(cp_status s);
+const char* cp_last_error_string(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CP_SIMPLE_H */

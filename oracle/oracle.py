@@ -93,6 +93,9 @@ def _lib(prec: str) -> ctypes.CDLL:
             "orc_set_inlet_velocity": (None, [vp, ctypes.c_double]),
             "orc_wall_flags": (None, [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_ubyte)]),
             "orc_assemble": (None, [vp, ctypes.c_int]),
+            "orc_momentum": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_void_p]),
+            "orc_pressure": (ctypes.c_int, [vp, ctypes.c_void_p]),
+            "orc_velocity_bc": (None, [vp, ctypes.c_void_p, ctypes.c_void_p]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(lib, name + sfx)
@@ -203,6 +206,21 @@ class Oracle:
 
     def assemble(self, isU: bool) -> None:
         self.lib.orc_assemble(self.h, 1 if isU else 0)
+
+    def _real(self):
+        return ctypes.c_float() if self.prec == "f32" else ctypes.c_double()
+
+    def momentum(self, isU: bool) -> tuple[int, float]:
+        """solveUMomentumImplicit / solveVMomentumImplicit on the current state."""
+        r = self._real()
+        it = self.lib.orc_momentum(self.h, 1 if isU else 0, ctypes.byref(r))
+        return it, float(r.value)
+
+    def pressure(self) -> tuple[int, float]:
+        """solvePressureSystem on the current u*, v*, dE, dN."""
+        r = self._real()
+        it = self.lib.orc_pressure(self.h, ctypes.byref(r))
+        return it, float(r.value)
 
 
 # --------------------------------------------------------------------------

@@ -106,6 +106,7 @@ typedef struct {
     real residU_RMS, residV_RMS, residMass_RMS, residU_RMS0, residV_RMS0, residMass_RMS0;
     int rmsU0set, rmsV0set, rmsM0set;
     int lastMomItersU, lastMomItersV, lastPressureIters, iter;
+    double lastError;   /* error of the last completed iteration (1 before any) */
 } orc_state;
 
 #define UI(s, i, j) ((size_t)(i) * (size_t)(s)->N + (size_t)(j))        /* u, dE: (M+1) x N */
@@ -196,6 +197,7 @@ static orc_state* state_alloc(int Ny, int Nx) {
     s->pdiag = alloc0(nm); s->pb = alloc0(nm); s->px = alloc0(nm);
     s->residU = s->residV = s->residMass = RL(1.0);
     s->residU_max = s->residV_max = s->residMass_max = RL(1.0);
+    s->lastError = 1.0;
     return s;
 }
 
@@ -880,10 +882,9 @@ void ORC(orc_sample_patch)(const orc_state* s, int inlet, double* out) {
 #define ORC_HIST_COLS 15
 
 int ORC(orc_run)(orc_state* s, int maxIter, double* hist, int histCap) {
-    double error = 1.0;
+    double error = s->lastError;
     int n = 0;
-    const int lim = maxIter < s->maxIterations ? maxIter : s->maxIterations;
-    while (s->iter < lim && error > (double)s->epsilon) {
+    while (n < maxIter && s->iter < s->maxIterations && error > (double)s->epsilon) {
         if (s->enableInletRamp && s->rampSteps > 0 && s->iter < s->rampSteps)
             s->inletVelocity = ((real)(s->iter + 1) / (real)s->rampSteps) * s->targetVel;
         else
@@ -891,6 +892,7 @@ int ORC(orc_run)(orc_state* s, int maxIter, double* hist, int histCap) {
         int pit = 0;
         real e = (real)ORC(orc_step)(s, &pit);
         error = (double)e;
+        s->lastError = error;
         double ci[5], co[5], fi[5], fo[5];
         ORC(orc_sample_plane)(s, (double)s->xCoreIn, ci);
         ORC(orc_sample_plane)(s, (double)s->xCoreOut, co);
