@@ -35,10 +35,13 @@ sys.path.insert(0, os.path.join(ROOT, "coldplate-solver_b200"))
 
 METRIC = "time-to-converge 2048×1024 (ΔP rel err ≤1e-5): mixed vs FP64 GPU; adjoint/fwd"
 DP_TOL = 1e-5
-# outer iterations of the FP64 solve of the default workload, measured by
-# the calibration run of this script on a B200 (used only by the reference
-# arm, which has no GPU run to count them from)
-DEFAULT_K64 = None
+# outer iterations of the FP64 solve of the default workload (2048 x 1024,
+# seed 0), measured by this script's calibration run on a B200; used only by
+# the reference arm, which has no GPU run to count them from
+DEFAULT_K64 = 146
+# the pressure solver of the timed workload: pressureSolverType 4 is the
+# reference's default (its AMG-CG GPU solver); here multigrid-PCG
+BENCH_KNOBS = dict(pressureSolverType=4, maxPressureIter=30, pTol=1e-8)
 
 
 def parse():
@@ -50,7 +53,7 @@ def parse():
     ap.add_argument("--ny", type=int, default=1024)
     ap.add_argument("--nx", type=int, default=2048)
     ap.add_argument("--seed", type=int, default=0)
-    ap.add_argument("--max-iter", type=int, default=60000)
+    ap.add_argument("--max-iter", type=int, default=3000)
     ap.add_argument("--cpu-sample-iters", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
@@ -120,12 +123,12 @@ def first_stable_iter(dp: np.ndarray, dp_star: float, tol: float = DP_TOL) -> in
 def calibrate(Simple, case, prec: str, max_iter: int):
     """Untimed run until the full pressure drop is stationary (relative
     change over 200 iterations below 1e-9, or residual epsilon 1e-12)."""
-    prm = case.params(precision=prec, maxIterations=max_iter, epsilon=1e-12, historyCapacity=max_iter,
-                      chunk=200)
+    prm = case.params(precision=prec, maxIterations=max_iter, epsilon=1e-14, historyCapacity=max_iter,
+                      chunk=100)
     with Simple(cellType=case.cellType, **prm) as g:
         done = 0
         while done < max_iter:
-            rep = g.step(1000)
+            rep = g.step(100)
             done = rep["iter"]
             h = g.history()
             dp = h["fullTotal"]
@@ -141,12 +144,17 @@ def calibrate(Simple, case, prec: str, max_iter: int):
 def cpu_baseline(case, n_iter: int, k_converge: int) -> dict | None:
     """The reference's own CPU path (oracle/_ref/ref_f32, built from its
     sources) on this workload, all host threads, a bounded sample of outer
-    iterations; time-to-converge extrapolated with the FP64 iteration count."""
+    iterations; time-to-converge extrapolated with the FP64 iteration count.
+    Without AMGCL the reference runs pressureSolverType 4 as its Jacobi-PCG
+    (SIMPLE.cpp:167-185), which needs far more outer iterations than k, so
+    the extrapolation is a lower bound on its time."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     from oracle import REF_DIR, write_case
     cores = os.cpu_count() or 1
     exe = os.path.join(REF_DIR, "ref_f32")
-    prm = case.params(maxIterations=n_iter, epsilon=1e-30)
+    # without AMGCL the reference resolves pressureSolverType 4 to its PCG
+    # at load time (SIMPLE.cpp:167-185)
+    prm = case.params(maxIterations=n_iter, epsilon=1e-30, pressureSolverType=1)
     if os.path.exists(exe):
         from oracle import ref_overrides
         with tempfile.TemporaryDirectory() as d:
@@ -169,7 +177,8 @@ def cpu_baseline(case, n_iter: int, k_converge: int) -> dict | None:
     s_per_it = float(np.mean(secs[1:] if len(secs) > 1 else secs))
     return {"value": s_per_it * k_converge, "unit": "s", "cores": used, "kind": kind,
             "sample": f"{len(secs)} outer iterations of the same workload, {s_per_it:.3f} s each, "
-                      f"extrapolated to {k_converge} iterations",
+                      f"extrapolated to {k_converge} iterations (lower bound: without AMGCL the "
+                      f"reference's pressure solver is Jacobi-PCG)",
             "s_per_outer_iteration": s_per_it}
 
 
@@ -208,7 +217,7 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     from coldplate_b200 import cases
-    case = cases.density_field(args.ny, args.nx, seed=args.seed + rank)
+    case = cases.density_field(args.ny, args.nx, seed=args.seed + rank, **BENCH_KNOBS)
     if args.impl == "reference":
         return reference_arm(args, case, rank)
 
@@ -268,7 +277,11 @@ def main():
     w_mix = 4
     pcg_ms = kt["ms"]["pcg"] / max(kt["launches"]["pcg"], 1)
     pcg_iters = kt["pcgIterations"] / max(kt["launches"]["pcg"], 1)
-    pcg_bytes = pcg_iters * 8 * w_mix * nP          # 8 w per unknown per PCG iteration
+    # 23 w per unknown per multigrid-PCG iteration: 8 w for the CG vectors
+    # (read x, r, p, dE, dN; write x, r, p) and 15 w for the V(1,1) cycle
+    # (fine-level restriction and prolongation-smoothing, 11.25 w, times 4/3
+    # for the coarse levels)
+    pcg_bytes = pcg_iters * 23 * w_mix * nP
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -277,7 +290,7 @@ def main():
     peak = float(peaks.get("hbm_gbs", 6650.0))
     achieved = pcg_bytes / (pcg_ms * 1e-3) / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": None, "kernel": "k_pcg<float>",
+                "traffic": None, "kernel": "k_pcg_mg<float>",
                 "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"}
 
     # ---- end to end through the public API with host buffers

@@ -12,8 +12,9 @@ Workloads
                     (3-6 inlets, widths 8-24 cells, split/merge probability
                     0.3), SOU, 2.5-D sink with Ht = 200 um
   density_field     continuous density: a Gaussian random field (correlation
-                    length 32 cells) through a tanh projection (beta 8,
-                    eta 0.5), Brinkman alpha_max 1e9 with q = 0.1, SOU, 2.5-D;
+                    length 32 cells, mean 0.6, std 0.2) through a tanh
+                    projection (beta 8, eta 0.5), Brinkman alpha_max 1e9 with
+                    q = 0.1, SOU, 2.5-D;
                     fluid inlet/outlet buffers keep the boundary patches pure
                     fluid so the pressure drop is defined
   batch             density fields of random sizes (Nx 256-1024, Ny 128-512)
@@ -175,10 +176,17 @@ def tanh_projection(g: np.ndarray, beta: float = 8.0, eta: float = 0.5) -> np.nd
 
 
 def density_gamma(Ny: int, Nx: int, seed: int, corr: float = 32.0, buffer: int = 32,
-                  wall: int | None = None) -> np.ndarray:
-    """gamma (1 fluid .. 0 solid) of the density workload."""
+                  wall: int | None = None, mean: float = 0.6, std: float = 0.2) -> np.ndarray:
+    """gamma (1 fluid .. 0 solid) of the density workload.  The random field
+    is standardised to the given mean and standard deviation before the
+    projection: with mean 0.6 about 70 % of the cells lie above eta = 0.5,
+    so the fluid phase percolates from inlet to outlet (a field centred on
+    eta sits at the 2-D percolation threshold and forces the flow through
+    Brinkman solid)."""
     rng = np.random.default_rng(seed)
-    gam = tanh_projection(gaussian_random_field(Ny, Nx, corr, rng))
+    g = gaussian_random_field(Ny, Nx, corr, rng)
+    g = mean + std * (g - g.mean()) / max(g.std(), 1e-300)
+    gam = tanh_projection(g)
     gam = np.clip(gam, 0.0, 1.0)
     b = min(buffer, Nx // 8)
     gam[:, :b] = 1.0

@@ -248,35 +248,115 @@ __global__ void k_assemble(KParams k, const Status* st, Fields f, MomSys<TC> U, 
 }
 
 // ------------------------------------------------------------------ Jacobi
-// Jacobi sweeps x+ = x + (b - A x) / aP on U and V together (they are
-// independent: V assembles from u, v, not from u*).  Each component stops
-// after the first sweep whose pre-update sum of r^2 is below tol^2 n, or
-// after maxMomentumIter sweeps (jacobi_solver.cpp:44-67).  One grid barrier
-// per sweep; the sums are per-block partials added in a fixed order.
+// One component's sweeps.  Each thread handles two rows per loop trip with
+// all loads issued before the arithmetic (memory-level parallelism); the
+// sum of r^2 is reduced per sweep, one grid barrier per sweep.  Returns the
+// buffer index holding the result (-1: the initial iterate) and the sweep
+// count, or false if a barrier gave up.
+template <typename TC, bool Mixed, bool IsU>
+__device__ __forceinline__ bool jacobi_component(const KParams& k, Status* st, const MomSys<TC>& S,
+                                                 const double* field, TC* x0, TC* x1, double* part,
+                                                 unsigned* bar, unsigned& target, int& cur, int& its) {
+    __shared__ double sm[32];
+    const Dims d = k.d;
+    const int G = gridDim.x;
+    int i1, j1;
+    mom_range<IsU>(d, i1, j1);
+    const int w = j1, n = i1 * j1;
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = G * blockDim.x;
+    const double lim = k.momTol * k.momTol * (double)n;
+    TC* xs[2] = {x0, x1};
+    cur = -1;
+    its = 0;
+    for (int s = 0; s < k.maxMom; ++s) {
+        const int nxt = cur < 0 ? 0 : 1 - cur;
+        const TC* xc = cur < 0 ? nullptr : xs[cur];
+        TC* __restrict__ xn = xs[nxt];
+        const bool first = cur < 0;
+        double acc[1] = {0.0};
+        for (int t0 = tid; t0 < n; t0 += 2 * nth) {
+            TC v[2][11];
+            size_t cc[2];
+            bool ok[2];
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                const int t = t0 + q * nth;
+                ok[q] = t < n;
+                const int tt = ok[q] ? t : t0;
+                const int i = 1 + tt / w, j = 1 + tt % w;
+                const size_t c = at(d, i, j);
+                cc[q] = c;
+                auto X = [&](size_t a) -> TC {
+                    if (first) return Mixed ? (TC)0 : (TC)field[a];
+                    return xc[a];
+                };
+                v[q][0] = S.aP[c]; v[q][1] = S.aE[c]; v[q][2] = S.aW[c]; v[q][3] = S.aN[c]; v[q][4] = S.aS[c];
+                v[q][5] = S.b[c];
+                v[q][6] = X(c);
+                v[q][7] = (i > 1) ? X(c - d.P) : (TC)0;
+                v[q][8] = (j > 1) ? X(c - 1) : (TC)0;
+                v[q][9] = (j < j1) ? X(c + 1) : (TC)0;
+                v[q][10] = (i < i1) ? X(c + d.P) : (TC)0;
+            }
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                if (!ok[q]) continue;
+                // S, W, P, E, N order of the reference's CSR rows
+                TC Ax = (TC)0;
+                Ax += (-v[q][4]) * v[q][7];
+                Ax += (-v[q][2]) * v[q][8];
+                Ax += v[q][0] * v[q][6];
+                Ax += (-v[q][1]) * v[q][9];
+                Ax += (-v[q][3]) * v[q][10];
+                const TC r = v[q][5] - Ax;
+                xn[cc[q]] = v[q][6] + r / v[q][0];
+                acc[0] += (double)r * (double)r;
+            }
+        }
+        block_sum<1>(acc, sm);
+        double* slot = part + (size_t)(s & 1) * G;
+        if (threadIdx.x == 0) slot[blockIdx.x] = acc[0];
+        target += G;
+        if (!grid_barrier(bar, target, &st->err)) return false;
+        double tot[1];
+        sum_partials<1>(slot, G, 1, tot, sm);
+        cur = nxt;
+        its = s + 1;
+        if (tot[0] < lim) break;
+    }
+    return true;
+}
+
+// scatter with clamp and max |u* - u| (momentum_solver.cpp:335-351)
+template <typename TC, bool Mixed, bool IsU>
+__device__ __forceinline__ double jacobi_scatter(const KParams& k, const double* field, const TC* xr,
+                                                 double* out, double maxVel, int tid, int nth) {
+    const Dims d = k.d;
+    int i1, j1;
+    mom_range<IsU>(d, i1, j1);
+    const int w = j1, n = i1 * j1;
+    double m = 0.0;
+    for (int t = tid; t < n; t += nth) {
+        const int i = 1 + t / w, j = 1 + t % w;
+        const size_t c = at(d, i, j);
+        double xv = xr ? (double)xr[c] : (Mixed ? 0.0 : field[c]);
+        if (Mixed) xv += field[c];
+        const double nv = dclamp(xv, -maxVel, maxVel);
+        m = dmax(m, fabs(nv - field[c]));
+        out[c] = nv;
+    }
+    return m;
+}
+
+// Jacobi sweeps x+ = x + (b - A x) / aP of the U system, then of the V
+// system (they are independent: V assembles from u, v, not from u*).  Each
+// component stops after the first sweep whose pre-update sum of r^2 is
+// below tol^2 n, or after maxMomentumIter sweeps (jacobi_solver.cpp:44-67).
+// Running the components one after the other keeps one component's system
+// resident in L2.  Then the scatter with clamps and the BCs on u*, v*.
 struct JacobiOut {
     double *uStar, *vStar;
 };
-
-template <typename TC, bool Mixed, bool IsU>
-__device__ __forceinline__ double jacobi_row(const Dims& d, const MomSys<TC>& s, const TC* xc, TC* xn,
-                                             const double* field, bool first, int i, int j, int i1, int j1) {
-    const size_t c = at(d, i, j);
-    // first sweep starts from the current field (FP64 form) or from 0 (mixed)
-    auto X = [&](size_t q) -> TC {
-        if (first) return Mixed ? (TC)0 : (TC)field[q];
-        return xc[q];
-    };
-    TC Ax = (TC)0;
-    if (i > 1) Ax += (-s.aS[c]) * X(c - d.P);
-    if (j > 1) Ax += (-s.aW[c]) * X(c - 1);
-    const TC xP = X(c);
-    Ax += s.aP[c] * xP;
-    if (j < j1) Ax += (-s.aE[c]) * X(c + 1);
-    if (i < i1) Ax += (-s.aN[c]) * X(c + d.P);
-    const TC r = s.b[c] - Ax;
-    xn[c] = xP + r / s.aP[c];
-    return (double)r * (double)r;
-}
 
 template <typename TC, bool Mixed>
 __global__ void __launch_bounds__(256) k_jacobi(KParams k, Status* st, MomSys<TC> U, MomSys<TC> V,
@@ -284,77 +364,19 @@ __global__ void __launch_bounds__(256) k_jacobi(KParams k, Status* st, MomSys<TC
                                                 TC* xV1, JacobiOut out, const double* gamma, double* part,
                                                 unsigned* bar, int doU, int doV, int applyBC) {
     if (st->done) return;
-    __shared__ double sm[64];
-    const Dims d = k.d;
     const int G = gridDim.x;
     const int iter = st->iter;
     const double maxVel = max_vel(inlet_velocity(k, iter));
-    const int nU = doU ? k.nU : 0, nV = doV ? k.nV : 0;
-    const int wU = d.N - 2, wV = d.N - 1;
-    const int iU1 = d.M - 1, jU1 = d.N - 2, iV1 = d.M - 2, jV1 = d.N - 1;
-    const double tolsq = k.momTol * k.momTol;
-    TC* xu[2] = {xU0, xU1};
-    TC* xv[2] = {xV0, xV1};
-    bool convU = (nU == 0), convV = (nV == 0);
-    int itU = 0, itV = 0, curU = -1, curV = -1;  // -1: still the initial iterate
-    unsigned target = 0;
     const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = G * blockDim.x;
-    for (int s = 0; s < k.maxMom && !(convU && convV); ++s) {
-        double acc[2] = {0.0, 0.0};
-        const int nxtU = curU < 0 ? 0 : 1 - curU, nxtV = curV < 0 ? 0 : 1 - curV;
-        const int nu = convU ? 0 : nU, nv = convV ? 0 : nV;
-        for (int t = tid; t < nu + nv; t += nth) {
-            if (t < nu) {
-                const int i = 1 + t / wU, j = 1 + t % wU;
-                acc[0] += jacobi_row<TC, Mixed, true>(d, U, curU < 0 ? nullptr : xu[curU], xu[nxtU], u, curU < 0, i, j,
-                                                      iU1, jU1);
-            } else {
-                const int q = t - nu;
-                const int i = 1 + q / wV, j = 1 + q % wV;
-                acc[1] += jacobi_row<TC, Mixed, false>(d, V, curV < 0 ? nullptr : xv[curV], xv[nxtV], v, curV < 0, i,
-                                                       j, iV1, jV1);
-            }
-        }
-        block_sum<2>(acc, sm);
-        double* slot = part + (size_t)(s & 1) * 2 * G;
-        if (threadIdx.x == 0) { slot[2 * blockIdx.x] = acc[0]; slot[2 * blockIdx.x + 1] = acc[1]; }
-        target += G;
-        if (!grid_barrier(bar, target, &st->err)) return;
-        double tot[2];
-        sum_partials<2>(slot, G, 2, tot, sm);
-        if (!convU) {
-            itU = s + 1;
-            curU = nxtU;
-            if (tot[0] < tolsq * (double)nU) convU = true;
-        }
-        if (!convV) {
-            itV = s + 1;
-            curV = nxtV;
-            if (tot[1] < tolsq * (double)nV) convV = true;
-        }
-    }
-    // scatter with clamp and max |u* - u| (momentum_solver.cpp:335-351)
+    unsigned target = 0;
+    int curU = -1, curV = -1, itU = 0, itV = 0;
+    if (doU && !jacobi_component<TC, Mixed, true>(k, st, U, u, xU0, xU1, part, bar, target, curU, itU)) return;
+    // V uses its own partial slots: blocks may still read U's last sums
+    if (doV && !jacobi_component<TC, Mixed, false>(k, st, V, v, xV0, xV1, part + 2 * G, bar, target, curV, itV))
+        return;
     double mu = 0.0, mv = 0.0;
-    for (int t = tid; t < nU + nV; t += nth) {
-        if (t < nU) {
-            const int i = 1 + t / wU, j = 1 + t % wU;
-            const size_t c = at(d, i, j);
-            double xval = curU < 0 ? (Mixed ? 0.0 : u[c]) : (double)xu[curU][c];
-            if (Mixed) xval += u[c];
-            const double nvv = dclamp(xval, -maxVel, maxVel);
-            mu = dmax(mu, fabs(nvv - u[c]));
-            out.uStar[c] = nvv;
-        } else {
-            const int q = t - nU;
-            const int i = 1 + q / wV, j = 1 + q % wV;
-            const size_t c = at(d, i, j);
-            double xval = curV < 0 ? (Mixed ? 0.0 : v[c]) : (double)xv[curV][c];
-            if (Mixed) xval += v[c];
-            const double nvv = dclamp(xval, -maxVel, maxVel);
-            mv = dmax(mv, fabs(nvv - v[c]));
-            out.vStar[c] = nvv;
-        }
-    }
+    if (doU) mu = jacobi_scatter<TC, Mixed, true>(k, u, curU < 0 ? nullptr : (curU ? xU1 : xU0), out.uStar, maxVel, tid, nth);
+    if (doV) mv = jacobi_scatter<TC, Mixed, false>(k, v, curV < 0 ? nullptr : (curV ? xV1 : xV0), out.vStar, maxVel, tid, nth);
     mu = warp_max(mu);
     mv = warp_max(mv);
     if ((threadIdx.x & 31) == 0) {

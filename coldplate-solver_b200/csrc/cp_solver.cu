@@ -20,6 +20,7 @@
 #include <vector>
 
 #include "cp_kernels.cuh"
+#include "cp_mg.cuh"
 
 using namespace cp;
 
@@ -73,6 +74,13 @@ struct cp_ctx {
     int histCap = 0;
     double* dpWin = nullptr;
     int gJac = 0, gPcg = 0, gElem = 0, nbMass = 0;
+    // multigrid hierarchy (pressureSolverType 2 / 4)
+    bool useMg = false;
+    int mgL = 0, mgLg = 0, gMg = 0;
+    int mgNI[kMgMaxLevels] = {}, mgNJ[kMgMaxLevels] = {}, mgP[kMgMaxLevels] = {};
+    void* mgArr[kMgMaxLevels][7] = {};   // fE fN d dx x y b
+    void* mgDense = nullptr;
+    double mgOmega = 0.8;
     cudaGraphExec_t graph = nullptr;
     bool graphTried = false;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -116,9 +124,9 @@ cp_status validate(const cp_params* p) {
         if (!finite(x)) return fail(CP_ERR_NONFINITE, "non-finite parameter");
     if (p->maxIterations < 0 || p->maxPressureIter < 0 || p->maxMomentumIter < 0)
         return fail(CP_ERR_BAD_PARAM, "iteration limits must be >= 0");
-    if (p->pressureSolverType != 1 && p->pressureSolverType != 4)
+    if (p->pressureSolverType != 1 && p->pressureSolverType != 2 && p->pressureSolverType != 4)
         return fail(CP_ERR_UNSUPPORTED,
-                    "pressureSolverType %d not available: types 1 (PCG) and 4 (GPU) run the native PCG",
+                    "pressureSolverType %d not available: 1 (Jacobi-PCG) and 2 / 4 (multigrid-PCG) run natively",
                     p->pressureSolverType);
     if (p->momentumSolverType != 1)
         return fail(CP_ERR_UNSUPPORTED, "momentumSolverType %d not available: only 1 (implicit Jacobi)",
@@ -264,6 +272,92 @@ PcgBufs<TV> pcg_bufs(cp_ctx* c) {
     return b;
 }
 
+template <typename TV>
+MgHier<TV> mg_hier(cp_ctx* c) {
+    MgHier<TV> H;
+    memset(&H, 0, sizeof(H));
+    H.L = c->mgL;
+    H.Lg = c->mgLg;
+    H.omega = c->mgOmega;
+    H.dense = (TV*)c->mgDense;
+    for (int l = 0; l < c->mgL; ++l) {
+        MgLevel<TV>& v = H.lv[l];
+        v.nI = c->mgNI[l]; v.nJ = c->mgNJ[l]; v.P = c->mgP[l];
+        TV** a = reinterpret_cast<TV**>(c->mgArr[l]);
+        v.fE = a[0]; v.fN = a[1]; v.d = a[2]; v.dx = a[3]; v.x = a[4]; v.y = a[5]; v.b = a[6];
+    }
+    return H;
+}
+
+constexpr int kMgThreads = 512;
+constexpr size_t kMgDynSmem = sizeof(double) * (size_t)(kMgDense * 2 * kMgDense + kMgDense);
+
+// Level sizes: halve (rounding up) until at most kMgDense unknowns; levels
+// above kMgCtaCells unknowns (and always level 0) run grid-wide.
+cp_status mg_build(cp_ctx* c) {
+    int nI = c->d.M - 1, nJ = c->d.N - 2;
+    int L = 0;
+    for (;;) {
+        if (L >= kMgMaxLevels) return fail(CP_ERR_BAD_PARAM, "multigrid hierarchy too deep");
+        c->mgNI[L] = nI; c->mgNJ[L] = nJ;
+        ++L;
+        if ((long long)nI * nJ <= kMgDense && L >= 2) break;
+        nI = (nI + 1) / 2; nJ = (nJ + 1) / 2;
+    }
+    c->mgL = L;
+    int Lg = 1;
+    while (Lg < L && (long long)c->mgNI[Lg] * c->mgNJ[Lg] > kMgCtaCells) ++Lg;
+    c->mgLg = Lg;
+    // level 0 shares the field layout and the PCG face / diagonal arrays
+    c->mgP[0] = c->d.P;
+    c->mgArr[0][0] = c->pcg[0];
+    c->mgArr[0][1] = c->pcg[1];
+    c->mgArr[0][2] = c->pcg[2];
+    for (int q = 3; q < 7; ++q) {
+        cp_status s = dalloc_bytes(c, &c->mgArr[0][q], c->nElem * c->es);
+        if (s != CP_OK) return s;
+    }
+    for (int l = 1; l < L; ++l) {
+        c->mgP[l] = ((c->mgNJ[l] + 2 + 31) / 32) * 32;
+        const size_t ne = (size_t)(c->mgNI[l] + 2) * c->mgP[l];
+        for (int q = 0; q < 7; ++q) {
+            cp_status s = dalloc_bytes(c, &c->mgArr[l][q], ne * c->es);
+            if (s != CP_OK) return s;
+        }
+    }
+    cp_status s = dalloc_bytes(c, &c->mgDense, (size_t)kMgDense * kMgDense * c->es);
+    if (s != CP_OK) return s;
+    const char* om = getenv("CP_MG_OMEGA");
+    if (om) c->mgOmega = atof(om);
+    // one CTA per SM (the dense set-up needs kMgDynSmem of shared memory)
+    int nb = 0;
+    if (c->prm.precision == CP_PREC_MIXED) {
+        cudaFuncSetAttribute(k_pcg_mg<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMgDynSmem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_pcg_mg<float>, kMgThreads, kMgDynSmem);
+    } else {
+        cudaFuncSetAttribute(k_pcg_mg<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMgDynSmem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_pcg_mg<double>, kMgThreads, kMgDynSmem);
+    }
+    if (nb < 1) return fail(CP_ERR_CUDA, "multigrid PCG kernel does not fit on an SM");
+    c->gMg = c->numSMs;
+    return CP_OK;
+}
+
+template <typename Kern, typename... Args>
+cudaError_t launch_coop_cfg(Kern kern, int grid, int threads, size_t smem, cudaStream_t s, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(threads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kern, args...);
+}
+
 template <typename TC, bool Mixed>
 cp_status enqueue_momentum(cp_ctx* c, int doU, int doV, int applyBC, EvRec* rec = nullptr) {
     Fields f{c->u, c->v, c->p, c->alpha, c->gamma};
@@ -291,8 +385,14 @@ cp_status enqueue_pressure(cp_ctx* c, EvRec* rec = nullptr) {
     CK(cudaGetLastError());
     CK(cudaMemsetAsync(c->barP, 0, sizeof(unsigned), c->stream));
     REC_BEGIN(rec, CP_K_PCG);
-    CK(launch_coop(k_pcg<TV>, c->gPcg, c->stream, c->k, c->st, (const double*)c->dE, (const double*)c->dN, B,
-                   c->pStar, c->partP, c->barP));
+    if (c->useMg) {
+        MgHier<TV> H = mg_hier<TV>(c);
+        CK(launch_coop_cfg(k_pcg_mg<TV>, c->gMg, kMgThreads, kMgDynSmem, c->stream, c->k, c->st,
+                           (const double*)c->dE, (const double*)c->dN, B, H, c->pStar, c->partP, c->barP));
+    } else {
+        CK(launch_coop(k_pcg<TV>, c->gPcg, c->stream, c->k, c->st, (const double*)c->dE, (const double*)c->dN, B,
+                       c->pStar, c->partP, c->barP));
+    }
     REC_END(rec);
     return CP_OK;
 }
@@ -580,15 +680,17 @@ cp_status cp_create(const cp_params* prm, cp_ctx** out) {
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nbP, k_pcg<double>, kThreads, 0);
     }
     if (nbJ < 1 || nbP < 1) return bail(fail(CP_ERR_CUDA, "cooperative kernels do not fit on an SM"));
-    c->gJac = c->numSMs * std::min(nbJ, 4);
+    c->gJac = c->numSMs * std::min(nbJ, 2);
     c->gPcg = c->numSMs * std::min(nbP, 4);
     c->gElem = c->numSMs * 4;
     c->nbMass = c->numSMs * 4;
     if (c->gJac > kMaxBlocks || c->gPcg > kMaxBlocks || c->nbMass > kMaxBlocks)
         return bail(fail(CP_ERR_CUDA, "too many SMs for the partial-sum buffers"));
+    c->useMg = (prm->pressureSolverType == 2 || prm->pressureSolverType == 4);
+    if (c->useMg && (s = mg_build(c)) != CP_OK) return bail(s);
     if ((s = dalloc(c, &c->partJ, (size_t)4 * c->gJac)) != CP_OK) return bail(s);
     if ((s = dalloc(c, &c->partM, (size_t)4 * c->nbMass)) != CP_OK) return bail(s);
-    if ((s = dalloc(c, &c->partP, (size_t)3 * c->gPcg)) != CP_OK) return bail(s);
+    if ((s = dalloc(c, &c->partP, (size_t)3 * std::max(c->gPcg, c->gMg))) != CP_OK) return bail(s);
     if ((s = dalloc(c, &c->barJ, 1)) != CP_OK) return bail(s);
     if ((s = dalloc(c, &c->barP, 1)) != CP_OK) return bail(s);
     if ((s = dalloc(c, &c->st, 1)) != CP_OK) return bail(s);

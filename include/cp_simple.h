@@ -87,8 +87,11 @@ typedef struct cp_params {
     double dpSlopeMaxDelta;
     /* OpenMP threads of the CPU code (SIMPLE.h:111); ignored */
     int numThreads;
-    /* pressure solver (SIMPLE.h:145-156): types 1 (PCG) and 4 (the GPU type)
-     * run the native matrix-free PCG; 0, 2, 3 are CP_ERR_UNSUPPORTED */
+    /* pressure solver (SIMPLE.h:145-156): type 1 runs the reference's
+     * Jacobi-preconditioned CG (pressure_solver.cpp:121-184); types 2 and 4
+     * (AMGCL AMG-CG in the reference; 4 is its default) run CG preconditioned
+     * by an aggregation-multigrid V-cycle; 0 (SOR) and 3 (LDLT) are
+     * CP_ERR_UNSUPPORTED */
     int pressureSolverType;
     int parallelizeDirectSolver;
     int maxPressureIter;

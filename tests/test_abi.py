@@ -91,6 +91,7 @@ def test_bad_parameters_are_rejected_before_any_device_work(built_lib):
     from coldplate_b200 import CpError, Simple, cases
     c = cases.straight_channel(8, 16)
     for over, code in ((dict(pressureSolverType=0), 2), (dict(pressureSolverType=3), 2),
+                       (dict(pressureSolverType=5), 2),
                        (dict(momentumSolverType=0), 2), (dict(enablePseudoTimeStepping=1), 2),
                        (dict(enableResidualViscosity=1), 2), (dict(hx=-1.0), 1), (dict(Nx=2), 1),
                        (dict(uvAlpha=float("nan")), 1), (dict(precision=7), 1)):
