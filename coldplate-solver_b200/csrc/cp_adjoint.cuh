@@ -1,0 +1,508 @@
+// Discrete adjoint of the pressure drop with respect to the density field.
+//
+// The reference has no flow adjoint (its only adjoint is the 2-D conduction
+// toy in AdjointMethod/thermal_adjoint.py); this is new.  It differentiates
+// the converged state of the SIMPLE discretisation exactly:
+//
+//   R(X; gamma) = 0,   X = (u on U unknowns, v on V unknowns, p on the
+//                          pressure unknowns [1,M-1] x [1,N-2])
+//
+// R_u: the U-momentum balance of momentum_solver.cpp:197-314 at u* = u with
+//      the relaxation cancelled, written in flux form
+//        De(2uP-uE-uW) + Dn(1+hN)(uP-uN) + Dn(1+hS)(uP-uS)
+//        + Fe phi_e - Fw phi_w + Fn phi_n - Fs phi_s + (sink + alpha vol) uP
+//        - hy (pP - pE)
+//      where F are the clamped face-average mass fluxes and phi the SOU face
+//      values of convection.cpp:53-186 (FOU where the SOU stencil is missing
+//      or convectionScheme = 0); the same for R_v;
+// R_c: the mass imbalance massW - massE + massS - massN of the pressure
+//      unknowns (pressure_solver.cpp:733-742).
+// Boundary values enter through the BCs of boundaries.cpp:50-146: the
+// outlet copies u(i,N-1) = u(i,N-2) and v(i,N) = v(i,N-1) map to unknowns,
+// walls, inlet and p(:,N-1) = 0 are constants.
+//
+// J = full-system total-pressure drop (SIMPLE.cpp:432): inlet patch
+// mass-flux-weighted total pressure minus the outlet patch's
+// (postprocessing.cpp:245-327).
+//
+// Adjoint: J_X^T lambda = dJ/dX, solved by defect correction
+//   lambda += P^{-1} (dJ/dX - J_X^T lambda)
+// with the exact transposed Jacobian product (every Newton term of the
+// upwind switches, SOU branches and face-velocity clamps) and a transposed
+// SIMPLE preconditioner P: Jacobi sweeps on the transposed Picard momentum
+// matrix, then a pressure-like correction whose operator
+// G^T diag(aP0)^-1 D^T equals the forward pressure-correction matrix, so the
+// same (multigrid) PCG kernel solves it.
+// Gradient: dJ/dgamma = -lambda^T dR/dgamma, which is local: gamma enters R
+// only through alpha_face = (alpha(cL) + alpha(cR)) / 2 with
+// alpha(g) = alpha_max (1 - g) / (1 + q g + 1e-10) (SIMPLE.cpp:770);
+// thresholds on gamma (inlet, half-cell and sampling masks) are piecewise
+// constant and contribute nothing.
+#pragma once
+
+#include "cp_kernels.cuh"
+
+namespace cp {
+
+struct AdjVecs {
+    double *lu, *lv, *lc;      // lambda on U / V / continuity rows
+    double *yu, *yv, *yp;      // J^T lambda on U / V / p unknowns
+    double *gu, *gv, *gp;      // dJ/dX
+    double *du, *dv;           // momentum corrections (Jacobi iterates, ping-pong with eu, ev)
+    double *eu, *ev;
+};
+
+// atomic add of a contribution to an unknown; `ok` is false for constants
+__device__ __forceinline__ void adj_add(double* y, size_t c, double v, bool ok) {
+    if (ok && v != 0.0) atomicAdd(y + c, v);
+}
+
+// Face value phi and its derivatives for one face, given the upwind side.
+// up/dn: the FOU value (upwind cell) and the SOU second point.
+struct Phi {
+    double val;
+    double dUp, dUpUp, dDn;   // d phi / d(upwind), d/d(second upwind), d/d(downwind)
+};
+
+// phi for F >= 0 (flow from "lo" to "hi"): FOU lo, SOU 1.5 lo - 0.5 lolo;
+// for F < 0: FOU hi, SOU 1.5 hi - 0.5 hihi.  Returns weights on (lo, lolo,
+// hi, hihi).
+struct FaceW {
+    double lo, lolo, hi, hihi, val;
+};
+
+__device__ __forceinline__ FaceW face_phi(double F, double lo, double lolo, double hi, double hihi, bool souLo,
+                                          bool souHi) {
+    FaceW w{0, 0, 0, 0, 0};
+    if (F >= 0.0) {
+        if (souLo) { w.lo = 1.5; w.lolo = -0.5; } else { w.lo = 1.0; }
+    } else {
+        if (souHi) { w.hi = 1.5; w.hihi = -0.5; } else { w.hi = 1.0; }
+    }
+    w.val = w.lo * lo + w.lolo * lolo + w.hi * hi + w.hihi * hihi;
+    return w;
+}
+
+// clamp derivative: 1 inside [-maxVel, maxVel], 0 where the clamp acts
+__device__ __forceinline__ double clampd(double x, double m) { return (x < -m || m < x) ? 0.0 : 1.0; }
+
+struct AdjCtx {
+    KParams k;
+    const double *u, *v, *p, *alpha, *gamma;
+    double maxVel;
+};
+
+// ---------------------------------------------------------------- J^T lambda
+// U row (i, j): accumulate lambda * dR_u/dX into y.  Returns R_u (for tests).
+__device__ double adj_row_u(const AdjCtx& a, int i, int j, double lam, AdjVecs V, bool scatter) {
+    const KParams& k = a.k;
+    const Dims d = k.d;
+    const int M = d.M, N = d.N;
+    const double* u = a.u;
+    const double* v = a.v;
+    const double hx = k.hx, hy = k.hy, vol = hx * hy;
+    const double cs = k.convScale, cE = cs * k.rho * hy, cN = cs * k.rho * hx;
+    const double De = k.eta * (hy / hx), Dn = k.eta * (hx / hy);
+    // unknown map: U unknowns i in [1,M-1], j in [1,N-2]; u(i,N-1) -> u(i,N-2)
+    auto U = [&](int ii, int jj, size_t& c) -> bool {
+        if (ii < 1 || ii > M - 1 || jj < 1) return false;
+        if (jj == N - 1) jj = N - 2;
+        if (jj > N - 2) return false;
+        c = at(d, ii, jj);
+        return true;
+    };
+    auto Vk = [&](int ii, int jj, size_t& c) -> bool {  // V unknowns i in [1,M-2], j in [1,N-1]
+        if (ii < 1 || ii > M - 2 || jj < 1) return false;
+        if (jj == N) jj = N - 1;
+        if (jj > N - 1) return false;
+        c = at(d, ii, jj);
+        return true;
+    };
+    auto uv = [&](int ii, int jj) -> double { return u[at(d, ii, jj)]; };
+    auto vv = [&](int ii, int jj) -> double { return v[at(d, ii, jj)]; };
+    const double uP = uv(i, j), uE = uv(i, j + 1), uW = uv(i, j - 1), uN = uv(i + 1, j), uS = uv(i - 1, j);
+    const double uEE = (j + 2 < N) ? uv(i, j + 2) : 0.0, uWW = (j >= 2) ? uv(i, j - 2) : 0.0;
+    const double uNN = (i + 2 <= M) ? uv(i + 2, j) : 0.0, uSS = (i >= 2) ? uv(i - 2, j) : 0.0;
+    const double mv = a.maxVel;
+    const double xe = 0.5 * (uP + uE), xw = 0.5 * (uW + uP);
+    const double xn = 0.5 * (vv(i, j) + vv(i, j + 1)), xs = 0.5 * (vv(i - 1, j) + vv(i - 1, j + 1));
+    const double Fe = cE * dclamp(xe, -mv, mv), Fw = cE * dclamp(xw, -mv, mv);
+    const double Fn = cN * dclamp(xn, -mv, mv), Fs = cN * dclamp(xs, -mv, mv);
+    const double gE = 0.5 * cE * clampd(xe, mv), gW = 0.5 * cE * clampd(xw, mv);
+    const double gN = 0.5 * cN * clampd(xn, mv), gS = 0.5 * cN * clampd(xs, mv);
+    const bool sou = k.sou;
+    // faces: east (lo = P, hi = E), west (lo = W, hi = P), north (lo = P, hi = N), south (lo = S, hi = P)
+    const FaceW pe = face_phi(Fe, uP, uW, uE, uEE, sou && j >= 2, sou && j + 2 < N);
+    const FaceW pw = face_phi(Fw, uW, uWW, uP, uE, sou && j >= 2, sou && j + 1 < N);
+    const FaceW pn = face_phi(Fn, uP, uS, uN, uNN, sou && i >= 1, sou && i + 2 <= M);
+    const FaceW ps = face_phi(Fs, uS, uSS, uP, uN, sou && i >= 2, sou && i + 1 <= M);
+    // half-cell wall flags (boundaries.cpp:148-171), as in the assembly
+    const double gF = 0.5 * (a.gamma[at(d, i - 1, j - 1)] + a.gamma[at(d, i - 1, j)]);
+    const double vt = 1e-8;
+    const bool hS = gF >= 0.999 && i == 1 && fabs(uv(0, j)) <= vt && fabs(vv(0, j)) <= vt && fabs(vv(0, j + 1)) <= vt;
+    const bool hN = gF >= 0.999 && i == M - 1 && fabs(uv(M, j)) <= vt && fabs(vv(M - 1, j)) <= vt &&
+                    fabs(vv(M - 1, j + 1)) <= vt;
+    const double DnN = Dn * (hN ? 2.0 : 1.0), DnS = Dn * (hS ? 2.0 : 1.0);
+    const double alphaF = 0.5 * (a.alpha[at(d, i - 1, j - 1)] + a.alpha[at(d, i - 1, j)]);
+    const double Kd = k.sinkDiag + alphaF * vol;
+    const double pP = a.p[at(d, i, j)], pE = a.p[at(d, i, j + 1)];
+    const double R = De * (2 * uP - uE - uW) + DnN * (uP - uN) + DnS * (uP - uS) + Fe * pe.val - Fw * pw.val +
+                     Fn * pn.val - Fs * ps.val + Kd * uP - hy * (pP - pE);
+    if (!scatter) return R;
+    // d/du: diffusion + flux derivative + face-value derivative
+    double dP = 2 * De + DnN + DnS + Kd + gE * pe.val - gW * pw.val + Fe * pe.lo - Fw * pw.hi + Fn * pn.lo - Fs * ps.hi;
+    double dE_ = -De + gE * pe.val + Fe * pe.hi - Fw * pw.hihi;
+    double dW_ = -De + Fe * pe.lolo - gW * pw.val - Fw * pw.lo;
+    double dEE = Fe * pe.hihi;
+    double dWW = -Fw * pw.lolo;
+    double dN_ = -DnN + Fn * pn.hi - Fs * ps.hihi;
+    double dNN = Fn * pn.hihi;
+    double dS_ = -DnS + Fn * pn.lolo - Fs * ps.lo;
+    double dSS = -Fs * ps.lolo;
+    size_t c;
+    if (U(i, j, c)) adj_add(V.yu, c, lam * dP, true);
+    if (U(i, j + 1, c)) adj_add(V.yu, c, lam * dE_, true);
+    if (U(i, j - 1, c)) adj_add(V.yu, c, lam * dW_, true);
+    if (j + 2 < N && U(i, j + 2, c)) adj_add(V.yu, c, lam * dEE, true);
+    if (j >= 2 && U(i, j - 2, c)) adj_add(V.yu, c, lam * dWW, true);
+    if (U(i + 1, j, c)) adj_add(V.yu, c, lam * dN_, true);
+    if (i + 2 <= M && U(i + 2, j, c)) adj_add(V.yu, c, lam * dNN, true);
+    if (U(i - 1, j, c)) adj_add(V.yu, c, lam * dS_, true);
+    if (i >= 2 && U(i - 2, j, c)) adj_add(V.yu, c, lam * dSS, true);
+    // d/dv through Fn, Fs
+    if (Vk(i, j, c)) adj_add(V.yv, c, lam * gN * pn.val, true);
+    if (Vk(i, j + 1, c)) adj_add(V.yv, c, lam * gN * pn.val, true);
+    if (Vk(i - 1, j, c)) adj_add(V.yv, c, -lam * gS * ps.val, true);
+    if (Vk(i - 1, j + 1, c)) adj_add(V.yv, c, -lam * gS * ps.val, true);
+    // d/dp: pP always an unknown here; pE unless j + 1 == N - 1 (p(:,N-1) = 0)
+    adj_add(V.yp, at(d, i, j), -lam * hy, true);
+    if (j + 1 <= N - 2) adj_add(V.yp, at(d, i, j + 1), lam * hy, true);
+    return R;
+}
+
+// V row (i, j)
+__device__ double adj_row_v(const AdjCtx& a, int i, int j, double lam, AdjVecs V, bool scatter) {
+    const KParams& k = a.k;
+    const Dims d = k.d;
+    const int M = d.M, N = d.N;
+    const double* u = a.u;
+    const double* v = a.v;
+    const double hx = k.hx, hy = k.hy, vol = hx * hy;
+    const double cs = k.convScale, cE = cs * k.rho * hy, cN = cs * k.rho * hx;
+    const double De = k.eta * (hy / hx), Dn = k.eta * (hx / hy);
+    auto U = [&](int ii, int jj, size_t& c) -> bool {
+        if (ii < 1 || ii > M - 1 || jj < 1) return false;
+        if (jj == N - 1) jj = N - 2;
+        if (jj > N - 2) return false;
+        c = at(d, ii, jj);
+        return true;
+    };
+    auto Vk = [&](int ii, int jj, size_t& c) -> bool {
+        if (ii < 1 || ii > M - 2 || jj < 1) return false;
+        if (jj == N) jj = N - 1;
+        if (jj > N - 1) return false;
+        c = at(d, ii, jj);
+        return true;
+    };
+    auto uv = [&](int ii, int jj) -> double { return u[at(d, ii, jj)]; };
+    auto vv = [&](int ii, int jj) -> double { return v[at(d, ii, jj)]; };
+    const double vP = vv(i, j), vE = vv(i, j + 1), vW = vv(i, j - 1), vN = vv(i + 1, j), vS = vv(i - 1, j);
+    const double vEE = (j + 2 <= N) ? vv(i, j + 2) : 0.0, vWW = (j >= 2) ? vv(i, j - 2) : 0.0;
+    const double vNN = (i + 2 < M) ? vv(i + 2, j) : 0.0, vSS = (i >= 2) ? vv(i - 2, j) : 0.0;
+    const double mv = a.maxVel;
+    const double xe = 0.5 * (uv(i, j) + uv(i + 1, j)), xw = 0.5 * (uv(i, j - 1) + uv(i + 1, j - 1));
+    const double xn = 0.5 * (vP + vN), xs = 0.5 * (vS + vP);
+    const double Fe = cE * dclamp(xe, -mv, mv), Fw = cE * dclamp(xw, -mv, mv);
+    const double Fn = cN * dclamp(xn, -mv, mv), Fs = cN * dclamp(xs, -mv, mv);
+    const double gE = 0.5 * cE * clampd(xe, mv), gW = 0.5 * cE * clampd(xw, mv);
+    const double gN = 0.5 * cN * clampd(xn, mv), gS = 0.5 * cN * clampd(xs, mv);
+    const bool sou = k.sou;
+    const FaceW pe = face_phi(Fe, vP, vW, vE, vEE, sou && j >= 2, sou && j + 2 <= N);
+    const FaceW pw = face_phi(Fw, vW, vWW, vP, vE, sou && j >= 2, sou && j + 1 <= N);
+    const FaceW pn = face_phi(Fn, vP, vS, vN, vNN, sou && i >= 1, sou && i + 2 < M);
+    const FaceW ps = face_phi(Fs, vS, vSS, vP, vN, sou && i >= 2, sou && i + 1 < M);
+    const double gF = 0.5 * (a.gamma[at(d, i - 1, j - 1)] + a.gamma[at(d, i, j - 1)]);
+    const double vt = 1e-8;
+    const bool hW = gF >= 0.999 && j == 1 && !(fabs(k.targetVel) > vt) && fabs(vv(i, 0)) <= vt &&
+                    fabs(uv(i, 0)) <= vt && fabs(uv(i + 1, 0)) <= vt;
+    const bool hE = gF >= 0.999 && j == N - 1 && !(fabs(a.p[at(d, i, N)]) <= 1e-8) && fabs(vv(i, N)) <= vt &&
+                    fabs(uv(i, N - 1)) <= vt && fabs(uv(i + 1, N - 1)) <= vt;
+    const double DeW = De * (hW ? 2.0 : 1.0), DeE = De * (hE ? 2.0 : 1.0);
+    const double alphaF = 0.5 * (a.alpha[at(d, i - 1, j - 1)] + a.alpha[at(d, i, j - 1)]);
+    const double Kd = k.sinkDiag + alphaF * vol;
+    const double pP = a.p[at(d, i, j)], pN = a.p[at(d, i + 1, j)];
+    const double R = DeW * (vP - vW) + DeE * (vP - vE) + Dn * (2 * vP - vN - vS) + Fe * pe.val - Fw * pw.val +
+                     Fn * pn.val - Fs * ps.val + Kd * vP - hx * (pP - pN);
+    if (!scatter) return R;
+    double dP = DeW + DeE + 2 * Dn + Kd + Fe * pe.lo - Fw * pw.hi + gN * pn.val - gS * ps.val + Fn * pn.lo - Fs * ps.hi;
+    double dE_ = -DeE + Fe * pe.hi - Fw * pw.hihi;
+    double dW_ = -DeW + Fe * pe.lolo - Fw * pw.lo;
+    double dEE = Fe * pe.hihi;
+    double dWW = -Fw * pw.lolo;
+    double dN_ = -Dn + gN * pn.val + Fn * pn.hi - Fs * ps.hihi;
+    double dNN = Fn * pn.hihi;
+    double dS_ = -Dn + Fn * pn.lolo - gS * ps.val - Fs * ps.lo;
+    double dSS = -Fs * ps.lolo;
+    size_t c;
+    if (Vk(i, j, c)) adj_add(V.yv, c, lam * dP, true);
+    if (Vk(i, j + 1, c)) adj_add(V.yv, c, lam * dE_, true);
+    if (Vk(i, j - 1, c)) adj_add(V.yv, c, lam * dW_, true);
+    if (j + 2 <= N && Vk(i, j + 2, c)) adj_add(V.yv, c, lam * dEE, true);
+    if (j >= 2 && Vk(i, j - 2, c)) adj_add(V.yv, c, lam * dWW, true);
+    if (Vk(i + 1, j, c)) adj_add(V.yv, c, lam * dN_, true);
+    if (i + 2 < M && Vk(i + 2, j, c)) adj_add(V.yv, c, lam * dNN, true);
+    if (Vk(i - 1, j, c)) adj_add(V.yv, c, lam * dS_, true);
+    if (i >= 2 && Vk(i - 2, j, c)) adj_add(V.yv, c, lam * dSS, true);
+    // d/du through Fe (u(i,j), u(i+1,j)) and Fw (u(i,j-1), u(i+1,j-1))
+    if (U(i, j, c)) adj_add(V.yu, c, lam * gE * pe.val, true);
+    if (U(i + 1, j, c)) adj_add(V.yu, c, lam * gE * pe.val, true);
+    if (U(i, j - 1, c)) adj_add(V.yu, c, -lam * gW * pw.val, true);
+    if (U(i + 1, j - 1, c)) adj_add(V.yu, c, -lam * gW * pw.val, true);
+    // d/dp: p(i,j) and p(i+1,j) are unknowns when j <= N-2
+    if (j <= N - 2) {
+        adj_add(V.yp, at(d, i, j), -lam * hx, true);
+        adj_add(V.yp, at(d, i + 1, j), lam * hx, true);
+    }
+    return R;
+}
+
+// continuity row (i, j): R_c = rho hy (u(i,j-1) - u(i,j)) + rho hx (v(i-1,j) - v(i,j))
+__device__ double adj_row_c(const AdjCtx& a, int i, int j, double lam, AdjVecs V, bool scatter) {
+    const KParams& k = a.k;
+    const Dims d = k.d;
+    const int M = d.M;
+    const double rh = k.rho * k.hy, rx = k.rho * k.hx;
+    const double R = rh * (a.u[at(d, i, j - 1)] - a.u[at(d, i, j)]) + rx * (a.v[at(d, i - 1, j)] - a.v[at(d, i, j)]);
+    if (!scatter) return R;
+    if (j - 1 >= 1) adj_add(V.yu, at(d, i, j - 1), lam * rh, true);
+    adj_add(V.yu, at(d, i, j), -lam * rh, true);
+    if (i - 1 >= 1) adj_add(V.yv, at(d, i - 1, j), lam * rx, true);
+    if (i <= M - 2) adj_add(V.yv, at(d, i, j), -lam * rx, true);
+    return R;
+}
+
+// y = J^T lambda (y zeroed by the caller); with resid != nullptr also the
+// residuals R(X) per row (U, V, C in the field layout).
+__global__ void k_adj_jt(AdjCtx a, AdjVecs V, double* rU, double* rV, double* rC) {
+    const Dims d = a.k.d;
+    const int M = d.M, N = d.N;
+    const int nU = (M - 1) * (N - 2), nV = (M - 2) * (N - 1), nC = (M - 1) * (N - 2);
+    const bool scatter = (rU == nullptr);
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nU + nV + nC; t += gridDim.x * blockDim.x) {
+        if (t < nU) {
+            const int i = 1 + t / (N - 2), j = 1 + t % (N - 2);
+            const double R = adj_row_u(a, i, j, scatter ? V.lu[at(d, i, j)] : 0.0, V, scatter);
+            if (!scatter) rU[at(d, i, j)] = R;
+        } else if (t < nU + nV) {
+            const int q = t - nU;
+            const int i = 1 + q / (N - 1), j = 1 + q % (N - 1);
+            const double R = adj_row_v(a, i, j, scatter ? V.lv[at(d, i, j)] : 0.0, V, scatter);
+            if (!scatter) rV[at(d, i, j)] = R;
+        } else {
+            const int q = t - nU - nV;
+            const int i = 1 + q / (N - 2), j = 1 + q % (N - 2);
+            const double R = adj_row_c(a, i, j, scatter ? V.lc[at(d, i, j)] : 0.0, V, scatter);
+            if (!scatter) rC[at(d, i, j)] = R;
+        }
+    }
+}
+
+// dJ/dX of the full-system pressure drop (one block).  Inlet patch: rows with
+// gamma(i-1, 0) pure fluid; static p(i,0) = p(i,1) (ghost copy of an
+// unknown), u(i,0) and v(.,0) are boundary constants.  Outlet patch: rows
+// with gamma(i-1, N-2) pure fluid; p(i,N) = 0, u(i,N-1) = u(i,N-2),
+// v(.,N) = v(.,N-1).  Also returns J (for checks).
+__global__ void __launch_bounds__(1024) k_adj_g(AdjCtx a, AdjVecs V, double* Jout) {
+    __shared__ double sm[32 * 5];
+    const KParams& k = a.k;
+    const Dims d = k.d;
+    const int M = d.M, N = d.N;
+    const double rho = k.rho, hy = k.hy;
+    // pass 1: sums of the inlet and outlet patches
+    double s[5] = {0, 0, 0, 0, 0};  // in: flux, tot*flux ; out: flux, tot*flux, area
+    for (int i = 1 + threadIdx.x; i < M; i += blockDim.x) {
+        if (a.gamma[at(d, i - 1, 0)] >= 1.0 - 1e-6) {
+            const double un = a.u[at(d, i, 0)];
+            const double vt = 0.5 * (a.v[at(d, i - 1, 0)] + a.v[at(d, i, 0)]);
+            const double fa = fabs(rho * un * hy);
+            const double tot = a.p[at(d, i, 0)] + 0.5 * rho * (un * un + vt * vt);
+            if (fa > 0.0) { s[0] += fa; s[1] += tot * fa; }
+        }
+        if (a.gamma[at(d, i - 1, N - 2)] >= 1.0 - 1e-6) {
+            const int vtI = i - 1, vbI = (i < M - 1) ? i : M - 1;
+            const double un = a.u[at(d, i, N - 1)];
+            const double vt = 0.5 * (a.v[at(d, vtI, N)] + a.v[at(d, vbI, N)]);
+            const double fa = fabs(rho * un * hy);
+            const double tot = a.p[at(d, i, N)] + 0.5 * rho * (un * un + vt * vt);
+            if (fa > 0.0) { s[2] += fa; s[3] += tot * fa; }
+            s[4] += hy;
+        }
+    }
+    block_sum<5>(s, sm);
+    const double inAvg = s[0] > 0.0 ? s[1] / s[0] : 0.0;
+    const double outAvg = s[2] > 0.0 ? s[3] / s[2] : 0.0;
+    if (threadIdx.x == 0 && Jout) *Jout = inAvg - outAvg;
+    // pass 2: derivatives
+    for (int i = 1 + threadIdx.x; i < M; i += blockDim.x) {
+        if (s[0] > 0.0 && a.gamma[at(d, i - 1, 0)] >= 1.0 - 1e-6) {
+            const double un = a.u[at(d, i, 0)];
+            const double fa = fabs(rho * un * hy);
+            // d inAvg / d p(i,1) (p(i,0) is the ghost copy of p(i,1))
+            if (fa > 0.0) V.gp[at(d, i, 1)] += fa / s[0];
+        }
+        if (s[2] > 0.0 && a.gamma[at(d, i - 1, N - 2)] >= 1.0 - 1e-6) {
+            const int vtI = i - 1, vbI = (i < M - 1) ? i : M - 1;
+            const double un = a.u[at(d, i, N - 1)];
+            const double vt = 0.5 * (a.v[at(d, vtI, N)] + a.v[at(d, vbI, N)]);
+            const double fa = fabs(rho * un * hy);
+            if (fa > 0.0) {
+                const double tot = a.p[at(d, i, N)] + 0.5 * rho * (un * un + vt * vt);
+                const double sg = un > 0.0 ? 1.0 : (un < 0.0 ? -1.0 : 0.0);
+                // d outAvg / d un and / d vt; J = in - out
+                const double dun = (rho * un * fa + (tot - outAvg) * rho * hy * sg) / s[2];
+                const double dvt = rho * vt * fa / s[2];
+                // un = u(i,N-1) = u(i,N-2) (outlet copy)
+                atomicAdd(V.gu + at(d, i, N - 2), -dun);
+                // vt = (v(i-1,N) + v(i,N)) / 2 = (v(i-1,N-1) + v(i,N-1)) / 2; walls are constants
+                if (vtI >= 1 && vtI <= M - 2) atomicAdd(V.gv + at(d, vtI, N - 1), -0.5 * dvt);
+                if (vbI >= 1 && vbI <= M - 2) atomicAdd(V.gv + at(d, vbI, N - 1), -0.5 * dvt);
+            }
+        }
+    }
+}
+
+// r = g - y on all unknowns; partial sums of r^2 and g^2 per block into part[b*2]
+__global__ void k_adj_defect(KParams k, AdjVecs V, double* ru, double* rv, double* rp, double* part) {
+    __shared__ double sm[64];
+    const Dims d = k.d;
+    const int M = d.M, N = d.N;
+    const int nU = (M - 1) * (N - 2), nV = (M - 2) * (N - 1), nP = (M - 1) * (N - 2);
+    double acc[2] = {0.0, 0.0};
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nU + nV + nP; t += gridDim.x * blockDim.x) {
+        if (t < nU) {
+            const size_t c = at(d, 1 + t / (N - 2), 1 + t % (N - 2));
+            const double r = V.gu[c] - V.yu[c];
+            ru[c] = r; acc[0] += r * r; acc[1] += V.gu[c] * V.gu[c];
+        } else if (t < nU + nV) {
+            const int q = t - nU;
+            const size_t c = at(d, 1 + q / (N - 1), 1 + q % (N - 1));
+            const double r = V.gv[c] - V.yv[c];
+            rv[c] = r; acc[0] += r * r; acc[1] += V.gv[c] * V.gv[c];
+        } else {
+            const int q = t - nU - nV;
+            const size_t c = at(d, 1 + q / (N - 2), 1 + q % (N - 2));
+            const double r = V.gp[c] - V.yp[c];
+            rp[c] = r; acc[0] += r * r; acc[1] += V.gp[c] * V.gp[c];
+        }
+    }
+    block_sum<2>(acc, sm);
+    if (threadIdx.x == 0) { part[2 * blockIdx.x] = acc[0]; part[2 * blockIdx.x + 1] = acc[1]; }
+}
+
+// One Jacobi sweep of the transposed, relaxed Picard momentum system for U
+// and V: (A_P^T x)(i,j) = aP x(i,j) - aW(i,j+1) x(i,j+1) - aE(i,j-1) x(i,j-1)
+// - aS(i+1,j) x(i+1,j) - aN(i-1,j) x(i-1,j) with the masked coefficients of
+// the converged assembly (aP = aP0 / uvAlpha).  first: x = 0.
+__global__ void k_adj_jacobi_t(KParams k, MomSys<double> Us, MomSys<double> Vs, const double* ru,
+                               const double* rv, const double* xu, const double* xv, double* yu, double* yv,
+                               int first) {
+    const Dims d = k.d;
+    const int M = d.M, N = d.N;
+    const int nU = (M - 1) * (N - 2), nV = (M - 2) * (N - 1);
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nU + nV; t += gridDim.x * blockDim.x) {
+        const bool isU = t < nU;
+        const int q = isU ? t : t - nU;
+        const int w = isU ? N - 2 : N - 1;
+        const int i = 1 + q / w, j = 1 + q % w;
+        const size_t c = at(d, i, j);
+        const MomSys<double>& S = isU ? Us : Vs;
+        const double* x = isU ? xu : xv;
+        const double* r = isU ? ru : rv;
+        double Ax = 0.0;
+        if (!first) {
+            Ax = S.aP[c] * x[c] - S.aW[c + 1] * x[c + 1] - S.aE[c - 1] * x[c - 1] - S.aS[c + d.P] * x[c + d.P] -
+                 S.aN[c - d.P] * x[c - d.P];
+        }
+        const double xn = (first ? 0.0 : x[c]) + (r[c] - Ax) / S.aP[c];
+        (isU ? yu : yv)[c] = xn;
+    }
+}
+
+// rhs of the pressure-like correction: G^T dm* - r_p, with
+// (G^T dm)(i,j) = hy (du(i,j-1) - du(i,j)) + hx (dv(i-1,j) - dv(i,j));
+// written into the PCG rhs (TV) on the pressure unknowns.
+template <typename TV>
+__global__ void k_adj_prhs(KParams k, const double* du, const double* dv, const double* rp, TV* rhs) {
+    const Dims d = k.d;
+    const int M = d.M, N = d.N, w = N - 2;
+    const int n = (M - 1) * w;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        const int i = 1 + t / w, j = 1 + t % w;
+        const size_t c = at(d, i, j);
+        const double uw = (j > 1) ? du[c - 1] : 0.0;
+        const double vs = (i > 1) ? dv[c - d.P] : 0.0;
+        const double vn = (i <= M - 2) ? dv[c] : 0.0;
+        rhs[c] = (TV)(k.hy * (uw - du[c]) + k.hx * (vs - vn) - rp[c]);
+    }
+}
+
+// corrections: dm = dm* - D_A^-1 D^T dc with (D_A^-1 D^T dc)_u(i,j) =
+// rho dE(i,j) (dc(i,j+1) - dc(i,j)) and for v rho dN(i,j) (dc(i+1,j) - dc(i,j))
+// (dc zero outside the pressure unknowns); lambda += dm, lambda_c += pAlpha dc
+__global__ void k_adj_update(KParams k, AdjVecs V, const double* du, const double* dv, const double* dc,
+                             const double* dE, const double* dN, double relaxC) {
+    const Dims d = k.d;
+    const int M = d.M, N = d.N;
+    const int nU = (M - 1) * (N - 2), nV = (M - 2) * (N - 1), nP = (M - 1) * (N - 2);
+    auto C = [&](int i, int j) -> double {
+        if (i < 1 || i > M - 1 || j < 1 || j > N - 2) return 0.0;
+        return dc[at(d, i, j)];
+    };
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nU + nV + nP; t += gridDim.x * blockDim.x) {
+        if (t < nU) {
+            const int i = 1 + t / (N - 2), j = 1 + t % (N - 2);
+            const size_t c = at(d, i, j);
+            V.lu[c] += du[c] - k.rho * dE[c] * (C(i, j + 1) - C(i, j));
+        } else if (t < nU + nV) {
+            const int q = t - nU;
+            const int i = 1 + q / (N - 1), j = 1 + q % (N - 1);
+            const size_t c = at(d, i, j);
+            V.lv[c] += dv[c] - k.rho * dN[c] * (C(i + 1, j) - C(i, j));
+        } else {
+            const int q = t - nU - nV;
+            const int i = 1 + q / (N - 2), j = 1 + q % (N - 2);
+            V.lc[at(d, i, j)] += relaxC * dc[at(d, i, j)];
+        }
+    }
+}
+
+// dJ/dgamma(cell a, b) = -sum over the faces the cell touches of
+// lambda_face * vol * vel_face * 0.5 * alpha'(gamma(a,b)); cells Ny x Nx.
+__global__ void k_adj_grad(AdjCtx a, AdjVecs V, double alphaMax, double q, double* grad) {
+    const KParams& k = a.k;
+    const Dims d = k.d;
+    const int M = d.M, N = d.N, Ny = M - 1, Nx = N - 1;
+    const double vol = k.hx * k.hy;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < Ny * Nx; t += gridDim.x * blockDim.x) {
+        const int ca = t / Nx, cb = t % Nx;
+        const double g = a.gamma[at(d, ca, cb)];
+        const double den = 1.0 + q * g + 1e-10;
+        const double dalpha = -alphaMax * (den + (1.0 - g) * q) / (den * den);
+        double s = 0.0;
+        // U faces (i, j) with i-1 = ca and j-1 = cb (left cell) or j = cb (right cell); j in [1, N-2]
+        const int iu = ca + 1;
+        if (iu >= 1 && iu <= M - 1) {
+            if (cb + 1 <= N - 2) s += V.lu[at(d, iu, cb + 1)] * a.u[at(d, iu, cb + 1)];
+            if (cb >= 1 && cb <= N - 2) s += V.lu[at(d, iu, cb)] * a.u[at(d, iu, cb)];
+        }
+        // V faces (i, j) with j-1 = cb and i-1 = ca (top cell) or i = ca (bottom cell); i in [1, M-2]
+        const int jv = cb + 1;
+        if (jv >= 1 && jv <= N - 1) {
+            if (ca + 1 <= M - 2) s += V.lv[at(d, ca + 1, jv)] * a.v[at(d, ca + 1, jv)];
+            if (ca >= 1 && ca <= M - 2) s += V.lv[at(d, ca, jv)] * a.v[at(d, ca, jv)];
+        }
+        grad[t] = -s * vol * 0.5 * dalpha;
+    }
+}
+
+}  // namespace cp
