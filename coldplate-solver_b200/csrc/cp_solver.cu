@@ -16,6 +16,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -919,3 +920,121 @@ cp_status cp_get_history(cp_ctx* c, double* rows, int max_rows, int* n_rows) {
 }
 
 }  // extern "C"
+
+// ======================================================================== no-allocation entry point
+// cp_pressure_noalloc: the Jacobi-PCG pressure-correction solve (k_mass +
+// k_pcg<double>, the kernels behind cp_pressure for pressureSolverType 1)
+// for callers that cannot allocate device memory.  All of its working
+// memory lives in one file-scope device array of fixed size, below; the
+// caller provides only the inputs and the output.
+namespace {
+
+// Largest pressure grid the array serves: (Ny + 2) * pitch elements per
+// working array, where pitch is the row pitch (in doubles) the caller uses.
+constexpr size_t kNoAllocCells = 131072;
+constexpr size_t kNoAllocArrays = 9;                  // fE fN d x r pa pb Ap rhs
+constexpr size_t kNoAllocHead = 256 + 256 + 8 * 4 * kMaxBlocks + 8 * 3 * kMaxBlocks;
+constexpr size_t kNoAllocBytes = kNoAllocHead + kNoAllocArrays * 8 * kNoAllocCells;
+
+// Every GPU that loads the library holds these bytes until the process exits.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+unsigned char* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+// device address of the array for the current device (looked up once per
+// device, with that device current)
+cp_status noalloc_scratch(unsigned char** out) {
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kNoAllocMaxDevices) return fail(CP_ERR_CUDA, "device ordinal %d out of range", dev);
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+        g_noalloc_ptr[dev] = static_cast<unsigned char*>(p);
+    }
+    *out = g_noalloc_ptr[dev];
+    return CP_OK;
+}
+
+// max |mass imbalance| of the k_mass partials into st->lastError
+__global__ void k_noalloc_massmax(const double* partM, int nb, Status* st) {
+    double m = 0.0;
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) m = dmax(m, partM[b * 4 + 3]);
+    m = warp_max(m);
+    __shared__ double sm[32];
+    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double r = 0.0;
+        for (int q = 0; q < (int)((blockDim.x + 31) >> 5); ++q) r = dmax(r, sm[q]);
+        st->lastError = r;
+    }
+}
+
+}  // namespace
+
+extern "C" cp_status cp_pressure_noalloc(const cp_params* p, const double* dE, const double* dN,
+                                         const double* uStar, const double* vStar, long pitch, double* pStar,
+                                         int* iters, double* residMass, void* stream) {
+    if (!p || !dE || !dN || !uStar || !vStar || !pStar) return fail(CP_ERR_BAD_PARAM, "NULL argument");
+    if (p->Ny < 2 || p->Nx < 3) return fail(CP_ERR_BAD_PARAM, "grid %d x %d too small", p->Ny, p->Nx);
+    if (p->pressureSolverType != 1)
+        return fail(CP_ERR_UNSUPPORTED, "cp_pressure_noalloc runs the Jacobi-PCG (pressureSolverType 1) only");
+    if (!(p->rho > 0.0) || !(p->hx > 0.0) || !(p->hy > 0.0) || !std::isfinite(p->pTol) || p->maxPressureIter < 0)
+        return fail(CP_ERR_BAD_PARAM, "rho, hx, hy must be > 0, pTol finite, maxPressureIter >= 0");
+    const int M = p->Ny + 1, N = p->Nx + 1;
+    if (pitch < N + 1) return fail(CP_ERR_BAD_PARAM, "pitch %ld < Nx + 2 = %d", pitch, N + 1);
+    const size_t cells = (size_t)(M + 2) * (size_t)pitch;
+    if (cells > kNoAllocCells)
+        return fail(CP_ERR_BAD_PARAM,
+                    "grid too large for cp_pressure_noalloc: (Ny + 3) * pitch = %zu exceeds %zu; use cp_pressure",
+                    cells, kNoAllocCells);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    unsigned char* base = nullptr;
+    cp_status st = noalloc_scratch(&base);
+    if (st != CP_OK) return st;
+    int dev = 0, sms = 0, nbP = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nbP, k_pcg<double>, kThreads, 0));
+    if (nbP < 1) return fail(CP_ERR_CUDA, "PCG kernel does not fit on an SM");
+    const int gPcg = sms * std::min(nbP, 4), nbMass = sms * 4;
+    if (gPcg > kMaxBlocks || nbMass > kMaxBlocks) return fail(CP_ERR_CUDA, "too many SMs");
+    // carve the array: status, barrier counter, partial sums, nine working arrays
+    Status* dst = reinterpret_cast<Status*>(base);
+    unsigned* bar = reinterpret_cast<unsigned*>(base + 256);
+    double* partM = reinterpret_cast<double*>(base + 512);
+    double* partP = partM + 4 * kMaxBlocks;
+    double* arr = reinterpret_cast<double*>(base + kNoAllocHead);
+    PcgBufs<double> B;
+    double* a[kNoAllocArrays];
+    for (size_t q = 0; q < kNoAllocArrays; ++q) a[q] = arr + q * cells;
+    B.fE = a[0]; B.fN = a[1]; B.d = a[2]; B.x = a[3]; B.r = a[4]; B.pa = a[5]; B.pb = a[6]; B.Ap = a[7];
+    B.rhs = a[8];
+    // the array keeps the previous call's contents: clear everything this
+    // call relies on being zero (status, counter, partials, the frames of
+    // the working arrays), and the output like the reference's pStar.setZero()
+    CK(cudaMemsetAsync(base, 0, kNoAllocHead + kNoAllocArrays * 8 * cells, s));
+    CK(cudaMemset2DAsync(pStar, (size_t)pitch * 8, 0, (size_t)(N + 1) * 8, (size_t)(M + 1), s));
+    KParams k{};
+    k.d.M = M; k.d.N = N; k.d.P = (int)pitch;
+    k.hx = p->hx; k.hy = p->hy; k.rho = p->rho;
+    k.pTol = p->pTol; k.maxP = p->maxPressureIter;
+    k.nU = (M - 1) * (N - 2); k.nV = (M - 2) * (N - 1); k.nP = (M - 1) * (N - 2);
+    // the RMS columns of k_mass are not reported here; u*/v* stand in for u/v
+    k_mass<double><<<nbMass, kThreads, 0, s>>>(k, dst, uStar, vStar, uStar, vStar, B.rhs, partM);
+    CK(cudaGetLastError());
+    CK(launch_coop(k_pcg<double>, gPcg, s, k, dst, dE, dN, B, pStar, partP, bar));
+    k_noalloc_massmax<<<1, 256, 0, s>>>(partM, nbMass, dst);
+    CK(cudaGetLastError());
+    Status hs;
+    CK(cudaMemcpyAsync(&hs, dst, sizeof(Status), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (hs.err != 0) return fail((cp_status)hs.err, "device reported %s", cp_status_string((cp_status)hs.err));
+    if (iters) *iters = hs.itersP;
+    if (residMass) *residMass = hs.lastError;
+    return CP_OK;
+}

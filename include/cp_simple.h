@@ -214,6 +214,33 @@ cp_status cp_momentum_u(cp_ctx* ctx, double* resid, int* iters);
 cp_status cp_momentum_v(cp_ctx* ctx, double* resid, int* iters);
 cp_status cp_pressure(cp_ctx* ctx, int* iters, double* residMass);
 
+/* Pressure-correction solve that allocates no device memory.  No
+ * counterpart in the reference: it exists for callers that cannot call
+ * cudaMalloc, e.g. a plugin inside a host application that has already
+ * committed the whole device-memory budget to its own pool, or a
+ * latency-bound control loop that must not stall in the allocator.  It runs
+ * the same Jacobi-PCG as cp_pressure with pressureSolverType 1 and returns
+ * the same p', iteration count and max mass imbalance.
+ *
+ * Inputs and output are device pointers the caller owns, row-major doubles
+ * with one common row pitch `pitch` (elements, >= Nx + 2) in the reference
+ * shapes: dE and uStar (Ny+2) x (Nx+1), dN and vStar (Ny+1) x (Nx+2), pStar
+ * (Ny+2) x (Nx+2).  Only p->Ny, Nx, hx, hy, rho, pTol, maxPressureIter and
+ * pressureSolverType (must be 1) are read.  `stream` is a cudaStream_t (or
+ * NULL); the call returns after the solve has finished on it.
+ *
+ * Working memory: one fixed device array inside the library, which every GPU
+ * that loads the library holds until the process exits.  It bounds the grid:
+ * (Ny + 3) * pitch must not exceed 131072 (e.g. Ny 254 with Nx up to 509 at
+ * pitch 512); larger grids return CP_ERR_BAD_PARAM.  The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress) with
+ * that device current; make that first call before capturing any stream.
+ * All calls share the array, so calls that overlap on the GPU (other streams
+ * or other threads) race and must be serialised by the caller. */
+cp_status cp_pressure_noalloc(const cp_params* p, const double* dE, const double* dN, const double* uStar,
+                              const double* vStar, long pitch, double* pStar, int* iters, double* residMass,
+                              void* stream);
+
 /* Per-iteration history rows (cp_iter_report layout without device_ms, as
  * doubles: see cp_history_columns()).  Returns the number of rows copied. */
 int cp_history_columns(void);
