@@ -77,6 +77,11 @@ class CpKernelTiming(ctypes.Structure):
                 ("iterations", ctypes.c_int)]
 
 
+class CpAdjointReport(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_int), ("converged", ctypes.c_int), ("residual", ctypes.c_double),
+                ("J", ctypes.c_double), ("device_ms", ctypes.c_double)]
+
+
 # history row columns (cp_device.cuh HistCol)
 HIST_COLS = ("iter", "error", "residU_RMS", "residV_RMS", "residMass_RMS", "residU_max", "residV_max",
              "residMass_max", "pIters", "coreTotal", "fullTotal", "coreStatic", "fullStatic",
@@ -105,6 +110,7 @@ SIGNATURES = {
     "cp_momentum_u": (_I, [_vp, _dp, _ip]),
     "cp_momentum_v": (_I, [_vp, _dp, _ip]),
     "cp_pressure": (_I, [_vp, _ip, _dp]),
+    "cp_adjoint_dp_dgamma": (_I, [_vp, _dp, _L, _L, _L, _L, _I, _D, ctypes.POINTER(CpAdjointReport)]),
     "cp_history_columns": (_I, []),
     "cp_get_history": (_I, [_vp, _dp, _I, _ip]),
     "cp_status_string": (ctypes.c_char_p, [_I]),

@@ -163,6 +163,18 @@ class Simple:
         rows = buf[: n.value]
         return {name: rows[:, k] for k, name in enumerate(nat.HIST_COLS)}
 
+    # -------------------------------------------------------------- adjoint
+    def adjoint_dp_dgamma(self, max_iter: int = 2000, tol: float = 1e-10) -> tuple[np.ndarray, dict]:
+        """dJ/dgamma (Ny x Nx) of the full-system total-pressure drop J at the
+        current state (converge the forward solve first), by the discrete
+        adjoint of the converged discretisation."""
+        Ny, Nx = self.M - 1, self.N - 1
+        g = np.empty((Ny, Nx), dtype=np.float64)
+        rep = nat.CpAdjointReport()
+        nat.check(self._lib.cp_adjoint_dp_dgamma(self._h, _dptr(g), Ny, Nx, Nx, 1, int(max_iter), float(tol),
+                                                   ctypes.byref(rep)))
+        return g, {name: getattr(rep, name) for name, _ in rep._fields_}
+
     # -------------------------------------------------------------- dispatch boundary
     def solveUMomentumImplicit(self) -> tuple[int, float]:
         r, it = ctypes.c_double(), ctypes.c_int()

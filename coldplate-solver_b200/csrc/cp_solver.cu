@@ -22,6 +22,7 @@
 
 #include "cp_kernels.cuh"
 #include "cp_mg.cuh"
+#include "cp_adjoint.cuh"
 
 using namespace cp;
 
@@ -82,6 +83,12 @@ struct cp_ctx {
     void* mgArr[kMgMaxLevels][7] = {};   // fE fN d dx x y b
     void* mgDense = nullptr;
     double mgOmega = 0.8;
+    // adjoint buffers (allocated on first use, double)
+    double* adj[20] = {};
+    void* adjMom[12] = {};
+    Status* adjSt = nullptr;
+    double* adjPart = nullptr;
+    unsigned* adjBar = nullptr;
     cudaGraphExec_t graph = nullptr;
     bool graphTried = false;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -920,6 +927,167 @@ cp_status cp_get_history(cp_ctx* c, double* rows, int max_rows, int* n_rows) {
 }
 
 }  // extern "C"
+
+// ======================================================================== adjoint
+namespace {
+
+cp_status adjoint_alloc(cp_ctx* c) {
+    if (c->adjSt) return CP_OK;
+    for (auto& a : c->adj) {
+        cp_status s = dalloc(c, &a, c->nElem);
+        if (s != CP_OK) return s;
+    }
+    for (auto& m : c->adjMom) {
+        cp_status s = dalloc_bytes(c, &m, c->nElem * sizeof(double));
+        if (s != CP_OK) return s;
+    }
+    cp_status s;
+    if ((s = dalloc(c, &c->adjSt, 1)) != CP_OK) return s;
+    if ((s = dalloc(c, &c->adjPart, (size_t)4 * kMaxBlocks)) != CP_OK) return s;
+    if ((s = dalloc(c, &c->adjBar, 1)) != CP_OK) return s;
+    return CP_OK;
+}
+
+template <typename TV>
+cp_status adjoint_pcg(cp_ctx* c, const KParams& k, double* out) {
+    PcgBufs<TV> B = pcg_bufs<TV>(c);
+    CK(cudaMemsetAsync(c->adjBar, 0, sizeof(unsigned), c->stream));
+    if (c->useMg) {
+        MgHier<TV> H = mg_hier<TV>(c);
+        CK(launch_coop_cfg(k_pcg_mg<TV>, c->gMg, kMgThreads, kMgDynSmem, c->stream, k, c->adjSt,
+                           (const double*)c->dE, (const double*)c->dN, B, H, out, c->adjPart, c->adjBar));
+    } else {
+        CK(launch_coop(k_pcg<TV>, c->gPcg, c->stream, k, c->adjSt, (const double*)c->dE, (const double*)c->dN, B,
+                       out, c->adjPart, c->adjBar));
+    }
+    return CP_OK;
+}
+
+template <typename TV>
+cp_status adjoint_prhs(cp_ctx* c, const KParams& k, const double* du, const double* dv, const double* rp) {
+    PcgBufs<TV> B = pcg_bufs<TV>(c);
+    k_adj_prhs<TV><<<c->gElem, kThreads, 0, c->stream>>>(k, du, dv, rp, B.rhs);
+    CK(cudaGetLastError());
+    return CP_OK;
+}
+
+}  // namespace
+
+extern "C" cp_status cp_adjoint_dp_dgamma(cp_ctx* c, double* grad, long rows, long cols, long rs, long cs,
+                                          int max_iter, double tol, cp_adjoint_report* rep) {
+    if (!c || !grad) return fail(CP_ERR_BAD_PARAM, "NULL argument");
+    const int M = c->d.M, N = c->d.N;
+    if (rows != M - 1 || cols != N - 1) return fail(CP_ERR_BAD_PARAM, "grad shape %ld x %ld, expected %d x %d",
+                                                    rows, cols, M - 1, N - 1);
+    if (max_iter < 1 || !(tol > 0.0)) return fail(CP_ERR_BAD_PARAM, "max_iter >= 1 and tol > 0 required");
+    cp_status s = adjoint_alloc(c);
+    if (s != CP_OK) return s;
+    CK(cudaEventRecord(c->ev0, c->stream));
+    // vectors
+    double** A = c->adj;
+    AdjVecs V;
+    V.lu = A[0]; V.lv = A[1]; V.lc = A[2]; V.yu = A[3]; V.yv = A[4]; V.yp = A[5];
+    V.gu = A[6]; V.gv = A[7]; V.gp = A[8]; V.du = A[9]; V.dv = A[10]; V.eu = A[11]; V.ev = A[12];
+    double *ru = A[13], *rv = A[14], *rp = A[15], *dc = A[16], *Jd = A[17];
+    const size_t bytes = c->nElem * sizeof(double);
+    for (int q = 0; q < 18; ++q) CK(cudaMemsetAsync(A[q], 0, bytes, c->stream));
+    CK(cudaMemsetAsync(c->adjSt, 0, sizeof(Status), c->stream));
+    // the converged state's iteration count fixes the inlet velocity (ramp)
+    CK(cudaMemcpyAsync(c->stHost, c->st, sizeof(Status), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    const int iterState = std::max(c->stHost->iter - 1, 0);
+    KParams k = c->k;
+    // Picard coefficients of the converged state (double), dE / dN
+    MomSys<double> Us, Vs;
+    {
+        double** m = reinterpret_cast<double**>(c->adjMom);
+        Us.aP = m[0]; Us.aE = m[1]; Us.aW = m[2]; Us.aN = m[3]; Us.aS = m[4]; Us.b = m[5];
+        Vs.aP = m[6]; Vs.aE = m[7]; Vs.aW = m[8]; Vs.aN = m[9]; Vs.aS = m[10]; Vs.b = m[11];
+    }
+    // the assembly reads Status::iter for the inlet velocity
+    CK(cudaMemcpyAsync(&c->adjSt->iter, &iterState, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    Fields f{c->u, c->v, c->p, c->alpha, c->gamma};
+    k_assemble<double, false><<<c->gElem, kThreads, 0, c->stream>>>(k, c->adjSt, f, Us, Vs, c->dE, c->dN, 1, 1);
+    CK(cudaGetLastError());
+    AdjCtx ac;
+    ac.k = k;
+    ac.u = c->u; ac.v = c->v; ac.p = c->p; ac.alpha = c->alpha; ac.gamma = c->gamma;
+    ac.maxVel = max_vel(inlet_velocity(k, iterState));
+    // right-hand side dJ/dX and J
+    k_adj_g<<<1, 1024, 0, c->stream>>>(ac, V, Jd);
+    CK(cudaGetLastError());
+    // pressure-like solves: fixed iteration count, no early stop
+    KParams kp = k;
+    kp.pTol = 0.0;
+    kp.maxP = c->useMg ? 8 : 100;
+    const int sweeps = 12;
+    const int nb = c->gElem;
+    std::vector<double> part((size_t)2 * nb);
+    double res = 1.0, gnorm = 0.0;
+    int it = 0;
+    bool conv = false;
+    for (; it <= max_iter; ++it) {
+        // y = J^T lambda; r = g - y
+        for (double* y : {V.yu, V.yv, V.yp}) CK(cudaMemsetAsync(y, 0, bytes, c->stream));
+        k_adj_jt<<<nb, kThreads, 0, c->stream>>>(ac, V, nullptr, nullptr, nullptr);
+        CK(cudaGetLastError());
+        k_adj_defect<<<nb, kThreads, 0, c->stream>>>(k, V, ru, rv, rp, c->adjPart);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(part.data(), c->adjPart, part.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                           c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        double rr = 0.0, gg = 0.0;
+        for (int b = 0; b < nb; ++b) { rr += part[2 * b]; gg += part[2 * b + 1]; }
+        gnorm = std::sqrt(gg);
+        res = gnorm > 0.0 ? std::sqrt(rr) / gnorm : 0.0;
+        if (!std::isfinite(res)) return fail(CP_ERR_NONFINITE, "adjoint residual is not finite at iteration %d", it);
+        if (res <= tol || it == max_iter) { conv = res <= tol; break; }
+        // momentum: Jacobi sweeps on the transposed relaxed Picard system
+        double *xu = V.du, *xv = V.dv;
+        double *yu = V.eu, *yv = V.ev;
+        for (int q = 0; q < sweeps; ++q) {
+            k_adj_jacobi_t<<<nb, kThreads, 0, c->stream>>>(k, Us, Vs, ru, rv, xu, xv, yu, yv, q == 0);
+            CK(cudaGetLastError());
+            std::swap(xu, yu);
+            std::swap(xv, yv);
+        }
+        // pressure-like correction with the forward pressure operator
+        s = c->prm.precision == CP_PREC_MIXED ? adjoint_prhs<float>(c, kp, xu, xv, rp)
+                                              : adjoint_prhs<double>(c, kp, xu, xv, rp);
+        if (s != CP_OK) return s;
+        CK(cudaMemsetAsync(c->adjSt, 0, sizeof(Status), c->stream));
+        s = c->prm.precision == CP_PREC_MIXED ? adjoint_pcg<float>(c, kp, dc) : adjoint_pcg<double>(c, kp, dc);
+        if (s != CP_OK) return s;
+        k_adj_update<<<nb, kThreads, 0, c->stream>>>(k, V, xu, xv, dc, c->dE, c->dN, c->prm.pAlpha);
+        CK(cudaGetLastError());
+    }
+    // gradient on the Ny x Nx cells
+    double* gd = A[18];
+    const double amax = c->prm.eta / std::max(c->prm.brinkmanKMin, 1e-20);
+    k_adj_grad<<<nb, kThreads, 0, c->stream>>>(ac, V, amax, c->prm.brinkmanQ, gd);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(c->ev1, c->stream));
+    std::vector<double> g((size_t)(M - 1) * (N - 1));
+    double Jh = 0.0;
+    CK(cudaMemcpyAsync(g.data(), gd, g.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(&Jh, Jd, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    Status hs;
+    CK(cudaMemcpy(&hs, c->adjSt, sizeof(Status), cudaMemcpyDeviceToHost));
+    if (hs.err) return fail((cp_status)hs.err, "device reported %s in the adjoint", cp_status_string((cp_status)hs.err));
+    for (long i = 0; i < rows; ++i)
+        for (long j = 0; j < cols; ++j) grad[i * rs + j * cs] = g[(size_t)i * (N - 1) + j];
+    if (rep) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+        rep->iterations = it;
+        rep->converged = conv ? 1 : 0;
+        rep->residual = res;
+        rep->J = Jh;
+        rep->device_ms = ms;
+    }
+    return CP_OK;
+}
 
 // ======================================================================== no-allocation entry point
 // cp_pressure_noalloc: the Jacobi-PCG pressure-correction solve (k_mass +

@@ -241,6 +241,24 @@ cp_status cp_pressure_noalloc(const cp_params* p, const double* dE, const double
                               const double* vStar, long pitch, double* pStar, int* iters, double* residMass,
                               void* stream);
 
+/* Discrete adjoint of the full-system total-pressure drop J (fullTotalDrop,
+ * SIMPLE.cpp:432) with respect to the density field gamma, at the context's
+ * current state (run the forward solve to convergence first).  New: the
+ * reference has no flow adjoint.  grad receives dJ/dgamma for the Ny x Nx
+ * cells (strides in elements).  The adjoint equations J_X^T lambda = dJ/dX
+ * of the converged discretisation are solved by defect correction with a
+ * transposed-SIMPLE preconditioner; iteration stops when
+ * ||dJ/dX - J_X^T lambda|| <= tol ||dJ/dX|| or after max_iter. */
+typedef struct cp_adjoint_report {
+    int iterations;        /* defect-correction iterations run          */
+    int converged;         /* 1 if the relative residual reached tol    */
+    double residual;       /* final relative residual                   */
+    double J;              /* pressure drop evaluated at the state [Pa] */
+    double device_ms;      /* device time of the adjoint (CUDA events)  */
+} cp_adjoint_report;
+cp_status cp_adjoint_dp_dgamma(cp_ctx* ctx, double* grad, long rows, long cols, long row_stride,
+                               long col_stride, int max_iter, double tol, cp_adjoint_report* rep);
+
 /* Per-iteration history rows (cp_iter_report layout without device_ms, as
  * doubles: see cp_history_columns()).  Returns the number of rows copied. */
 int cp_history_columns(void);
