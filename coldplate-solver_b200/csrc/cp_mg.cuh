@@ -22,11 +22,12 @@
 #pragma once
 
 #include "cp_kernels.cuh"
+#include "cp_tma.cuh"
 
 namespace cp {
 
 constexpr int kMgMaxLevels = 16;
-constexpr int kMgCtaCells = 16384;   // levels at or below this size run on one CTA
+constexpr int kMgCtaCells = 1024;    // levels at or below this size run on one CTA
 constexpr int kMgDense = 64;         // coarsest level size solved by a dense inverse
 
 template <typename TV>
@@ -43,7 +44,11 @@ struct MgHier {
     MgLevel<TV> lv[kMgMaxLevels];
     TV* dense;              // kMgDense^2 inverse of the coarsest operator
     double omega;           // Jacobi damping
+    double scale;           // coarse-correction scaling (1: plain Galerkin correction)
+    unsigned long long* prof;  // optional per-phase device-time accumulators (ns), or null
 };
+
+enum MgPhase { MG_P_SETUP = 0, MG_P_A, MG_P_B, MG_P_DOWN, MG_P_CTA, MG_P_UP, MG_P_COUNT };
 
 // ---------------------------------------------------------------- level ops
 template <typename TV>
@@ -109,17 +114,67 @@ __device__ __forceinline__ void mg_restrict_cell(const MgLevel<TV>& f, const MgL
 // x' = x + P e; y = x' + omega D^-1 (b - A x').  Writes y (the other buffer).
 template <typename TV>
 __device__ __forceinline__ TV mg_prolong_smooth_cell(const MgLevel<TV>& f, const MgLevel<TV>& c, const TV* e,
-                                                     int i, int j, double omega) {
+                                                     int i, int j, double omega, double c_scale) {
     // e: the coarse level's corrected iterate (its x or y buffer)
+    const TV sc = (TV)c_scale;
     auto xp = [&](int ii, int jj) -> TV {
         if (ii < 1 || ii > f.nI || jj < 1 || jj > f.nJ) return (TV)0;
-        return f.x[lidx(f, ii, jj)] + e[lidx(c, (ii + 1) >> 1, (jj + 1) >> 1)];
+        return f.x[lidx(f, ii, jj)] + sc * e[lidx(c, (ii + 1) >> 1, (jj + 1) >> 1)];
     };
     const size_t q = lidx(f, i, j);
     const TV xc = xp(i, j);
     const TV ax = f.d[q] * xc - f.fE[q] * xp(i, j + 1) - f.fE[q - 1] * xp(i, j - 1) - f.fN[q] * xp(i + 1, j) -
                   f.fN[q - f.P] * xp(i - 1, j);
     const TV y = xc + (TV)omega * (f.b[q] - ax) / f.d[q];
+    f.y[q] = y;
+    return y;
+}
+
+// ---------------------------------------------------------------- level 0
+// Level 0 keeps no iterate of its own: its right-hand side is the CG
+// residual r (f.b aliases it) and the pre-smoothed iterate from zero is
+// x0 = omega r / d, recomputed where needed (zero off the unknowns, where
+// r and d are zero).
+template <typename TV>
+__device__ __forceinline__ TV l0_x(const MgLevel<TV>& f, size_t q, TV om) {
+    const TV dd = f.d[q];
+    return dd != (TV)0 ? om * f.b[q] / dd : (TV)0;
+}
+
+// restriction of the level-0 residual b - A x0 over one 2 x 2 aggregate;
+// d x0 = omega b, so the residual is (1 - omega) b + off-diagonal terms
+template <typename TV>
+__device__ __forceinline__ void mg_restrict0_cell(const MgLevel<TV>& f, const MgLevel<TV>& c, int I, int J,
+                                                  double omega) {
+    const int i0 = 2 * I - 1, i1 = min(2 * I, f.nI), j0 = 2 * J - 1, j1 = min(2 * J, f.nJ);
+    const TV om = (TV)omega;
+    double s = 0.0;
+    for (int i = i0; i <= i1; ++i)
+        for (int j = j0; j <= j1; ++j) {
+            const size_t q = lidx(f, i, j);
+            const TV r = ((TV)1 - om) * f.b[q] + f.fE[q] * l0_x(f, q + 1, om) + f.fE[q - 1] * l0_x(f, q - 1, om) +
+                         f.fN[q] * l0_x(f, q + f.P, om) + f.fN[q - f.P] * l0_x(f, q - f.P, om);
+            s += (double)r;
+        }
+    const size_t q = lidx(c, I, J);
+    c.b[q] = (TV)s;
+    c.x[q] = (TV)(omega * s / (double)c.d[q]);
+}
+
+// prolongation into level 0 + one Jacobi sweep: x' = x0 + P e, y = x' + omega (b - A x') / d
+template <typename TV>
+__device__ __forceinline__ TV mg_prolong0_cell(const MgLevel<TV>& f, const MgLevel<TV>& c, const TV* e, int i,
+                                               int j, double omega) {
+    const TV om = (TV)omega;
+    auto xp = [&](int ii, int jj) -> TV {
+        if (ii < 1 || ii > f.nI || jj < 1 || jj > f.nJ) return (TV)0;
+        return l0_x(f, lidx(f, ii, jj), om) + e[lidx(c, (ii + 1) >> 1, (jj + 1) >> 1)];
+    };
+    const size_t q = lidx(f, i, j);
+    const TV xc = xp(i, j);
+    const TV ax = f.d[q] * xc - f.fE[q] * xp(i, j + 1) - f.fE[q - 1] * xp(i, j - 1) - f.fN[q] * xp(i + 1, j) -
+                  f.fN[q - f.P] * xp(i - 1, j);
+    const TV y = xc + om * (f.b[q] - ax) / f.d[q];
     f.y[q] = y;
     return y;
 }
@@ -196,23 +251,82 @@ __device__ void mg_cta_cycle(const MgHier<TV>& H) {
     for (int l = H.L - 2; l >= H.Lg; --l) {
         const MgLevel<TV>& f = H.lv[l];
         for_cells(s, f.nI, f.nJ,
-                  [&](int i, int j) { mg_prolong_smooth_cell(f, H.lv[l + 1], H.lv[l + 1].x, i, j, H.omega); });
+                  [&](int i, int j) { mg_prolong_smooth_cell(f, H.lv[l + 1], H.lv[l + 1].x, i, j, H.omega, H.scale); });
         __syncthreads();
         for_cells(s, f.nI, f.nJ, [&](int i, int j) { const size_t q = lidx(f, i, j); f.x[q] = f.y[q]; });
         __syncthreads();
     }
 }
 
+// ---------------------------------------------------------------- TMA tiles of level 0
+// Tensor maps of the arrays the level-0 phases read (built per context).
+struct MgMaps {
+    CUtensorMap z, pa, pb, r, d, fE, fN, e1;
+};
+
+template <typename TV>
+struct TileSmem {
+    static constexpr int kBox = ((kBoxR * kBoxW * (int)sizeof(TV) + 127) / 128) * 128;
+    static constexpr int kCBox = ((kCBoxR * kCBoxW * (int)sizeof(TV) + 127) / 128) * 128;
+    static constexpr int kStage = 5 * kBox;   // up to five boxes per stage
+    static constexpr int kBytes = 2 * kStage;
+};
+
+// Runs compute(tile, stage) over this CTA's tiles (tile = blockIdx.x + k G)
+// with a two-stage TMA pipeline; issue(tile, stage) is called by thread 0
+// and must arm the stage's mbarrier and start the copies.  `parity` holds
+// the phase bit of each stage's mbarrier (kept in step by all threads).
+template <typename Issue, typename Compute>
+__device__ __forceinline__ bool tile_loop(int ntiles, uint64_t* bars, unsigned& parity, int* err, Issue&& issue,
+                                          Compute&& compute) {
+    const int G = gridDim.x;
+    if (threadIdx.x == 0) {
+        fence_proxy_async_global();
+        for (int s = 0; s < 2; ++s) {
+            const int t = blockIdx.x + s * G;
+            if (t < ntiles) issue(t, s);
+        }
+    }
+    int k = 0;
+    for (int t = blockIdx.x; t < ntiles; t += G, ++k) {
+        const int s = k & 1;
+        if (!mbar_wait(&bars[s], (parity >> s) & 1u, err)) return false;
+        parity ^= (1u << s);
+        compute(t, s);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const int tn = t + 2 * G;
+            if (tn < ntiles) {
+                fence_proxy_async_shared();
+                issue(tn, s);
+            }
+        }
+    }
+    return true;
+}
+
 // ---------------------------------------------------------------- the solver
 // B (PcgBufs) holds level-0 faces, diagonal and the CG vectors in the field
 // layout; H.lv[0] aliases them (fE, fN, d) plus its own x/y/b/dx buffers.
 template <typename TV>
-__global__ void __launch_bounds__(512) k_pcg_mg(KParams k, Status* st, const double* dE, const double* dN,
+__global__ void __launch_bounds__(512, 1) k_pcg_mg(KParams k, Status* st, const double* dE, const double* dN,
                                                 PcgBufs<TV> B, MgHier<TV> H, double* pStar, double* part,
-                                                unsigned* bar) {
+                                                unsigned* bar, const __grid_constant__ MgMaps maps) {
     if (st->done) return;
-    extern __shared__ double dsm[];   // dense setup workspace (kMgDense x 2 kMgDense)
+    // dynamic shared memory: dense set-up workspace, later the TMA tile stages
+    extern __shared__ __align__(128) double dsm[];
     __shared__ double sm[96];
+    __shared__ __align__(8) uint64_t tbar[2];
+    unsigned tpar = 0;
+    if (threadIdx.x == 0) {
+        mbar_init(&tbar[0], 1);
+        mbar_init(&tbar[1], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    unsigned char* stg = reinterpret_cast<unsigned char*>(dsm);
+    typedef TileSmem<TV> TS;
+    auto box = [&](int stage, int q) -> TV* { return reinterpret_cast<TV*>(stg + stage * TS::kStage + q * TS::kBox); };
     const Dims d = k.d;
     const int M = d.M, N = d.N, w = N - 2;
     const int n = (M - 1) * w;
@@ -265,46 +379,169 @@ __global__ void __launch_bounds__(512) k_pcg_mg(KParams k, Status* st, const dou
     if (blockIdx.x == 0) mg_dense_setup(H.lv[H.L - 1], H.dense, dsm);
     MG_SYNC();
 
-    // ---- z = M r (V-cycle); level-0 rhs is r; result in L0.y; also r.z
-    // The pre-smoothing step of level 0 (x0 = omega r / d) is written by the
-    // caller phase; `rz` returns the global r.z.
-    auto vcycle = [&](double& rz) -> bool {
-        // down over grid-wide levels
-        for (int l = 0; l < H.Lg - 1; ++l) {
-            for_cells(all, H.lv[l + 1].nI, H.lv[l + 1].nJ,
-                      [&](int I, int J) { mg_restrict_cell(H.lv[l], H.lv[l + 1], I, J, om); });
-            target += G;
-            if (!grid_barrier(bar, target, &st->err)) return false;
+    auto tick = [&](int ph, unsigned long long& t0) {
+        if (H.prof && blockIdx.x == 0 && threadIdx.x == 0) {
+            const unsigned long long t = globaltimer_ns();
+            atomicAdd(H.prof + ph, t - t0);
+            t0 = t;
         }
-        {
-            if (blockIdx.x == 0) {
-                // restrict the last grid-wide level into the first CTA level
-                const int l = H.Lg - 1;
-                for_cells(Split{(int)threadIdx.x, (int)blockDim.x}, H.lv[l + 1].nI, H.lv[l + 1].nJ,
-                          [&](int I, int J) { mg_restrict_cell(H.lv[l], H.lv[l + 1], I, J, om); });
-                __syncthreads();
-                if (H.Lg < H.L - 1) {
-                    mg_cta_cycle(H);
-                } else {
-                    mg_dense_solve(H.lv[H.L - 1], H.dense);
+    };
+    unsigned long long tp = (H.prof && blockIdx.x == 0 && threadIdx.x == 0) ? globaltimer_ns() : 0ull;
+
+    // ---- level-0 tile phases (TMA staged)
+    const int nI0 = M - 1, nJ0 = w;
+    const int tilesI = (nI0 + kTileR - 1) / kTileR, tilesJ = (nJ0 + kTileC - 1) / kTileC;
+    const int ntiles = tilesI * tilesJ;
+    const TV omT = (TV)om;
+    const unsigned fineBox = kBoxR * kBoxW * sizeof(TV);
+    const unsigned coarseBox = kCBoxR * kCBoxW * sizeof(TV);
+    auto issue_fine = [&](int t, int s, const CUtensorMap* const* mp, int nb, bool withCoarse) {
+        const int tI = t / tilesJ, tJ = t % tilesJ;
+        mbar_expect_tx(&tbar[s], nb * fineBox + (withCoarse ? coarseBox : 0u));
+        for (int q = 0; q < nb; ++q) tma_load_2d(box(s, q), mp[q], kTileC * tJ, kTileR * tI, &tbar[s]);
+        if (withCoarse)
+            tma_load_2d(box(s, nb), &maps.e1, (kTileC / 2) * tJ, (kTileR / 2) * tI, &tbar[s]);
+    };
+    // smem element (li, lj) of a fine box: array row i0 - 1 + li, column j0 - 1 + lj
+#define SB(q, li, lj) (bx[q][(li) * kBoxW + (lj)])
+    // level-0 pre-smoothed iterate omega r / d in the box
+    auto x0s = [&](TV* const* bx, int li, int lj) -> TV {
+        const TV dd = SB(1, li, lj);
+        return dd != (TV)0 ? omT * SB(0, li, lj) / dd : (TV)0;
+    };
+    // restriction of the level-0 residual into level 1 (boxes: r, d, fE, fN)
+    auto restrict0_tiles = [&]() -> bool {
+        const CUtensorMap* mp[4] = {&maps.r, &maps.d, &maps.fE, &maps.fN};
+        const MgLevel<TV>& C1 = H.lv[1];
+        return tile_loop(ntiles, tbar, tpar, &st->err,
+                         [&](int t, int s) { issue_fine(t, s, mp, 4, false); },
+                         [&](int t, int s) {
+            TV* bx[4] = {box(s, 0), box(s, 1), box(s, 2), box(s, 3)};
+            const int tI = t / tilesJ, tJ = t % tilesJ;
+            const int i0 = 1 + kTileR * tI, j0 = 1 + kTileC * tJ;
+            for (int u = threadIdx.x; u < 2 * (kTileR / 2) * (kTileC / 2); u += blockDim.x) {
+                const int cc = u >> 1, h = u & 1;
+                const int cr = cc / (kTileC / 2), ccol = cc % (kTileC / 2);
+                const int a = 2 * cr + h;
+                double sum = 0.0;
+#pragma unroll
+                for (int q = 0; q < 2; ++q) {
+                    const int b = 2 * ccol + q;
+                    if (i0 + a <= nI0 && j0 + b <= nJ0) {
+                        const int li = a + 1, lj = b + 1;
+                        const TV r = ((TV)1 - omT) * SB(0, li, lj) + SB(2, li, lj) * x0s(bx, li, lj + 1) +
+                                     SB(2, li, lj - 1) * x0s(bx, li, lj - 1) + SB(3, li, lj) * x0s(bx, li + 1, lj) +
+                                     SB(3, li - 1, lj) * x0s(bx, li - 1, lj);
+                        sum += (double)r;
+                    }
+                }
+                sum += __shfl_xor_sync(0xffffffffu, sum, 1);
+                const int I = 1 + (kTileR / 2) * tI + cr, J = 1 + (kTileC / 2) * tJ + ccol;
+                if (h == 0 && I <= C1.nI && J <= C1.nJ) {
+                    const size_t q = lidx(C1, I, J);
+                    C1.b[q] = (TV)sum;
+                    C1.x[q] = (TV)(om * sum / (double)C1.d[q]);
                 }
             }
+        });
+    };
+    // prolongation from level 1 + post-smoothing of level 0 (boxes: r, d,
+    // fE, fN and the coarse correction); writes z = L0.y, accumulates r.z
+    const TV scT = (TV)H.scale;
+    auto prolong0_tiles = [&](double& rzacc) -> bool {
+        const CUtensorMap* mp[4] = {&maps.r, &maps.d, &maps.fE, &maps.fN};
+        const MgLevel<TV>& F0 = H.lv[0];
+        return tile_loop(ntiles, tbar, tpar, &st->err,
+                         [&](int t, int s) { issue_fine(t, s, mp, 4, true); },
+                         [&](int t, int s) {
+            TV* bx[4] = {box(s, 0), box(s, 1), box(s, 2), box(s, 3)};
+            const TV* ce = box(s, 4);
+            const int tI = t / tilesJ, tJ = t % tilesJ;
+            const int i0 = 1 + kTileR * tI, j0 = 1 + kTileC * tJ;
+            // x' = x0 + e(agg) on unknowns, 0 elsewhere
+            auto xp = [&](int li, int lj) -> TV {
+                const int ii = i0 - 1 + li, jj = j0 - 1 + lj;
+                if (ii < 1 || ii > nI0 || jj < 1 || jj > nJ0) return (TV)0;
+                const int cli = ((ii + 1) >> 1) - (kTileR / 2) * tI, clj = ((jj + 1) >> 1) - (kTileC / 2) * tJ;
+                return x0s(bx, li, lj) + scT * ce[cli * kCBoxW + clj];
+            };
+            for (int u = threadIdx.x; u < kTileR * kTileC; u += blockDim.x) {
+                const int a = u / kTileC, b = u % kTileC;
+                if (i0 + a > nI0 || j0 + b > nJ0) continue;
+                const int li = a + 1, lj = b + 1;
+                const TV xc = xp(li, lj);
+                const TV ax = SB(1, li, lj) * xc - SB(2, li, lj) * xp(li, lj + 1) - SB(2, li, lj - 1) * xp(li, lj - 1) -
+                              SB(3, li, lj) * xp(li + 1, lj) - SB(3, li - 1, lj) * xp(li - 1, lj);
+                const TV rb = SB(0, li, lj);
+                const TV y = xc + omT * (rb - ax) / SB(1, li, lj);
+                F0.y[at(d, i0 + a, j0 + b)] = y;
+                rzacc += (double)rb * (double)y;
+            }
+        });
+    };
+    // CG matvec on the new direction p = z + beta p_old (boxes: z, p_old, d, fE, fN)
+    auto cgA_tiles = [&](bool first, double beta, TV* pnew, const CUtensorMap* pold, double& acc) -> bool {
+        const CUtensorMap* mp[5] = {&maps.z, pold, &maps.d, &maps.fE, &maps.fN};
+        const TV bt = (TV)beta;
+        return tile_loop(ntiles, tbar, tpar, &st->err,
+                         [&](int t, int s) { issue_fine(t, s, mp, 5, false); },
+                         [&](int t, int s) {
+            TV* bx[5] = {box(s, 0), box(s, 1), box(s, 2), box(s, 3), box(s, 4)};
+            const int tI = t / tilesJ, tJ = t % tilesJ;
+            const int i0 = 1 + kTileR * tI, j0 = 1 + kTileC * tJ;
+            auto dir = [&](int li, int lj) -> TV {
+                return first ? SB(0, li, lj) : (TV)(SB(0, li, lj) + bt * SB(1, li, lj));
+            };
+            for (int u = threadIdx.x; u < kTileR * kTileC; u += blockDim.x) {
+                const int a = u / kTileC, b = u % kTileC;
+                if (i0 + a > nI0 || j0 + b > nJ0) continue;
+                const int li = a + 1, lj = b + 1;
+                const TV pc = dir(li, lj);
+                const TV ap = SB(2, li, lj) * pc - SB(4, li - 1, lj) * dir(li - 1, lj) - SB(3, li, lj - 1) * dir(li, lj - 1) -
+                              SB(3, li, lj) * dir(li, lj + 1) - SB(4, li, lj) * dir(li + 1, lj);
+                const size_t c = at(d, i0 + a, j0 + b);
+                pnew[c] = pc;
+                B.Ap[c] = ap;
+                acc += (double)pc * (double)ap;
+            }
+        });
+    };
+
+    // ---- z = M r (V-cycle).  Level 0's rhs is r (L0.b aliases B.r) and its
+    // pre-smoothed iterate omega r / d is implicit.  Result z in L0.y, and
+    // `rz` gets the global r.z.
+    auto vcycle = [&](double& rz) -> bool {
+        // down: restrict into every level up to the first CTA level
+        for (int l = 0; l < H.Lg; ++l) {
+            if (l == 0) {
+                if (!restrict0_tiles()) return false;
+            } else
+                for_cells(all, H.lv[l + 1].nI, H.lv[l + 1].nJ,
+                          [&](int I, int J) { mg_restrict_cell(H.lv[l], H.lv[l + 1], I, J, om); });
             target += G;
             if (!grid_barrier(bar, target, &st->err)) return false;
         }
-        // up over grid-wide levels: prolongate + post-smooth into y (the
-        // corrected iterate of a grid-wide level stays in y, of a CTA level in x)
+        tick(MG_P_DOWN, tp);
+        // the small levels on CTA 0
+        if (blockIdx.x == 0) {
+            if (H.Lg < H.L - 1) mg_cta_cycle(H);
+            else mg_dense_solve(H.lv[H.L - 1], H.dense);
+        }
+        target += G;
+        if (!grid_barrier(bar, target, &st->err)) return false;
+        tick(MG_P_CTA, tp);
+        // up: prolongate + post-smooth into y (the corrected iterate of a
+        // grid-wide level stays in y, of a CTA level in x)
         for (int l = H.Lg - 1; l >= 0; --l) {
             const MgLevel<TV>& f = H.lv[l];
             const TV* e = (l + 1 < H.Lg) ? H.lv[l + 1].y : H.lv[l + 1].x;
             double acc[1] = {0.0};
-            for_cells(all, f.nI, f.nJ, [&](int i, int j) {
-                const TV y = mg_prolong_smooth_cell(f, H.lv[l + 1], e, i, j, om);
-                if (l == 0) acc[0] += (double)f.b[lidx(f, i, j)] * (double)y;
-            });
             if (l == 0) {
+                if (!prolong0_tiles(acc[0])) return false;
                 block_sum<1>(acc, sm);
                 if (threadIdx.x == 0) partB[2 * blockIdx.x + 1] = acc[0];
+            } else {
+                for_cells(all, f.nI, f.nJ, [&](int i, int j) { mg_prolong_smooth_cell(f, H.lv[l + 1], e, i, j, om, H.scale); });
             }
             target += G;
             if (!grid_barrier(bar, target, &st->err)) return false;
@@ -312,17 +549,11 @@ __global__ void __launch_bounds__(512) k_pcg_mg(KParams k, Status* st, const dou
         double t2[2];
         sum_partials<2>(partB, G, 2, t2, sm);
         rz = t2[1];
+        tick(MG_P_UP, tp);
         return true;
     };
 
-    // first preconditioning: level-0 b is r, x = omega r / d
-    for (int t = tid; t < n; t += nth) {
-        const int i = 1 + t / w, j = 1 + t % w;
-        const size_t c = at(d, i, j);
-        L0.b[c] = B.r[c];
-        L0.x[c] = (TV)(om * (double)B.r[c] / (double)B.d[c]);
-    }
-    MG_SYNC();
+    tick(MG_P_SETUP, tp);
     double rz = 0.0;
     if (!vcycle(rz)) return;
     // z lives in L0.y; p_new = z + beta p_old recomputed at the neighbours
@@ -331,47 +562,47 @@ __global__ void __launch_bounds__(512) k_pcg_mg(KParams k, Status* st, const dou
     TV* pbuf[2] = {B.pa, B.pb};
     for (; it < k.maxP; ++it) {
         const bool first = (it == 0);
-        const TV* pold = pbuf[(it + 1) & 1];
-        TV* pnew = pbuf[it & 1];
-        const TV* z = L0.y;
-        auto dir = [&](size_t c) -> TV { return first ? z[c] : (TV)(z[c] + (TV)beta * pold[c]); };
+        TV* __restrict__ pnew = pbuf[it & 1];
         double accA[1] = {0.0};
-        for (int t = tid; t < n; t += nth) {
-            const int i = 1 + t / w, j = 1 + t % w;
-            const size_t c = at(d, i, j);
-            const TV pc = dir(c);
-            const TV pS = (i > 1) ? dir(c - d.P) : (TV)0;
-            const TV pW = (j > 1) ? dir(c - 1) : (TV)0;
-            const TV pE = (j < w) ? dir(c + 1) : (TV)0;
-            const TV pN = (i < M - 1) ? dir(c + d.P) : (TV)0;
-            const TV ap = B.d[c] * pc - B.fN[c - d.P] * pS - B.fE[c - 1] * pW - B.fE[c] * pE - B.fN[c] * pN;
-            pnew[c] = pc;
-            B.Ap[c] = ap;
-            accA[0] += (double)pc * (double)ap;
-        }
+        if (!cgA_tiles(first, beta, pnew, (it & 1) ? &maps.pa : &maps.pb, accA[0])) return;
         block_sum<1>(accA, sm);
         if (threadIdx.x == 0) partA[blockIdx.x] = accA[0];
         MG_SYNC();
         double pAp[1];
         sum_partials<1>(partA, G, 1, pAp, sm);
+        tick(MG_P_A, tp);
         if (fabs(pAp[0]) < 1e-20) break;
         const double alpha = rz / pAp[0];
+        const TV al = (TV)alpha;
         double accB[1] = {0.0};
-        for (int t = tid; t < n; t += nth) {
-            const int i = 1 + t / w, j = 1 + t % w;
-            const size_t c = at(d, i, j);
-            B.x[c] = B.x[c] + (TV)alpha * pnew[c];
-            const TV r = B.r[c] - (TV)alpha * B.Ap[c];
-            B.r[c] = r;
-            accB[0] += (double)r * (double)r;
-            L0.b[c] = r;
-            L0.x[c] = (TV)(om * (double)r / (double)B.d[c]);
+        for (int t0 = tid; t0 < n; t0 += 2 * nth) {
+            TV xv[2], pv[2], rv[2], av[2];
+            size_t cc[2];
+            bool ok[2];
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                const int t = t0 + q * nth;
+                ok[q] = t < n;
+                const int tt = ok[q] ? t : t0;
+                const size_t c = at(d, 1 + tt / w, 1 + tt % w);
+                cc[q] = c;
+                xv[q] = B.x[c]; pv[q] = pnew[c]; rv[q] = B.r[c]; av[q] = B.Ap[c];
+            }
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                if (!ok[q]) continue;
+                B.x[cc[q]] = xv[q] + al * pv[q];
+                const TV r = rv[q] - al * av[q];
+                B.r[cc[q]] = r;
+                accB[0] += (double)r * (double)r;
+            }
         }
         block_sum<1>(accB, sm);
         if (threadIdx.x == 0) partB[2 * blockIdx.x] = accB[0];
         MG_SYNC();
         double tB[2];
         sum_partials<2>(partB, G, 2, tB, sm);
+        tick(MG_P_B, tp);
         if (sqrt(tB[0]) < k.pTol) break;
         double rzn = 0.0;
         if (!vcycle(rzn)) return;
@@ -386,6 +617,7 @@ __global__ void __launch_bounds__(512) k_pcg_mg(KParams k, Status* st, const dou
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) st->itersP = it;
 #undef MG_SYNC
+#undef SB
 }
 
 }  // namespace cp

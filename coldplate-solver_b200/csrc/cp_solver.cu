@@ -83,6 +83,9 @@ struct cp_ctx {
     void* mgArr[kMgMaxLevels][7] = {};   // fE fN d dx x y b
     void* mgDense = nullptr;
     double mgOmega = 0.8;
+    double mgScale = 1.0;
+    unsigned long long* mgProf = nullptr;   // per-phase timers when CP_MG_PROFILE is set
+    MgMaps mgMaps;                           // TMA tensor maps of the level-0 tile phases
     // adjoint buffers (allocated on first use, double)
     double* adj[20] = {};
     void* adjMom[12] = {};
@@ -280,6 +283,37 @@ PcgBufs<TV> pcg_bufs(cp_ctx* c) {
     return b;
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda link)
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+cp_status encode_map(CUtensorMap* m, void* base, int elemBytes, int pitch, int rows, int boxW, int boxR) {
+    static EncodeTiledFn fn = nullptr;
+    if (!fn) {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !f)
+            return fail(CP_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+        fn = reinterpret_cast<EncodeTiledFn>(f);
+    }
+    // tile origins are multiples of 32 elements and the boxes' inner extents
+    // multiples of 16 bytes; the pitch must keep every row 16-byte aligned
+    if (((size_t)pitch * elemBytes) % 16 != 0 || ((size_t)boxW * elemBytes) % 16 != 0 ||
+        (reinterpret_cast<uintptr_t>(base) & 15) != 0)
+        return fail(CP_ERR_CUDA, "tensor map alignment");
+    const cuuint64_t dims[2] = {(cuuint64_t)pitch, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)pitch * elemBytes};
+    const cuuint32_t box[2] = {(cuuint32_t)boxW, (cuuint32_t)boxR};
+    const cuuint32_t es[2] = {1, 1};
+    CUresult r = fn(m, elemBytes == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, base,
+                    dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                    CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(CP_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return CP_OK;
+}
+
 template <typename TV>
 MgHier<TV> mg_hier(cp_ctx* c) {
     MgHier<TV> H;
@@ -287,7 +321,9 @@ MgHier<TV> mg_hier(cp_ctx* c) {
     H.L = c->mgL;
     H.Lg = c->mgLg;
     H.omega = c->mgOmega;
+    H.scale = c->mgScale;
     H.dense = (TV*)c->mgDense;
+    H.prof = c->mgProf;
     for (int l = 0; l < c->mgL; ++l) {
         MgLevel<TV>& v = H.lv[l];
         v.nI = c->mgNI[l]; v.nJ = c->mgNJ[l]; v.P = c->mgP[l];
@@ -298,7 +334,11 @@ MgHier<TV> mg_hier(cp_ctx* c) {
 }
 
 constexpr int kMgThreads = 512;
-constexpr size_t kMgDynSmem = sizeof(double) * (size_t)(kMgDense * 2 * kMgDense + kMgDense);
+// dynamic shared memory: the dense set-up workspace and, afterwards, the two
+// TMA tile stages (sized for double; the float kernel uses less of it)
+constexpr size_t kMgDenseSmem = sizeof(double) * (size_t)(kMgDense * 2 * kMgDense + kMgDense);
+constexpr size_t kMgDynSmem = kMgDenseSmem > (size_t)TileSmem<double>::kBytes ? kMgDenseSmem
+                                                                               : (size_t)TileSmem<double>::kBytes;
 
 // Level sizes: halve (rounding up) until at most kMgDense unknowns; levels
 // above kMgCtaCells unknowns (and always level 0) run grid-wide.
@@ -321,10 +361,13 @@ cp_status mg_build(cp_ctx* c) {
     c->mgArr[0][0] = c->pcg[0];
     c->mgArr[0][1] = c->pcg[1];
     c->mgArr[0][2] = c->pcg[2];
-    for (int q = 3; q < 7; ++q) {
+    // level 0: dx and y of its own; its rhs is the CG residual r; it keeps no x
+    for (int q = 3; q < 6; ++q) {
+        if (q == 4) continue;
         cp_status s = dalloc_bytes(c, &c->mgArr[0][q], c->nElem * c->es);
         if (s != CP_OK) return s;
     }
+    c->mgArr[0][6] = c->pcg[4];
     for (int l = 1; l < L; ++l) {
         c->mgP[l] = ((c->mgNJ[l] + 2 + 31) / 32) * 32;
         const size_t ne = (size_t)(c->mgNI[l] + 2) * c->mgP[l];
@@ -335,8 +378,27 @@ cp_status mg_build(cp_ctx* c) {
     }
     cp_status s = dalloc_bytes(c, &c->mgDense, (size_t)kMgDense * kMgDense * c->es);
     if (s != CP_OK) return s;
+    // tensor maps of the level-0 tile phases: z (level-0 y), p_a, p_b, r, d,
+    // fE, fN on the field layout; the level-1 corrected iterate for the
+    // prolongation (y of a grid-wide level 1, x of a CTA level)
+    {
+        const int R0 = c->d.M + 2, P0 = c->d.P, es = c->es;
+        void* a0[7] = {c->mgArr[0][5], c->pcg[5], c->pcg[6], c->pcg[4], c->pcg[2], c->pcg[0], c->pcg[1]};
+        CUtensorMap* m0[7] = {&c->mgMaps.z, &c->mgMaps.pa, &c->mgMaps.pb, &c->mgMaps.r, &c->mgMaps.d,
+                              &c->mgMaps.fE, &c->mgMaps.fN};
+        for (int q = 0; q < 7; ++q)
+            if ((s = encode_map(m0[q], a0[q], es, P0, R0, kBoxW, kBoxR)) != CP_OK) return s;
+        void* e1 = (Lg > 1) ? c->mgArr[1][5] : c->mgArr[1][4];
+        if ((s = encode_map(&c->mgMaps.e1, e1, es, c->mgP[1], c->mgNI[1] + 2, kCBoxW, kCBoxR)) != CP_OK) return s;
+    }
     const char* om = getenv("CP_MG_OMEGA");
     if (om) c->mgOmega = atof(om);
+    const char* sc = getenv("CP_MG_SCALE");
+    if (sc) c->mgScale = atof(sc);
+    if (getenv("CP_MG_PROFILE")) {
+        cp_status s2 = dalloc(c, &c->mgProf, (size_t)MG_P_COUNT);
+        if (s2 != CP_OK) return s2;
+    }
     // one CTA per SM (the dense set-up needs kMgDynSmem of shared memory)
     int nb = 0;
     if (c->prm.precision == CP_PREC_MIXED) {
@@ -396,7 +458,7 @@ cp_status enqueue_pressure(cp_ctx* c, EvRec* rec = nullptr) {
     if (c->useMg) {
         MgHier<TV> H = mg_hier<TV>(c);
         CK(launch_coop_cfg(k_pcg_mg<TV>, c->gMg, kMgThreads, kMgDynSmem, c->stream, c->k, c->st,
-                           (const double*)c->dE, (const double*)c->dN, B, H, c->pStar, c->partP, c->barP));
+                           (const double*)c->dE, (const double*)c->dN, B, H, c->pStar, c->partP, c->barP, c->mgMaps));
     } else {
         CK(launch_coop(k_pcg<TV>, c->gPcg, c->stream, c->k, c->st, (const double*)c->dE, (const double*)c->dN, B,
                        c->pStar, c->partP, c->barP));
@@ -870,6 +932,16 @@ cp_status cp_kernel_times(cp_ctx* c, int n_outer, cp_kernel_timing* out) {
         if ((s = device_error(c)) != CP_OK) break;
     }
     for (auto& e : rec.ev) cudaEventDestroy(e);
+    if (c->mgProf && out->iterations > 0) {
+        unsigned long long pr[MG_P_COUNT];
+        if (cudaMemcpy(pr, c->mgProf, sizeof pr, cudaMemcpyDeviceToHost) == cudaSuccess) {
+            const char* names[MG_P_COUNT] = {"setup", "cg_A", "cg_B", "vdown", "vcta", "vup"};
+            fprintf(stderr, "[cp mg profile] per outer iteration (us):");
+            for (int q = 0; q < MG_P_COUNT; ++q) fprintf(stderr, " %s %.1f", names[q], pr[q] * 1e-3 / out->iterations);
+            fprintf(stderr, "\n");
+        }
+        cudaMemset(c->mgProf, 0, sizeof pr);
+    }
     return s;
 }
 
@@ -955,7 +1027,7 @@ cp_status adjoint_pcg(cp_ctx* c, const KParams& k, double* out) {
     if (c->useMg) {
         MgHier<TV> H = mg_hier<TV>(c);
         CK(launch_coop_cfg(k_pcg_mg<TV>, c->gMg, kMgThreads, kMgDynSmem, c->stream, k, c->adjSt,
-                           (const double*)c->dE, (const double*)c->dN, B, H, out, c->adjPart, c->adjBar));
+                           (const double*)c->dE, (const double*)c->dN, B, H, out, c->adjPart, c->adjBar, c->mgMaps));
     } else {
         CK(launch_coop(k_pcg<TV>, c->gPcg, c->stream, k, c->adjSt, (const double*)c->dE, (const double*)c->dN, B,
                        out, c->adjPart, c->adjBar));

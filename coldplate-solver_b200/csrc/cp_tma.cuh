@@ -1,0 +1,97 @@
+// TMA (cp.async.bulk.tensor) tile staging for the stencil phases.
+//
+// A 2-D tensor map describes one array of the padded field layout: inner
+// extent P (the pitch, elements), outer extent R rows, row stride P * size.
+// Boxes are loaded into shared memory by one thread and completed on an
+// mbarrier with an expected byte count; reads outside the tensor extents are
+// filled with zeros by the hardware.
+//
+// Alignment: every box starts at an x coordinate that is a multiple of 32
+// elements (the tile origins below) and its inner extent in bytes is a
+// multiple of 16, as cp.async.bulk.tensor requires.  No multicast is used.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "cp_device.cuh"
+
+namespace cp {
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n"
+        " .reg .pred p;\n"
+        " mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n"
+        "}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait for the phase with the given parity; false after ~2 s.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, int* err) {
+    unsigned spins = 0;
+    unsigned long long t0 = 0;
+    while (!mbar_try_wait(bar, parity)) {
+        if (((++spins) & 1023u) == 0) {
+            const unsigned long long t = globaltimer_ns();
+            if (t0 == 0) t0 = t;
+            else if (t - t0 > kBarrierNs) {
+                atomicCAS(err, 0, (int)CP_ERR_TIMEOUT);
+                return false;
+            }
+        }
+    }
+    return true;
+}
+
+// Order this thread's later async-proxy (TMA) reads of global memory after
+// generic-proxy writes made visible to it (e.g. by a grid barrier).
+__device__ __forceinline__ void fence_proxy_async_global() {
+    asm volatile("fence.proxy.async.global;" ::: "memory");
+}
+__device__ __forceinline__ void fence_proxy_async_shared() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::
+            "r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
+}
+
+// Tile geometry of the level-0 stencil phases: TR x TC unknowns with a
+// one-cell halo, loaded as boxes of (TR + 2) x BW elements whose origin is
+// (x = TC * tJ, y = TR * tI) in array coordinates (the unknowns start at
+// i = j = 1, so the halo column/row sits exactly on a multiple of TC / TR).
+constexpr int kTileR = 16;
+constexpr int kTileC = 64;
+constexpr int kBoxR = kTileR + 2;   // 18
+constexpr int kBoxW = kTileC + 4;   // 68: >= TC + 2 and a multiple of 16 bytes for 4- and 8-byte types
+// coarse (level-1) box of the prolongation: rows 8 tI .. 8 tI + 9, cols 32 tJ .. 32 tJ + 35
+constexpr int kCBoxR = kTileR / 2 + 2;   // 10
+constexpr int kCBoxW = kTileC / 2 + 4;   // 36
+
+}  // namespace cp
