@@ -25,14 +25,15 @@
 // mass-flux-weighted total pressure minus the outlet patch's
 // (postprocessing.cpp:245-327).
 //
-// Adjoint: J_X^T lambda = dJ/dX, solved by defect correction
-//   lambda += P^{-1} (dJ/dX - J_X^T lambda)
-// with the exact transposed Jacobian product (every Newton term of the
-// upwind switches, SOU branches and face-velocity clamps) and a transposed
-// SIMPLE preconditioner P: Jacobi sweeps on the transposed Picard momentum
-// matrix, then a pressure-like correction whose operator
-// G^T diag(aP0)^-1 D^T equals the forward pressure-correction matrix, so the
-// same (multigrid) PCG kernel solves it.
+// Adjoint: J_X^T lambda = dJ/dX, solved by restarted flexible GMRES with
+// the exact transposed Jacobian product (every Newton term of the upwind
+// switches, SOU branches and face-velocity clamps) and a transposed SIMPLE
+// preconditioner P: Jacobi sweeps on the transposed Picard momentum matrix,
+// then a pressure-like correction whose operator G^T diag(aP0)^-1 D^T equals
+// the forward pressure-correction matrix, so the same (multigrid) PCG kernel
+// solves it.  The PCG runs a fixed number of iterations, which makes P
+// slightly different from one application to the next; the flexible variant
+// keeps the preconditioned directions and stays exact under that.
 // Gradient: dJ/dgamma = -lambda^T dR/dgamma, which is local: gamma enters R
 // only through alpha_face = (alpha(cL) + alpha(cR)) / 2 with
 // alpha(g) = alpha_max (1 - g) / (1 + q g + 1e-10) (SIMPLE.cpp:770);
@@ -371,8 +372,11 @@ __global__ void __launch_bounds__(1024) k_adj_g(AdjCtx a, AdjVecs V, double* Jou
     }
 }
 
-// r = g - y on all unknowns; partial sums of r^2 and g^2 per block into part[b*2]
-__global__ void k_adj_defect(KParams k, AdjVecs V, double* ru, double* rv, double* rp, double* part) {
+// r = gs g - ys y on all unknowns; partial sums of r^2 and g^2 per block
+// into part[b*2].  (gs, ys) = (1, 1): the adjoint residual; (0, -1): the
+// product y = J^T z restricted to the unknowns.
+__global__ void k_adj_defect(KParams k, AdjVecs V, double gs, double ys, double* ru, double* rv, double* rp,
+                             double* part) {
     __shared__ double sm[64];
     const Dims d = k.d;
     const int M = d.M, N = d.N;
@@ -381,17 +385,17 @@ __global__ void k_adj_defect(KParams k, AdjVecs V, double* ru, double* rv, doubl
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nU + nV + nP; t += gridDim.x * blockDim.x) {
         if (t < nU) {
             const size_t c = at(d, 1 + t / (N - 2), 1 + t % (N - 2));
-            const double r = V.gu[c] - V.yu[c];
+            const double r = gs * V.gu[c] - ys * V.yu[c];
             ru[c] = r; acc[0] += r * r; acc[1] += V.gu[c] * V.gu[c];
         } else if (t < nU + nV) {
             const int q = t - nU;
             const size_t c = at(d, 1 + q / (N - 1), 1 + q % (N - 1));
-            const double r = V.gv[c] - V.yv[c];
+            const double r = gs * V.gv[c] - ys * V.yv[c];
             rv[c] = r; acc[0] += r * r; acc[1] += V.gv[c] * V.gv[c];
         } else {
             const int q = t - nU - nV;
             const size_t c = at(d, 1 + q / (N - 2), 1 + q % (N - 2));
-            const double r = V.gp[c] - V.yp[c];
+            const double r = gs * V.gp[c] - ys * V.yp[c];
             rp[c] = r; acc[0] += r * r; acc[1] += V.gp[c] * V.gp[c];
         }
     }
@@ -448,9 +452,10 @@ __global__ void k_adj_prhs(KParams k, const double* du, const double* dv, const 
 
 // corrections: dm = dm* - D_A^-1 D^T dc with (D_A^-1 D^T dc)_u(i,j) =
 // rho dE(i,j) (dc(i,j+1) - dc(i,j)) and for v rho dN(i,j) (dc(i+1,j) - dc(i,j))
-// (dc zero outside the pressure unknowns); lambda += dm, lambda_c += pAlpha dc
-__global__ void k_adj_update(KParams k, AdjVecs V, const double* du, const double* dv, const double* dc,
-                             const double* dE, const double* dN, double relaxC) {
+// (dc zero outside the pressure unknowns); out = (dm, pAlpha dc) on the
+// U / V / continuity unknowns
+__global__ void k_adj_update(KParams k, const double* du, const double* dv, const double* dc, const double* dE,
+                             const double* dN, double relaxC, double* ou, double* ov, double* oc) {
     const Dims d = k.d;
     const int M = d.M, N = d.N;
     const int nU = (M - 1) * (N - 2), nV = (M - 2) * (N - 1), nP = (M - 1) * (N - 2);
@@ -462,18 +467,83 @@ __global__ void k_adj_update(KParams k, AdjVecs V, const double* du, const doubl
         if (t < nU) {
             const int i = 1 + t / (N - 2), j = 1 + t % (N - 2);
             const size_t c = at(d, i, j);
-            V.lu[c] += du[c] - k.rho * dE[c] * (C(i, j + 1) - C(i, j));
+            ou[c] = du[c] - k.rho * dE[c] * (C(i, j + 1) - C(i, j));
         } else if (t < nU + nV) {
             const int q = t - nU;
             const int i = 1 + q / (N - 1), j = 1 + q % (N - 1);
             const size_t c = at(d, i, j);
-            V.lv[c] += dv[c] - k.rho * dN[c] * (C(i + 1, j) - C(i, j));
+            ov[c] = dv[c] - k.rho * dN[c] * (C(i + 1, j) - C(i, j));
         } else {
             const int q = t - nU - nV;
             const int i = 1 + q / (N - 2), j = 1 + q % (N - 2);
-            V.lc[at(d, i, j)] += relaxC * dc[at(d, i, j)];
+            oc[at(d, i, j)] = relaxC * dc[at(d, i, j)];
         }
     }
+}
+
+// ---------------------------------------------------------------- Krylov vectors
+// A Krylov vector is three field-layout arrays (U, V, continuity) stored
+// back to back, L = 3 * nElem doubles; entries off the unknowns stay zero.
+constexpr int kKryMaxDots = 32;
+
+// part[b * 32 + q] = block b's share of <w, B_q>, q < nv, B_q = B + q L
+__global__ void __launch_bounds__(256) k_kry_mdot(const double* __restrict__ w, const double* __restrict__ B,
+                                                  size_t L, int nv, double* part) {
+    double acc[kKryMaxDots];
+#pragma unroll
+    for (int q = 0; q < kKryMaxDots; ++q) acc[q] = 0.0;
+    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < L; t += (size_t)gridDim.x * blockDim.x) {
+        const double wt = w[t];
+#pragma unroll
+        for (int q = 0; q < kKryMaxDots; ++q)
+            if (q < nv) acc[q] += B[q * L + t] * wt;
+    }
+    __shared__ double sm[8][kKryMaxDots];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q < kKryMaxDots; ++q) {
+        if (q < nv) {
+            double v = acc[q];
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if (lane == 0) sm[wid][q] = v;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < nv) {
+        double v = 0.0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); ++q) v += sm[q][threadIdx.x];
+        part[(size_t)blockIdx.x * kKryMaxDots + threadIdx.x] = v;
+    }
+}
+
+// out[q] = sum over blocks of part[b * 32 + q]; one block of 32 warps, warp q
+// sums entry q in a fixed order
+__global__ void __launch_bounds__(1024) k_kry_sum(const double* part, int nb, int nv, double* out) {
+    const int q = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (q >= nv) return;
+    double v = 0.0;
+    for (int b = lane; b < nb; b += 32) v += part[(size_t)b * kKryMaxDots + q];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) out[q] = v;
+}
+
+// w += sign * sum_q h[q] B_q
+__global__ void __launch_bounds__(256) k_kry_axpy(double* __restrict__ w, const double* __restrict__ B, size_t L,
+                                                  int nv, const double* __restrict__ h, double sign) {
+    __shared__ double hs[kKryMaxDots];
+    if (threadIdx.x < nv) hs[threadIdx.x] = sign * h[threadIdx.x];
+    __syncthreads();
+    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < L; t += (size_t)gridDim.x * blockDim.x) {
+        double a = w[t];
+        for (int q = 0; q < nv; ++q) a += hs[q] * B[q * L + t];
+        w[t] = a;
+    }
+}
+
+// dst = s * src
+__global__ void k_kry_scale(double* dst, const double* src, size_t L, double s) {
+    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < L; t += (size_t)gridDim.x * blockDim.x)
+        dst[t] = s * src[t];
 }
 
 // dJ/dgamma(cell a, b) = -sum over the faces the cell touches of

@@ -17,8 +17,14 @@
 //     bounded grid barriers; smaller levels run on CTA 0 alone with block
 //     barriers; the coarsest level (<= kMgDense unknowns) is solved with a
 //     dense inverse built once per pressure solve.
-// The CG recurrences, the stop rules (|p.Ap| < 1e-20, sqrt(r.r) < pTol) and
-// the returned count are those of pressure_solver.cpp:121-184.
+// The CG recurrences and the |p.Ap| < 1e-20 exit are those of
+// pressure_solver.cpp:121-184.  The convergence test is AMGCL's, since the
+// reference hands pTol and maxPressureIter to AMGCL's CG for these types
+// (pressure_solver.cpp:754-757, pressure_solver.cu:114-116): stop once
+// ||r|| <= pTol ||b|| (relative to the right-hand side, x0 = 0), and report
+// the number of completed iterations.  AMGCL (github.com/ddemidov/amgcl) is
+// not vendored with the reference (its directory there is empty), so this
+// follows AMGCL's published CG; its version is not pinned.
 #pragma once
 
 #include "cp_kernels.cuh"
@@ -345,6 +351,7 @@ __global__ void __launch_bounds__(512, 1) k_pcg_mg(KParams k, Status* st, const 
     } while (0)
 
     // ---- setup: level-0 operator (reference formulas), x = 0, r = b
+    double bb[1] = {0.0};
     for (int t = tid; t < n; t += nth) {
         const int i = 1 + t / w, j = 1 + t % w;
         const size_t c = at(d, i, j);
@@ -361,8 +368,15 @@ __global__ void __launch_bounds__(512, 1) k_pcg_mg(KParams k, Status* st, const 
         L0.dx[c] = (TV)extra;
         B.x[c] = (TV)0;
         B.r[c] = B.rhs[c];
+        bb[0] += (double)B.rhs[c] * (double)B.rhs[c];
     }
+    block_sum<1>(bb, sm);
+    if (threadIdx.x == 0) partA[blockIdx.x] = bb[0];
     MG_SYNC();
+    // partA is next written in the first CG iteration, after several grid barriers
+    double bnorm2[1];
+    sum_partials<1>(partA, G, 1, bnorm2, sm);
+    const double rTol = k.pTol * sqrt(bnorm2[0]);
     // ---- setup: coarse operators
     for (int l = 0; l < H.L - 1; ++l) {
         const bool cta = (l + 1) >= H.Lg;
@@ -603,7 +617,7 @@ __global__ void __launch_bounds__(512, 1) k_pcg_mg(KParams k, Status* st, const 
         double tB[2];
         sum_partials<2>(partB, G, 2, tB, sm);
         tick(MG_P_B, tp);
-        if (sqrt(tB[0]) < k.pTol) break;
+        if (sqrt(tB[0]) <= rTol) { ++it; break; }
         double rzn = 0.0;
         if (!vcycle(rzn)) return;
         beta = rzn / rz;

@@ -247,7 +247,9 @@ cp_status cp_pressure_noalloc(const cp_params* p, const double* dE, const double
  * reference has no flow adjoint.  grad receives dJ/dgamma for the Ny x Nx
  * cells (strides in elements).  The adjoint equations J_X^T lambda = dJ/dX
  * of the converged discretisation are solved by defect correction with a
- * transposed-SIMPLE preconditioner; iteration stops when
+ * transposed-SIMPLE preconditioner (transposed momentum Jacobi sweeps and a
+ * PCG solve of the pressure-like block, whose matrix is the forward pressure
+ * matrix); iteration stops when
  * ||dJ/dX - J_X^T lambda|| <= tol ||dJ/dX|| or after max_iter. */
 typedef struct cp_adjoint_report {
     int iterations;        /* defect-correction iterations run          */

@@ -56,7 +56,7 @@ def test_multigrid_pcg_solves_the_pressure_system(name, prec):
     dE, dN, uS, vS = o.get("dE"), o.get("dN"), o.get("uStar"), o.get("vStar")
     A, b, nI, nJ = pressure_system(dE, dN, uS, vS, 1000.0, case.hx, case.hy)
     x = spl.spsolve(A.tocsc(), b)
-    tol = 1e-13 * np.linalg.norm(b) if prec == "fp64" else 1e-7 * np.linalg.norm(b)
+    tol = 1e-13 if prec == "fp64" else 1e-7     # relative to ||b|| for types 2 / 4
     with gpu_for(case, pressureSolverType=4, maxPressureIter=200, pTol=tol, precision=prec) as g:
         for f, a in (("dE", dE), ("dN", dN), ("uStar", uS), ("vStar", vS)):
             g.set(f, a)
@@ -77,3 +77,30 @@ def test_multigrid_and_jacobi_pcg_reach_the_same_fixed_point():
             g.step(3000)
             out[t] = g.history()["fullTotal"][-1]
     assert abs(out[4] - out[1]) <= 1e-7 * abs(out[1]), out
+
+
+@pytest.mark.parametrize("ptol", [1e-3, 1e-6])
+def test_multigrid_pcg_stops_on_the_relative_residual(ptol):
+    """Types 2 / 4 take pTol as AMGCL's CG does: stop after the first
+    iteration with ||b - A x|| <= pTol ||b|| and report the iterations done."""
+    case = small_cases()["density"]
+    o = oracle_for(case)
+    o.run(15)
+    o.momentum(True)
+    o.momentum(False)
+    dE, dN, uS, vS = o.get("dE"), o.get("dN"), o.get("uStar"), o.get("vStar")
+    A, b, nI, nJ = pressure_system(dE, dN, uS, vS, 1000.0, case.hx, case.hy)
+
+    def solve(max_it):
+        with gpu_for(case, pressureSolverType=4, maxPressureIter=max_it, pTol=ptol, precision="fp64") as g:
+            for f, a in (("dE", dE), ("dN", dN), ("uStar", uS), ("vStar", vS)):
+                g.set(f, a)
+            it, _ = g.solvePressureSystem()
+            x = g.get("pStar")[1:-1, 1:-2].reshape(-1)
+        return it, np.linalg.norm(b - A @ x) / np.linalg.norm(b)
+
+    it, rel = solve(200)
+    assert 1 <= it < 200 and rel <= ptol * 1.001, (it, rel)
+    if it > 1:
+        it2, rel2 = solve(it - 1)
+        assert it2 == it - 1 and rel2 > ptol * 0.999, (it2, rel2)
