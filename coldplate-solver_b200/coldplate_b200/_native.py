@@ -82,6 +82,11 @@ class CpAdjointReport(ctypes.Structure):
                 ("J", ctypes.c_double), ("device_ms", ctypes.c_double)]
 
 
+class CpBatchReport(ctypes.Structure):
+    _fields_ = [("outerIterations", ctypes.c_int), ("fieldsDone", ctypes.c_int), ("launches", ctypes.c_int),
+                ("tileRows", ctypes.c_int), ("tileCols", ctypes.c_int), ("device_ms", ctypes.c_double)]
+
+
 # history row columns (cp_device.cuh HistCol)
 HIST_COLS = ("iter", "error", "residU_RMS", "residV_RMS", "residMass_RMS", "residU_max", "residV_max",
              "residMass_max", "pIters", "coreTotal", "fullTotal", "coreStatic", "fullStatic",
@@ -111,6 +116,11 @@ SIGNATURES = {
     "cp_momentum_v": (_I, [_vp, _dp, _ip]),
     "cp_pressure": (_I, [_vp, _ip, _dp]),
     "cp_adjoint_dp_dgamma": (_I, [_vp, _dp, _L, _L, _L, _L, _I, _D, ctypes.POINTER(CpAdjointReport)]),
+    "cp_batch_create": (_I, [ctypes.POINTER(_vp), _I, ctypes.POINTER(_vp)]),
+    "cp_batch_destroy": (_I, [_vp]),
+    "cp_batch_set_tile": (_I, [_vp, _I, _I]),
+    "cp_batch_run": (_I, [_vp, _I, ctypes.POINTER(CpBatchReport)]),
+    "cp_batch_autotune": (_I, [_vp, _I, ctypes.POINTER(CpBatchReport)]),
     "cp_history_columns": (_I, []),
     "cp_get_history": (_I, [_vp, _dp, _I, _ip]),
     "cp_status_string": (ctypes.c_char_p, [_I]),

@@ -190,3 +190,51 @@ class Simple:
         it, r = ctypes.c_int(), ctypes.c_double()
         nat.check(self._lib.cp_pressure(self._h, ctypes.byref(it), ctypes.byref(r)))
         return it.value, r.value
+
+
+class Batch:
+    """Several ``Simple`` fields (grid sizes, geometries and inlet velocities
+    may all differ) advanced together by one persistent kernel per launch
+    (cp_batch_run).  Each field keeps its own stop rules, history and state:
+    after ``run`` read results from the ``Simple`` objects as usual.  The
+    fields must use pressureSolverType 2 or 4 and one precision, and must
+    stay open while the batch exists."""
+
+    def __init__(self, fields: list[Simple]):
+        self._lib = nat.lib()
+        self.fields = list(fields)
+        arr = (ctypes.c_void_p * len(self.fields))(*[f._h.value for f in self.fields])
+        h = ctypes.c_void_p()
+        nat.check(self._lib.cp_batch_create(arr, len(self.fields), ctypes.byref(h)))
+        self._h = h
+
+    def set_tile(self, rows: int, cols: int) -> None:
+        nat.check(self._lib.cp_batch_set_tile(self._h, int(rows), int(cols)))
+
+    def autotune(self, trial_outer: int = 4) -> dict:
+        """Pick the fastest cell tile on trial_outer iterations; resets every field."""
+        r = nat.CpBatchReport()
+        nat.check(self._lib.cp_batch_autotune(self._h, int(trial_outer), ctypes.byref(r)))
+        return {name: getattr(r, name) for name, _ in r._fields_}
+
+    def run(self, max_outer: int) -> dict:
+        r = nat.CpBatchReport()
+        nat.check(self._lib.cp_batch_run(self._h, int(max_outer), ctypes.byref(r)))
+        return {name: getattr(r, name) for name, _ in r._fields_}
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None and self._h.value:
+            self._lib.cp_batch_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

@@ -680,8 +680,9 @@ struct FinalizeArgs {
     double* dpWin;         // [dpWindow]
 };
 
-__global__ void __launch_bounds__(1024) k_finalize(KParams k, Status* st, FinalizeArgs a) {
-    if (st->done) return;
+// One block: residual norms from the k_mass partials, the four pressure
+// samples, the history row and the stop rules of one field.
+__device__ __forceinline__ void finalize_block(const KParams& k, Status* st, const FinalizeArgs& a) {
     __shared__ double sm[32 * 5];
     __shared__ double met[4][5];
     double sums[4];
@@ -777,6 +778,11 @@ __global__ void __launch_bounds__(1024) k_finalize(KParams k, Status* st, Finali
     if (!done && iter + 1 >= k.maxIterations) { done = 1; reason = CP_STOP_MAX_ITER; }
     st->iter = iter + 1;
     if (done) { st->reason = reason; __threadfence(); st->done = 1; }
+}
+
+__global__ void __launch_bounds__(1024) k_finalize(KParams k, Status* st, FinalizeArgs a) {
+    if (st->done) return;
+    finalize_block(k, st, a);
 }
 
 }  // namespace cp

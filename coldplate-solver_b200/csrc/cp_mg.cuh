@@ -167,14 +167,14 @@ __device__ __forceinline__ void mg_restrict0_cell(const MgLevel<TV>& f, const Mg
     c.x[q] = (TV)(omega * s / (double)c.d[q]);
 }
 
-// prolongation into level 0 + one Jacobi sweep: x' = x0 + P e, y = x' + omega (b - A x') / d
+// prolongation into level 0 + one Jacobi sweep: x' = x0 + s P e, y = x' + omega (b - A x') / d
 template <typename TV>
 __device__ __forceinline__ TV mg_prolong0_cell(const MgLevel<TV>& f, const MgLevel<TV>& c, const TV* e, int i,
-                                               int j, double omega) {
-    const TV om = (TV)omega;
+                                               int j, double omega, double c_scale) {
+    const TV om = (TV)omega, sc = (TV)c_scale;
     auto xp = [&](int ii, int jj) -> TV {
         if (ii < 1 || ii > f.nI || jj < 1 || jj > f.nJ) return (TV)0;
-        return l0_x(f, lidx(f, ii, jj), om) + e[lidx(c, (ii + 1) >> 1, (jj + 1) >> 1)];
+        return l0_x(f, lidx(f, ii, jj), om) + sc * e[lidx(c, (ii + 1) >> 1, (jj + 1) >> 1)];
     };
     const size_t q = lidx(f, i, j);
     const TV xc = xp(i, j);

@@ -23,6 +23,7 @@
 #include "cp_kernels.cuh"
 #include "cp_mg.cuh"
 #include "cp_adjoint.cuh"
+#include "cp_batch.cuh"
 
 using namespace cp;
 
@@ -1404,3 +1405,342 @@ extern "C" cp_status cp_pressure_noalloc(const cp_params* p, const double* dE, c
     if (residMass) *residMass = hs.lastError;
     return CP_OK;
 }
+
+// ======================================================================== batched solves
+// cp_batch: the fields of several contexts advanced by one persistent
+// cooperative kernel (k_batch).  The batch keeps only the per-field
+// descriptors, the tile tables and the scratch of the shared reductions;
+// every field's buffers stay in its own context.
+struct cp_batch {
+    std::vector<cp_ctx*> f;
+    int dev = 0, numSMs = 0, grid = 0;
+    bool mixed = false;
+    int R = 16, C = 64;
+    int maxLg = 1, maxMom = 0, maxP = 0;
+    size_t partCap = 0;          // tiles of level 0 the partial array holds
+    void* dF = nullptr;          // BField<TC>[n]
+    int* dToff = nullptr;
+    BState* dBs = nullptr;
+    double* dPart = nullptr;
+    unsigned* dBar = nullptr;
+    int* dErr = nullptr;
+    int* dAllDone = nullptr;
+    int* hFlags = nullptr;       // pinned: allDone, err
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    int graphOuter = 0;
+    std::vector<void*> allocs;
+};
+
+namespace {
+
+constexpr int kBatchChunk = 64;   // outer iterations per launch
+// tile shapes the autotuner tries (rows x columns)
+constexpr int kBatchTiles[][2] = {{16, 64}, {8, 128}, {32, 32}, {4, 256}, {8, 64}, {16, 32},
+                                  {16, 128}, {32, 64}, {8, 256}};
+constexpr size_t kBatchDynSmem = kMgDenseSmem;
+
+size_t batch_tiles0(const cp_batch* b, int R, int C) {
+    size_t t = 0;
+    for (cp_ctx* c : b->f)
+        t += (size_t)((c->d.M - 1 + R - 1) / R) * (size_t)((c->d.N - 1 + C - 1) / C);
+    return t;
+}
+
+// first tile of every field per level: level 0 tiles the (M-1) x (N-1)
+// cells, level l >= 1 its nI x nJ unknowns where the field runs level l
+// grid-wide or restricts into it (l <= Lg)
+std::vector<int> batch_toff(const cp_batch* b, int R, int C) {
+    const int n = (int)b->f.size();
+    std::vector<int> t((size_t)(b->maxLg + 1) * (n + 1), 0);
+    for (int l = 0; l <= b->maxLg; ++l) {
+        int acc = 0;
+        for (int q = 0; q < n; ++q) {
+            const cp_ctx* c = b->f[q];
+            t[(size_t)l * (n + 1) + q] = acc;
+            int nI = 0, nJ = 0;
+            if (l == 0) { nI = c->d.M - 1; nJ = c->d.N - 1; }
+            else if (l <= c->mgLg && l < c->mgL) { nI = c->mgNI[l]; nJ = c->mgNJ[l]; }
+            acc += ((nI + R - 1) / R) * ((nJ + C - 1) / C);
+        }
+        t[(size_t)l * (n + 1) + n] = acc;
+    }
+    return t;
+}
+
+template <typename TC>
+BField<TC> batch_field(cp_ctx* c) {
+    BField<TC> bf;
+    memset(&bf, 0, sizeof(bf));
+    bf.k = c->k;
+    bf.st = c->st;
+    bf.u = c->u; bf.v = c->v; bf.p = c->p; bf.uStar = c->uStar; bf.vStar = c->vStar; bf.pStar = c->pStar;
+    bf.dE = c->dE; bf.dN = c->dN; bf.alpha = c->alpha; bf.gamma = c->gamma;
+    bf.U = mom_sys<TC>(c, 0);
+    bf.V = mom_sys<TC>(c, 1);
+    bf.xU0 = (TC*)c->xb[0]; bf.xU1 = (TC*)c->xb[1]; bf.xV0 = (TC*)c->xb[2]; bf.xV1 = (TC*)c->xb[3];
+    bf.B = pcg_bufs<TC>(c);
+    bf.H = mg_hier<TC>(c);
+    bf.H.prof = nullptr;
+    bf.hist = c->hist; bf.histCap = c->histCap; bf.dpWin = c->dpWin;
+    return bf;
+}
+
+cp_status batch_balloc(cp_batch* b, void** p, size_t bytes) {
+    CK(cudaMalloc(p, std::max<size_t>(bytes, 1)));
+    b->allocs.push_back(*p);
+    CK(cudaMemsetAsync(*p, 0, std::max<size_t>(bytes, 1), b->stream));
+    return CP_OK;
+}
+
+cp_status batch_set_tile(cp_batch* b, int R, int C) {
+    if (R < 1 || C < 1 || R * C < 256 || R * C > 4096)
+        return fail(CP_ERR_BAD_PARAM, "tile %d x %d: rows x cols must lie in [256, 4096]", R, C);
+    if (batch_tiles0(b, R, C) > b->partCap)
+        return fail(CP_ERR_BAD_PARAM, "tile %d x %d: more tiles than the batch was sized for", R, C);
+    std::vector<int> t = batch_toff(b, R, C);
+    CK(cudaMemcpyAsync(b->dToff, t.data(), t.size() * sizeof(int), cudaMemcpyHostToDevice, b->stream));
+    CK(cudaStreamSynchronize(b->stream));
+    b->R = R;
+    b->C = C;
+    if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; }
+    return CP_OK;
+}
+
+template <typename TC, bool Mixed>
+cp_status batch_launch(cp_batch* b, int nOuter) {
+    BatchArgs a{};
+    a.nf = (int)b->f.size();
+    a.R = b->R; a.C = b->C;
+    a.maxLg = b->maxLg; a.maxMom = b->maxMom; a.maxP = b->maxP;
+    a.nOuter = nOuter;
+    a.toff = b->dToff; a.bs = b->dBs; a.ipart = b->dPart; a.bar = b->dBar; a.err = b->dErr;
+    a.allDone = b->dAllDone;
+    CK(cudaMemsetAsync(b->dBar, 0, sizeof(unsigned), b->stream));
+    CK(launch_coop_cfg(k_batch<TC, Mixed>, b->grid, kBatchThreads, kBatchDynSmem, b->stream, a,
+                       (const BField<TC>*)b->dF));
+    return CP_OK;
+}
+
+cp_status batch_launch_any(cp_batch* b, int nOuter) {
+    return b->mixed ? batch_launch<float, true>(b, nOuter) : batch_launch<double, false>(b, nOuter);
+}
+
+// one graph of [barrier reset, k_batch(nOuter)], replayed per chunk
+cp_status batch_graph(cp_batch* b, int nOuter) {
+    if (b->graph && b->graphOuter == nOuter) return CP_OK;
+    if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; }
+    cudaGraph_t g = nullptr;
+    if (cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        cudaGetLastError();
+        return CP_OK;
+    }
+    cp_status s = batch_launch_any(b, nOuter);
+    cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+    if (s != CP_OK || e != cudaSuccess || !g) {
+        cudaGetLastError();
+        if (g) cudaGraphDestroy(g);
+        g_err.clear();
+        return CP_OK;   // launched directly instead
+    }
+    cudaGraphExec_t ex = nullptr;
+    e = cudaGraphInstantiate(&ex, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return CP_OK;
+    }
+    b->graph = ex;
+    b->graphOuter = nOuter;
+    return CP_OK;
+}
+
+template <typename TC>
+cp_status batch_upload_fields(cp_batch* b) {
+    std::vector<BField<TC>> h;
+    for (cp_ctx* c : b->f) h.push_back(batch_field<TC>(c));
+    CK(cudaMemcpyAsync(b->dF, h.data(), h.size() * sizeof(BField<TC>), cudaMemcpyHostToDevice, b->stream));
+    CK(cudaStreamSynchronize(b->stream));
+    return CP_OK;
+}
+
+cp_status batch_sync_fields(cp_batch* b) {
+    for (cp_ctx* c : b->f) CK(cudaStreamSynchronize(c->stream));
+    return CP_OK;
+}
+
+// run up to max_outer outer iterations (every field stops on its own rules
+// before that); rep gets the totals
+cp_status batch_run(cp_batch* b, int max_outer, cp_batch_report* rep, bool useGraph) {
+    cp_status s = batch_sync_fields(b);
+    if (s != CP_OK) return s;
+    CK(cudaMemsetAsync(b->dErr, 0, sizeof(int), b->stream));
+    CK(cudaMemsetAsync(b->dAllDone, 0, sizeof(int), b->stream));
+    CK(cudaEventRecord(b->ev0, b->stream));
+    int done = 0, launches = 0;
+    bool all = false;
+    while (done < max_outer && !all) {
+        const int n = std::min(kBatchChunk, max_outer - done);
+        if (useGraph && n == kBatchChunk) {
+            if ((s = batch_graph(b, n)) != CP_OK) return s;
+        }
+        if (useGraph && b->graph && b->graphOuter == n) CK(cudaGraphLaunch(b->graph, b->stream));
+        else if ((s = batch_launch_any(b, n)) != CP_OK) return s;
+        ++launches;
+        done += n;
+        CK(cudaMemcpyAsync(b->hFlags, b->dAllDone, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
+        CK(cudaMemcpyAsync(b->hFlags + 1, b->dErr, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
+        CK(cudaStreamSynchronize(b->stream));
+        if (b->hFlags[1] != 0)
+            return fail((cp_status)b->hFlags[1], "device reported %s in the batch",
+                        cp_status_string((cp_status)b->hFlags[1]));
+        all = b->hFlags[0] != 0;
+    }
+    CK(cudaEventRecord(b->ev1, b->stream));
+    CK(cudaEventSynchronize(b->ev1));
+    if (rep) {
+        memset(rep, 0, sizeof(*rep));
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, b->ev0, b->ev1);
+        rep->device_ms = ms;
+        rep->launches = launches;
+        rep->tileRows = b->R;
+        rep->tileCols = b->C;
+        int maxIt = 0, nd = 0;
+        for (cp_ctx* c : b->f) {
+            CK(cudaMemcpy(c->stHost, c->st, sizeof(Status), cudaMemcpyDeviceToHost));
+            maxIt = std::max(maxIt, c->stHost->iter);
+            nd += c->stHost->done ? 1 : 0;
+        }
+        rep->outerIterations = maxIt;
+        rep->fieldsDone = nd;
+    }
+    return CP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+cp_status cp_batch_create(cp_ctx* const* fields, int n, cp_batch** out) {
+    if (!fields || !out) return fail(CP_ERR_BAD_PARAM, "NULL argument");
+    *out = nullptr;
+    if (n < 1 || n > kBatchMaxFields) return fail(CP_ERR_BAD_PARAM, "batch of %d fields (1..%d)", n, kBatchMaxFields);
+    for (int q = 0; q < n; ++q) {
+        cp_ctx* c = fields[q];
+        if (!c) return fail(CP_ERR_BAD_PARAM, "field %d is NULL", q);
+        for (int r = 0; r < q; ++r)
+            if (fields[r] == c) return fail(CP_ERR_BAD_PARAM, "field %d repeats field %d", q, r);
+        if (!c->useMg)
+            return fail(CP_ERR_UNSUPPORTED, "field %d: batches run pressureSolverType 2 or 4 (multigrid-PCG)", q);
+        if (c->prm.precision != fields[0]->prm.precision)
+            return fail(CP_ERR_BAD_PARAM, "field %d: every field of a batch needs the same precision", q);
+        if (c->dev != fields[0]->dev) return fail(CP_ERR_BAD_PARAM, "field %d is on another device", q);
+        if (c->mgLg + 1 > kBatchMaxLevels) return fail(CP_ERR_BAD_PARAM, "field %d: grid too large for a batch", q);
+    }
+    cp_batch* b = new cp_batch();
+    b->f.assign(fields, fields + n);
+    b->dev = fields[0]->dev;
+    b->numSMs = fields[0]->numSMs;
+    b->mixed = fields[0]->prm.precision == CP_PREC_MIXED;
+    for (cp_ctx* c : b->f) {
+        b->maxLg = std::max(b->maxLg, c->mgLg);
+        b->maxMom = std::max(b->maxMom, c->k.maxMom);
+        b->maxP = std::max(b->maxP, c->k.maxP);
+    }
+    auto bail = [&](cp_status s) {
+        std::string keep = g_err;
+        cp_batch_destroy(b);
+        g_err = keep;
+        return s;
+    };
+    cp_status s = CP_OK;
+    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess ||
+        cudaMallocHost(&b->hFlags, 2 * sizeof(int)) != cudaSuccess)
+        return bail(fail(CP_ERR_CUDA, "batch stream / events / pinned flags"));
+    // one block per SM: the kernel must fit with its dense set-up workspace
+    int nb = 0;
+    if (b->mixed) {
+        cudaFuncSetAttribute(k_batch<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBatchDynSmem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_batch<float, true>, kBatchThreads, kBatchDynSmem);
+    } else {
+        cudaFuncSetAttribute(k_batch<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)kBatchDynSmem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_batch<double, false>, kBatchThreads, kBatchDynSmem);
+    }
+    if (nb < 1) return bail(fail(CP_ERR_CUDA, "the batch kernel does not fit on an SM"));
+    b->grid = b->numSMs;
+    for (const auto& t : kBatchTiles) b->partCap = std::max(b->partCap, batch_tiles0(b, t[0], t[1]));
+    const size_t nt = (size_t)(b->maxLg + 1) * (n + 1);
+    const size_t fbytes = b->mixed ? sizeof(BField<float>) : sizeof(BField<double>);
+    if ((s = batch_balloc(b, &b->dF, fbytes * n)) != CP_OK) return bail(s);
+    if ((s = batch_balloc(b, (void**)&b->dToff, nt * sizeof(int))) != CP_OK) return bail(s);
+    if ((s = batch_balloc(b, (void**)&b->dBs, (size_t)n * sizeof(BState))) != CP_OK) return bail(s);
+    if ((s = batch_balloc(b, (void**)&b->dPart, b->partCap * kBatchPartStride * sizeof(double))) != CP_OK)
+        return bail(s);
+    if ((s = batch_balloc(b, (void**)&b->dBar, sizeof(unsigned))) != CP_OK) return bail(s);
+    if ((s = batch_balloc(b, (void**)&b->dErr, sizeof(int))) != CP_OK) return bail(s);
+    if ((s = batch_balloc(b, (void**)&b->dAllDone, sizeof(int))) != CP_OK) return bail(s);
+    s = b->mixed ? batch_upload_fields<float>(b) : batch_upload_fields<double>(b);
+    if (s != CP_OK) return bail(s);
+    if ((s = batch_set_tile(b, b->R, b->C)) != CP_OK) return bail(s);
+    *out = b;
+    return CP_OK;
+}
+
+cp_status cp_batch_destroy(cp_batch* b) {
+    if (!b) return CP_OK;
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    for (void* q : b->allocs) cudaFree(q);
+    if (b->hFlags) cudaFreeHost(b->hFlags);
+    if (b->ev0) cudaEventDestroy(b->ev0);
+    if (b->ev1) cudaEventDestroy(b->ev1);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+    return CP_OK;
+}
+
+cp_status cp_batch_set_tile(cp_batch* b, int rows, int cols) {
+    if (!b) return fail(CP_ERR_BAD_PARAM, "batch is NULL");
+    return batch_set_tile(b, rows, cols);
+}
+
+cp_status cp_batch_run(cp_batch* b, int max_outer, cp_batch_report* rep) {
+    if (!b) return fail(CP_ERR_BAD_PARAM, "batch is NULL");
+    if (max_outer < 0) return fail(CP_ERR_BAD_PARAM, "max_outer < 0");
+    return batch_run(b, max_outer, rep, true);
+}
+
+cp_status cp_batch_autotune(cp_batch* b, int trial_outer, cp_batch_report* best) {
+    if (!b) return fail(CP_ERR_BAD_PARAM, "batch is NULL");
+    if (trial_outer < 1) return fail(CP_ERR_BAD_PARAM, "trial_outer >= 1 required");
+    double bestMs = -1.0;
+    int bR = b->R, bC = b->C;
+    for (const auto& t : kBatchTiles) {
+        if (batch_tiles0(b, t[0], t[1]) > b->partCap) continue;
+        cp_status s = batch_set_tile(b, t[0], t[1]);
+        if (s != CP_OK) return s;
+        for (cp_ctx* c : b->f)
+            if ((s = cp_reset(c)) != CP_OK) return s;
+        cp_batch_report r;
+        if ((s = batch_run(b, trial_outer, &r, false)) != CP_OK) return s;
+        if (bestMs < 0.0 || r.device_ms < bestMs) { bestMs = r.device_ms; bR = t[0]; bC = t[1]; }
+    }
+    cp_status s = batch_set_tile(b, bR, bC);
+    if (s != CP_OK) return s;
+    for (cp_ctx* c : b->f)
+        if ((s = cp_reset(c)) != CP_OK) return s;
+    if (best) {
+        memset(best, 0, sizeof(*best));
+        best->tileRows = bR;
+        best->tileCols = bC;
+        best->device_ms = bestMs;
+        best->outerIterations = trial_outer;
+    }
+    return CP_OK;
+}
+
+}  // extern "C"

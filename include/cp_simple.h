@@ -284,6 +284,36 @@ typedef struct cp_kernel_timing {
 } cp_kernel_timing;
 cp_status cp_kernel_times(cp_ctx* ctx, int n_outer, cp_kernel_timing* out);
 
+/* ---------------------------------------------------------------- batches
+ * New (the reference runs one field per process, run_solvers.py:248): many
+ * fields, each its own context with its own grid size, geometry and
+ * parameters, advanced together by one persistent cooperative kernel per
+ * launch.  Every phase of the outer iteration covers the rows x cols cell
+ * tiles of all fields still iterating; each field keeps its own stop rules
+ * (Jacobi, CG and outer loop), history and status, so cp_get_field,
+ * cp_get_history and cp_adjoint_dp_dgamma work on a field's context after a
+ * batch run as after cp_step.  Requirements: pressureSolverType 2 or 4, the
+ * same precision for every field, contexts on one device.  The contexts must
+ * outlive the batch and must not be stepped while a batch call runs. */
+typedef struct cp_batch cp_batch;
+typedef struct cp_batch_report {
+    int outerIterations;   /* largest completed outer iteration count     */
+    int fieldsDone;        /* fields whose loop has stopped               */
+    int launches;          /* persistent-kernel launches (64 iterations each at most) */
+    int tileRows, tileCols;/* cell tile used                              */
+    double device_ms;      /* device time of the call (CUDA events)       */
+} cp_batch_report;
+cp_status cp_batch_create(cp_ctx* const* fields, int n, cp_batch** out);
+cp_status cp_batch_destroy(cp_batch* batch);
+/* rows x cols in [256, 4096]; the default is 16 x 64 */
+cp_status cp_batch_set_tile(cp_batch* batch, int rows, int cols);
+/* Runs until every field has stopped or max_outer iterations, in launches of
+ * up to 64 outer iterations replayed from a captured CUDA graph. */
+cp_status cp_batch_run(cp_batch* batch, int max_outer, cp_batch_report* rep);
+/* Times trial_outer iterations from the initial state for each candidate tile
+ * shape, keeps the fastest, and resets every field (cp_reset) afterwards. */
+cp_status cp_batch_autotune(cp_batch* batch, int trial_outer, cp_batch_report* best);
+
 const char* cp_status_string(cp_status s);
 const char* cp_last_error_string(void);
 

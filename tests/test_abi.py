@@ -66,11 +66,14 @@ def _c_offsets(struct_name, fields):
     return [int(x) for x in out]
 
 
-@pytest.mark.parametrize("which", ["params", "report"])
+@pytest.mark.parametrize("which", ["params", "report", "adjoint", "batch", "timing"])
 def test_ctypes_layout_matches_c(which):
     from coldplate_b200 import _native as nat
-    cls, name, fields = ((nat.CpParams, "cp_params", nat.PARAM_FIELDS) if which == "params"
-                         else (nat.CpIterReport, "cp_iter_report", nat.REPORT_FIELDS))
+    cls, name = {"params": (nat.CpParams, "cp_params"), "report": (nat.CpIterReport, "cp_iter_report"),
+                 "adjoint": (nat.CpAdjointReport, "cp_adjoint_report"),
+                 "batch": (nat.CpBatchReport, "cp_batch_report"),
+                 "timing": (nat.CpKernelTiming, "cp_kernel_timing")}[which]
+    fields = cls._fields_
     c = _c_offsets(name, [f for f, _ in fields])
     assert c[0] == ctypes.sizeof(cls)
     assert c[1:] == [getattr(cls, f).offset for f, _ in fields]
