@@ -63,3 +63,4 @@ def test_autograd_function():
         s.step(4000)
         g2, _ = s.adjoint_dp_dgamma(tol=1e-10)
     np.testing.assert_allclose(gamma.grad.numpy(), g2, rtol=1e-6, atol=1e-9 * np.abs(g2).max())
+
