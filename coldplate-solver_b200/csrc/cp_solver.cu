@@ -83,7 +83,10 @@ struct cp_ctx {
     int mgNI[kMgMaxLevels] = {}, mgNJ[kMgMaxLevels] = {}, mgP[kMgMaxLevels] = {};
     void* mgArr[kMgMaxLevels][7] = {};   // fE fN d dx x y b
     void* mgDense = nullptr;
-    double mgOmega = 0.8;
+    // Jacobi damping of the V-cycle smoother: with the 1.8 coarse scale,
+    // 0.9 reaches pTol 1e-6 in 29 CG iterations at 2048 x 1024 against 32 at
+    // 0.8 and 38 at 0.7 (measured)
+    double mgOmega = 0.9;
     // Scaling of the coarse-grid correction.  Piecewise-constant aggregation
     // under-corrects smooth error; an over-correction s in (0, 2) keeps the
     // V-cycle symmetric positive definite.  On the 2048 x 1024 density
@@ -369,7 +372,9 @@ cp_status mg_build(cp_ctx* c) {
     }
     c->mgL = L;
     int Lg = 1;
-    while (Lg < L && (long long)c->mgNI[Lg] * c->mgNJ[Lg] > kMgCtaCells) ++Lg;
+    long long ctaCells = kMgCtaCells;
+    if (const char* e = getenv("CP_MG_CTA_CELLS")) ctaCells = std::max(atoll(e), 1LL);
+    while (Lg < L && (long long)c->mgNI[Lg] * c->mgNJ[Lg] > ctaCells) ++Lg;
     c->mgLg = Lg;
     // level 0 shares the field layout and the PCG face / diagonal arrays
     c->mgP[0] = c->d.P;
