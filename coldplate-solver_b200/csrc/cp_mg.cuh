@@ -55,6 +55,9 @@ struct MgHier {
 };
 
 enum MgPhase { MG_P_SETUP = 0, MG_P_A, MG_P_B, MG_P_DOWN, MG_P_CTA, MG_P_UP, MG_P_COUNT };
+// per-level timers follow the phase timers: restriction out of level l at
+// MG_P_COUNT + l, prolongation into level l at MG_P_COUNT + kMgMaxLevels + l
+constexpr int kMgProfSlots = MG_P_COUNT + 2 * kMgMaxLevels;
 
 // ---------------------------------------------------------------- level ops
 template <typename TV>
@@ -267,7 +270,7 @@ __device__ void mg_cta_cycle(const MgHier<TV>& H) {
 // ---------------------------------------------------------------- TMA tiles of level 0
 // Tensor maps of the arrays the level-0 phases read (built per context).
 struct MgMaps {
-    CUtensorMap z, pa, pb, r, d, fE, fN, e1;
+    CUtensorMap z, pa, pb, r, d, fE, fN, e1, x0;
 };
 
 // Depth of the TMA pipeline of the level-0 tile phases: up to kTmaStages
@@ -280,7 +283,7 @@ template <typename TV>
 struct TileSmem {
     static constexpr int kBox = ((kBoxR * kBoxW * (int)sizeof(TV) + 127) / 128) * 128;
     static constexpr int kCBox = ((kCBoxR * kCBoxW * (int)sizeof(TV) + 127) / 128) * 128;
-    static constexpr int kStage = 5 * kBox;   // up to five boxes per stage
+    static constexpr int kStage = 6 * kBox;   // up to five fine boxes and a coarse one per stage
     static constexpr int kBytes = kTmaStages * kStage;
 };
 
@@ -369,11 +372,14 @@ __global__ void __launch_bounds__(512, 1) k_pcg_mg(KParams k, Status* st, const 
         if (aP < 1e-20) { extra = 1.0 - aP; aP = 1.0; }
         B.fE[c] = (TV)aE;
         if (i < M - 1) B.fN[c] = (TV)aN;
-        B.d[c] = (TV)aP;
+        const TV dt = (TV)aP;
+        B.d[c] = dt;
         L0.dx[c] = (TV)extra;
         B.x[c] = (TV)0;
-        B.r[c] = B.rhs[c];
-        bb[0] += (double)B.rhs[c] * (double)B.rhs[c];
+        const TV rt = B.rhs[c];
+        B.r[c] = rt;
+        L0.x[c] = (TV)om * rt / dt;   // pre-smoothed level-0 iterate omega r / d
+        bb[0] += (double)rt * (double)rt;
     }
     block_sum<1>(bb, sm);
     if (threadIdx.x == 0) partA[blockIdx.x] = bb[0];
@@ -423,14 +429,12 @@ __global__ void __launch_bounds__(512, 1) k_pcg_mg(KParams k, Status* st, const 
     };
     // smem element (li, lj) of a fine box: array row i0 - 1 + li, column j0 - 1 + lj
 #define SB(q, li, lj) (bx[q][(li) * kBoxW + (lj)])
-    // level-0 pre-smoothed iterate omega r / d in the box
-    auto x0s = [&](TV* const* bx, int li, int lj) -> TV {
-        const TV dd = SB(1, li, lj);
-        return dd != (TV)0 ? omT * SB(0, li, lj) / dd : (TV)0;
-    };
-    // restriction of the level-0 residual into level 1 (boxes: r, d, fE, fN)
+    // The level-0 pre-smoothed iterate x0 = omega r / d is stored (L0.x) by
+    // the set-up and by every CG update, and read as a box: one division per
+    // unknown per CG iteration instead of one per stencil point.
+    // restriction of the level-0 residual into level 1 (boxes: r, x0, fE, fN)
     auto restrict0_tiles = [&]() -> bool {
-        const CUtensorMap* mp[4] = {&maps.r, &maps.d, &maps.fE, &maps.fN};
+        const CUtensorMap* mp[4] = {&maps.r, &maps.x0, &maps.fE, &maps.fN};
         const MgLevel<TV>& C1 = H.lv[1];
         return tile_loop(ntiles, tbar, tpar, &st->err,
                          [&](int t, int s) { issue_fine(t, s, mp, 4, false); },
@@ -448,9 +452,9 @@ __global__ void __launch_bounds__(512, 1) k_pcg_mg(KParams k, Status* st, const 
                     const int b = 2 * ccol + q;
                     if (i0 + a <= nI0 && j0 + b <= nJ0) {
                         const int li = a + 1, lj = b + 1;
-                        const TV r = ((TV)1 - omT) * SB(0, li, lj) + SB(2, li, lj) * x0s(bx, li, lj + 1) +
-                                     SB(2, li, lj - 1) * x0s(bx, li, lj - 1) + SB(3, li, lj) * x0s(bx, li + 1, lj) +
-                                     SB(3, li - 1, lj) * x0s(bx, li - 1, lj);
+                        const TV r = ((TV)1 - omT) * SB(0, li, lj) + SB(2, li, lj) * SB(1, li, lj + 1) +
+                                     SB(2, li, lj - 1) * SB(1, li, lj - 1) + SB(3, li, lj) * SB(1, li + 1, lj) +
+                                     SB(3, li - 1, lj) * SB(1, li - 1, lj);
                         sum += (double)r;
                     }
                 }
@@ -465,16 +469,16 @@ __global__ void __launch_bounds__(512, 1) k_pcg_mg(KParams k, Status* st, const 
         });
     };
     // prolongation from level 1 + post-smoothing of level 0 (boxes: r, d,
-    // fE, fN and the coarse correction); writes z = L0.y, accumulates r.z
+    // fE, fN, x0 and the coarse correction); writes z = L0.y, accumulates r.z
     const TV scT = (TV)H.scale;
     auto prolong0_tiles = [&](double& rzacc) -> bool {
-        const CUtensorMap* mp[4] = {&maps.r, &maps.d, &maps.fE, &maps.fN};
+        const CUtensorMap* mp[5] = {&maps.r, &maps.d, &maps.fE, &maps.fN, &maps.x0};
         const MgLevel<TV>& F0 = H.lv[0];
         return tile_loop(ntiles, tbar, tpar, &st->err,
-                         [&](int t, int s) { issue_fine(t, s, mp, 4, true); },
+                         [&](int t, int s) { issue_fine(t, s, mp, 5, true); },
                          [&](int t, int s) {
-            TV* bx[4] = {box(s, 0), box(s, 1), box(s, 2), box(s, 3)};
-            const TV* ce = box(s, 4);
+            TV* bx[5] = {box(s, 0), box(s, 1), box(s, 2), box(s, 3), box(s, 4)};
+            const TV* ce = box(s, 5);
             const int tI = t / tilesJ, tJ = t % tilesJ;
             const int i0 = 1 + kTileR * tI, j0 = 1 + kTileC * tJ;
             // x' = x0 + e(agg) on unknowns, 0 elsewhere
@@ -482,7 +486,7 @@ __global__ void __launch_bounds__(512, 1) k_pcg_mg(KParams k, Status* st, const 
                 const int ii = i0 - 1 + li, jj = j0 - 1 + lj;
                 if (ii < 1 || ii > nI0 || jj < 1 || jj > nJ0) return (TV)0;
                 const int cli = ((ii + 1) >> 1) - (kTileR / 2) * tI, clj = ((jj + 1) >> 1) - (kTileC / 2) * tJ;
-                return x0s(bx, li, lj) + scT * ce[cli * kCBoxW + clj];
+                return SB(4, li, lj) + scT * ce[cli * kCBoxW + clj];
             };
             for (int u = threadIdx.x; u < kTileR * kTileC; u += blockDim.x) {
                 const int a = u / kTileC, b = u % kTileC;
@@ -539,6 +543,7 @@ __global__ void __launch_bounds__(512, 1) k_pcg_mg(KParams k, Status* st, const 
                           [&](int I, int J) { mg_restrict_cell(H.lv[l], H.lv[l + 1], I, J, om); });
             target += G;
             if (!grid_barrier(bar, target, &st->err)) return false;
+            tick(MG_P_COUNT + l, tp);
         }
         tick(MG_P_DOWN, tp);
         // the small levels on CTA 0
@@ -564,6 +569,7 @@ __global__ void __launch_bounds__(512, 1) k_pcg_mg(KParams k, Status* st, const 
             }
             target += G;
             if (!grid_barrier(bar, target, &st->err)) return false;
+            tick(MG_P_COUNT + kMgMaxLevels + l, tp);
         }
         double t2[2];
         sum_partials<2>(partB, G, 2, t2, sm);
@@ -595,7 +601,7 @@ __global__ void __launch_bounds__(512, 1) k_pcg_mg(KParams k, Status* st, const 
         const TV al = (TV)alpha;
         double accB[1] = {0.0};
         for (int t0 = tid; t0 < n; t0 += 2 * nth) {
-            TV xv[2], pv[2], rv[2], av[2];
+            TV xv[2], pv[2], rv[2], av[2], dv[2];
             size_t cc[2];
             bool ok[2];
 #pragma unroll
@@ -605,7 +611,7 @@ __global__ void __launch_bounds__(512, 1) k_pcg_mg(KParams k, Status* st, const 
                 const int tt = ok[q] ? t : t0;
                 const size_t c = at(d, 1 + tt / w, 1 + tt % w);
                 cc[q] = c;
-                xv[q] = B.x[c]; pv[q] = pnew[c]; rv[q] = B.r[c]; av[q] = B.Ap[c];
+                xv[q] = B.x[c]; pv[q] = pnew[c]; rv[q] = B.r[c]; av[q] = B.Ap[c]; dv[q] = B.d[c];
             }
 #pragma unroll
             for (int q = 0; q < 2; ++q) {
@@ -613,6 +619,7 @@ __global__ void __launch_bounds__(512, 1) k_pcg_mg(KParams k, Status* st, const 
                 B.x[cc[q]] = xv[q] + al * pv[q];
                 const TV r = rv[q] - al * av[q];
                 B.r[cc[q]] = r;
+                L0.x[cc[q]] = omT * r / dv[q];
                 accB[0] += (double)r * (double)r;
             }
         }

@@ -381,9 +381,9 @@ cp_status mg_build(cp_ctx* c) {
     c->mgArr[0][0] = c->pcg[0];
     c->mgArr[0][1] = c->pcg[1];
     c->mgArr[0][2] = c->pcg[2];
-    // level 0: dx and y of its own; its rhs is the CG residual r; it keeps no x
+    // level 0: dx, y and x of its own (x holds the pre-smoothed iterate
+    // omega r / d); its rhs is the CG residual r
     for (int q = 3; q < 6; ++q) {
-        if (q == 4) continue;
         cp_status s = dalloc_bytes(c, &c->mgArr[0][q], c->nElem * c->es);
         if (s != CP_OK) return s;
     }
@@ -408,6 +408,7 @@ cp_status mg_build(cp_ctx* c) {
                               &c->mgMaps.fE, &c->mgMaps.fN};
         for (int q = 0; q < 7; ++q)
             if ((s = encode_map(m0[q], a0[q], es, P0, R0, kBoxW, kBoxR)) != CP_OK) return s;
+        if ((s = encode_map(&c->mgMaps.x0, c->mgArr[0][4], es, P0, R0, kBoxW, kBoxR)) != CP_OK) return s;
         void* e1 = (Lg > 1) ? c->mgArr[1][5] : c->mgArr[1][4];
         if ((s = encode_map(&c->mgMaps.e1, e1, es, c->mgP[1], c->mgNI[1] + 2, kCBoxW, kCBoxR)) != CP_OK) return s;
     }
@@ -416,7 +417,7 @@ cp_status mg_build(cp_ctx* c) {
     const char* sc = getenv("CP_MG_SCALE");
     if (sc) c->mgScale = atof(sc);
     if (getenv("CP_MG_PROFILE")) {
-        cp_status s2 = dalloc(c, &c->mgProf, (size_t)MG_P_COUNT);
+        cp_status s2 = dalloc(c, &c->mgProf, (size_t)kMgProfSlots);
         if (s2 != CP_OK) return s2;
     }
     // one CTA per SM (the dense set-up needs kMgDynSmem of shared memory)
@@ -953,11 +954,16 @@ cp_status cp_kernel_times(cp_ctx* c, int n_outer, cp_kernel_timing* out) {
     }
     for (auto& e : rec.ev) cudaEventDestroy(e);
     if (c->mgProf && out->iterations > 0) {
-        unsigned long long pr[MG_P_COUNT];
+        unsigned long long pr[kMgProfSlots];
         if (cudaMemcpy(pr, c->mgProf, sizeof pr, cudaMemcpyDeviceToHost) == cudaSuccess) {
             const char* names[MG_P_COUNT] = {"setup", "cg_A", "cg_B", "vdown", "vcta", "vup"};
             fprintf(stderr, "[cp mg profile] per outer iteration (us):");
             for (int q = 0; q < MG_P_COUNT; ++q) fprintf(stderr, " %s %.1f", names[q], pr[q] * 1e-3 / out->iterations);
+            fprintf(stderr, "\n[cp mg profile] restriction out of level l:");
+            for (int l = 0; l < c->mgLg; ++l) fprintf(stderr, " %d:%.1f", l, pr[MG_P_COUNT + l] * 1e-3 / out->iterations);
+            fprintf(stderr, "\n[cp mg profile] prolongation into level l:");
+            for (int l = 0; l < c->mgLg; ++l)
+                fprintf(stderr, " %d:%.1f", l, pr[MG_P_COUNT + kMgMaxLevels + l] * 1e-3 / out->iterations);
             fprintf(stderr, "\n");
         }
         cudaMemset(c->mgProf, 0, sizeof pr);
