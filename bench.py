@@ -63,6 +63,8 @@ def parse():
     ap.add_argument("--cpu-sample-iters", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--batch-fields", type=int, default=64)
+    ap.add_argument("--batch-outer", type=int, default=200)
     return ap.parse_args()
 
 
@@ -218,30 +220,30 @@ def reference_arm(args, case, rank: int):
 
 
 # ------------------------------------------------------------------ batched solves
-BATCH_FIELDS = 64
-BATCH_OUTER = 200
 BATCH_SINGLE_OUTER = 20
 
 
 def batch_leg(Simple, torch, args) -> dict:
-    """64 density fields (Nx in 256-1024, Ny in 128-512, U_in in 0.2-1.0 m/s,
-    mixed precision, epsilon 1e-6) advanced by the batched kernel for
-    BATCH_OUTER outer iterations with the autotuned tile, against the same
+    """--batch-fields density fields (64 by default: Nx in 256-1024, Ny in
+    128-512, U_in in 0.2-1.0 m/s, mixed precision, epsilon 1e-6) advanced by
+    the batched kernel for --batch-outer outer iterations (200) with the
+    autotuned tile, against the same
     fields solved one after the other (BATCH_SINGLE_OUTER iterations each).
     Most of these fields never reach epsilon 1e-6 with the reference's SIMPLE
     iteration (their residual RMS levels off near 1e-5), so the leg times a
     fixed number of iterations and reports cell-iterations per second."""
     from coldplate_b200 import Batch, cases
-    cs = cases.batch(BATCH_FIELDS, seed=args.seed, **BENCH_KNOBS)
+    nf, nout = args.batch_fields, args.batch_outer
+    cs = cases.batch(nf, seed=args.seed, **BENCH_KNOBS)
     cells = [c.cellType.shape[0] * c.cellType.shape[1] for c in cs]
-    prm = dict(precision="mixed", epsilon=1e-6, maxIterations=BATCH_OUTER, historyCapacity=BATCH_OUTER)
+    prm = dict(precision="mixed", epsilon=1e-6, maxIterations=nout, historyCapacity=nout)
     fields = [Simple(cellType=c.cellType, **c.params(**prm)) for c in cs]
     try:
         with Batch(fields) as b:
             tune = b.autotune(3)
             flush_l2(torch)
             torch.cuda.synchronize()
-            rep = b.run(BATCH_OUTER)
+            rep = b.run(nout)
             its = [len(f.history()["iter"]) for f in fields]
     finally:
         for f in fields:
@@ -255,8 +257,8 @@ def batch_leg(Simple, torch, args) -> dict:
             r = s.step(BATCH_SINGLE_OUTER)
             t1 += r["device_ms"] / 1e3
             work1 += n * BATCH_SINGLE_OUTER
-    return {"workload": f"{BATCH_FIELDS} density fields, Nx 256-1024, Ny 128-512, U_in 0.2-1.0 m/s, seed {args.seed}, "
-                        f"mixed, {BATCH_OUTER} outer iterations",
+    return {"workload": f"{nf} density fields, Nx 256-1024, Ny 128-512, U_in 0.2-1.0 m/s, seed {args.seed}, "
+                        f"mixed, {nout} outer iterations",
             "cells": int(sum(cells)), "t_s": t, "launches": rep["launches"],
             "tile": [rep["tileRows"], rep["tileCols"]], "autotune_trial_ms": tune["device_ms"],
             "cell_iterations_per_s": work / t,
