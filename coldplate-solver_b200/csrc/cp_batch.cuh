@@ -353,6 +353,7 @@ __global__ void __launch_bounds__(kBatchThreads, 1) k_batch(BatchArgs a, const B
                     fs.H.lv[0].dx[c] = (TC)extra;
                     fs.B.x[c] = (TC)0;
                     fs.B.r[c] = rb;
+                    fs.H.lv[0].x[c] = (TC)fs.H.omega * rb / (TC)aP;   // stored pre-smoothed iterate
                     acc[4] += (double)rb * (double)rb;
                 }
                 if (i <= M - 2) {
@@ -419,7 +420,7 @@ __global__ void __launch_bounds__(kBatchThreads, 1) k_batch(BatchArgs a, const B
         auto vcycle = [&]() -> bool {
             for (int l = 0; l < a.maxLg; ++l) {
                 for_tiles(l + 1, [&](int f) { return cgOn(f) && l < F[f].H.Lg; }, [&](int I, int J) {
-                    if (l == 0) mg_restrict0_cell(fs.H.lv[0], fs.H.lv[1], I, J, fs.H.omega);
+                    if (l == 0) mg_restrict0x_cell(fs.H.lv[0], fs.H.lv[1], I, J, fs.H.omega);
                     else mg_restrict_cell(fs.H.lv[l], fs.H.lv[l + 1], I, J, fs.H.omega);
                 }, noFin);
                 if (!sync()) return false;
@@ -437,7 +438,7 @@ __global__ void __launch_bounds__(kBatchThreads, 1) k_batch(BatchArgs a, const B
                     const TC* e = (l + 1 < fs.H.Lg) ? cl.y : cl.x;
                     if (l == 0) {
                         if (j > fl.nJ) return;
-                        const TC y = mg_prolong0_cell(fl, cl, e, i, j, fs.H.omega, fs.H.scale);
+                        const TC y = mg_prolong0x_cell(fl, cl, e, i, j, fs.H.omega, fs.H.scale);
                         acc[0] += (double)fl.b[lidx(fl, i, j)] * (double)y;
                     } else {
                         mg_prolong_smooth_cell(fl, cl, e, i, j, fs.H.omega, fs.H.scale);
@@ -520,6 +521,7 @@ __global__ void __launch_bounds__(kBatchThreads, 1) k_batch(BatchArgs a, const B
                     fs.B.x[c] = fs.B.x[c] + al * pnew[c];
                     const TC r = fs.B.r[c] - al * fs.B.Ap[c];
                     fs.B.r[c] = r;
+                    fs.H.lv[0].x[c] = (TC)fs.H.omega * r / fs.B.d[c];
                     acc[0] += (double)r * (double)r;
                 }, [&](int, int g) {
                     block_sum<1>(acc, sm);

@@ -170,6 +170,43 @@ __device__ __forceinline__ void mg_restrict0_cell(const MgLevel<TV>& f, const Mg
     c.x[q] = (TV)(omega * s / (double)c.d[q]);
 }
 
+// The same two level-0 operators with the pre-smoothed iterate stored in
+// f.x (omega r / d, zero off the unknowns) instead of recomputed.
+template <typename TV>
+__device__ __forceinline__ void mg_restrict0x_cell(const MgLevel<TV>& f, const MgLevel<TV>& c, int I, int J,
+                                                   double omega) {
+    const int i0 = 2 * I - 1, i1 = min(2 * I, f.nI), j0 = 2 * J - 1, j1 = min(2 * J, f.nJ);
+    const TV om = (TV)omega;
+    double s = 0.0;
+    for (int i = i0; i <= i1; ++i)
+        for (int j = j0; j <= j1; ++j) {
+            const size_t q = lidx(f, i, j);
+            const TV r = ((TV)1 - om) * f.b[q] + f.fE[q] * f.x[q + 1] + f.fE[q - 1] * f.x[q - 1] +
+                         f.fN[q] * f.x[q + f.P] + f.fN[q - f.P] * f.x[q - f.P];
+            s += (double)r;
+        }
+    const size_t q = lidx(c, I, J);
+    c.b[q] = (TV)s;
+    c.x[q] = (TV)(omega * s / (double)c.d[q]);
+}
+
+template <typename TV>
+__device__ __forceinline__ TV mg_prolong0x_cell(const MgLevel<TV>& f, const MgLevel<TV>& c, const TV* e, int i,
+                                                int j, double omega, double c_scale) {
+    const TV om = (TV)omega, sc = (TV)c_scale;
+    auto xp = [&](int ii, int jj) -> TV {
+        if (ii < 1 || ii > f.nI || jj < 1 || jj > f.nJ) return (TV)0;
+        return f.x[lidx(f, ii, jj)] + sc * e[lidx(c, (ii + 1) >> 1, (jj + 1) >> 1)];
+    };
+    const size_t q = lidx(f, i, j);
+    const TV xc = xp(i, j);
+    const TV ax = f.d[q] * xc - f.fE[q] * xp(i, j + 1) - f.fE[q - 1] * xp(i, j - 1) - f.fN[q] * xp(i + 1, j) -
+                  f.fN[q - f.P] * xp(i - 1, j);
+    const TV y = xc + om * (f.b[q] - ax) / f.d[q];
+    f.y[q] = y;
+    return y;
+}
+
 // prolongation into level 0 + one Jacobi sweep: x' = x0 + s P e, y = x' + omega (b - A x') / d
 template <typename TV>
 __device__ __forceinline__ TV mg_prolong0_cell(const MgLevel<TV>& f, const MgLevel<TV>& c, const TV* e, int i,
