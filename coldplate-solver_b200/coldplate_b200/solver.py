@@ -163,6 +163,23 @@ class Simple:
         rows = buf[: n.value]
         return {name: rows[:, k] for k, name in enumerate(nat.HIST_COLS)}
 
+    # -------------------------------------------------------------- result files
+    def saveAll(self, export_dir: str = "ExportFiles", u_old=None, v_old=None) -> list[str]:
+        """The reference's result files (SIMPLE::saveAll, output.cpp:74-200)
+        from the current fields; see coldplate_b200.output.  u_old / v_old
+        (the fields before the last iteration) add u_resid_full /
+        v_resid_full."""
+        from . import output
+        return output.save_all(export_dir, self.get("u"), self.get("v"), self.get("p"), self.params.hx,
+                               self.params.hy, self.params.N_in_buffer, self.params.N_out_buffer, u_old, v_old)
+
+    def writeIterationLogs(self, export_dir: str = "ExportFiles") -> None:
+        """residuals.txt and pressure_drop_history.txt for the iterations run
+        so far (output.cpp:302-364)."""
+        from . import output
+        output.write_logs(export_dir, self.history(), bool(self.params.enableNormalizedResiduals),
+                          self.params.residNormFloorVel, self.params.residNormFloorMass)
+
     # -------------------------------------------------------------- adjoint
     def adjoint_dp_dgamma(self, max_iter: int = 2000, tol: float = 1e-10) -> tuple[np.ndarray, dict]:
         """dJ/dgamma (Ny x Nx) of the full-system total-pressure drop J at the
