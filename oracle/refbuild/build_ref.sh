@@ -67,3 +67,12 @@ find "$SRC64" \( -name '*.cpp' -o -name '*.h' \) -print0 | xargs -0 sed -i -E \
     -e 's/MatrixXf/MatrixXd/g' -e 's/VectorXf/VectorXd/g' \
     -e 's/\b([0-9][0-9]*\.?[0-9]*([eE][-+]?[0-9]+)?)[fF]\b/\1/g'
 build ref_f64_pin "$SRC64" double -O2 -ffp-contract=off
+
+# the thermal solver (ThermalSolver/thermal_solver.cpp, one translation unit)
+# against the AMGCL API stand-in in shim/amgcl: the reference's own assembly,
+# solved by the stand-in to a tight tolerance; -ffp-contract=off pins it
+if [ -f "$REF_DIR/ThermalSolver/thermal_solver.cpp" ]; then
+    $CXX -std=c++17 -O2 -ffp-contract=off -fopenmp "${GOMP_B[@]}" -I"$HERE/shim" -I"$REF_DIR/ThermalSolver" \
+        "$REF_DIR/ThermalSolver/thermal_solver.cpp" -o "$OUT/thermal_ref_pin"
+    echo "built $OUT/thermal_ref_pin"
+fi

@@ -1,0 +1,49 @@
+"""The thermal oracle (oracle/thermal_oracle.py) against the reference's own
+thermal solver: ThermalSolver/thermal_solver.cpp built against the AMGCL API
+stand-in (oracle/refbuild/shim/amgcl), which dumps the system the reference
+assembled and its tight solution.  The restated assembly must give the same
+matrix and right-hand side bit for bit."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+REF = os.path.join(ROOT, "oracle", "_ref", "thermal_ref_pin")
+
+
+def thermal_inputs(Ny, Nx, seed):
+    """A seeded density geometry with cell-centred velocities of both signs."""
+    from coldplate_b200 import cases
+    gam = cases.density_gamma(Ny, Nx, seed, buffer=4)
+    rng = np.random.default_rng(seed)
+    u = gam * (0.4 + 0.2 * rng.random((Ny, Nx))) - 0.05 * rng.random((Ny, Nx))
+    v = 0.1 * (rng.random((Ny, Nx)) - 0.5) * gam
+    pm = 20.0 + 80.0 * rng.random((Ny, Nx))        # W/cm^2
+    return gam, u, v, pm
+
+
+@pytest.mark.skipif(not os.path.exists(REF), reason="reference build (oracle/_ref) not present")
+@pytest.mark.parametrize("with_map", [False, True])
+def test_assembly_matches_the_reference_bit_for_bit(tmp_path, with_map):
+    from thermal_oracle import ThermalParams, assemble, read_dump, solve, write_case
+    Ny, Nx, dx, dy, qf, Ht = 20, 44, 2e-5, 2e-5, 5.0e5, 2e-4
+    gam, u, v, pm = thermal_inputs(Ny, Nx, 3)
+    case = str(tmp_path / "case")
+    geom = 1.0 - gam                       # the file holds 0 = fluid, 1 = solid
+    write_case(case, geom, u, v, dx, dy, qf, Ht, pm if with_map else None)
+    gam = 1.0 - geom                       # what the reference reads back (thermal_solver.cpp:738)
+    dump = str(tmp_path / "dump.bin")
+    subprocess.run([REF, case], check=True, capture_output=True, text=True, timeout=600,
+                   env=dict(os.environ, CP_AMGCL_SHIM_DUMP=dump, OMP_NUM_THREADS="1"))
+    A_ref, b_ref, x_ref = read_dump(dump)
+    p = ThermalParams(Nx=Nx, Ny=Ny, dx=dx, dy=dy, H_t=Ht)
+    q0 = pm * 10000.0 if with_map else np.full((Ny, Nx), qf)
+    A, b = assemble(p, gam, u, v, q0)
+    A_ref.sort_indices()
+    assert np.array_equal(A.indptr, A_ref.indptr) and np.array_equal(A.indices, A_ref.indices)
+    assert np.array_equal(A.data, A_ref.data), np.abs(A.data - A_ref.data).max()
+    assert np.array_equal(b, b_ref)
+    T = solve(p, gam, u, v, q0).ravel()
+    assert np.linalg.norm(T - x_ref) <= 1e-10 * np.linalg.norm(x_ref)
