@@ -87,6 +87,17 @@ class CpBatchReport(ctypes.Structure):
                 ("tileRows", ctypes.c_int), ("tileCols", ctypes.c_int), ("device_ms", ctypes.c_double)]
 
 
+class CpThermalParams(ctypes.Structure):
+    """struct cp_thermal_params (include/cp_thermal.h)."""
+    _fields_ = [("Nx", _I), ("Ny", _I), ("nz_solid", _I), ("nz_fluid", _I), ("dx", _D), ("dy", _D),
+                ("H_b", _D), ("H_t", _D), ("k_s", _D), ("k_f", _D), ("rho", _D), ("Cp", _D), ("T_inlet", _D),
+                ("rtol", _D), ("maxiter", _I), ("k_interp_mode", _I), ("qk", _D)]
+
+
+class CpThermalReport(ctypes.Structure):
+    _fields_ = [("iterations", _I), ("converged", _I), ("residual", _D), ("device_ms", _D)]
+
+
 # history row columns (cp_device.cuh HistCol)
 HIST_COLS = ("iter", "error", "residU_RMS", "residV_RMS", "residMass_RMS", "residU_max", "residV_max",
              "residMass_max", "pIters", "coreTotal", "fullTotal", "coreStatic", "fullStatic",
@@ -121,6 +132,14 @@ SIGNATURES = {
     "cp_batch_set_tile": (_I, [_vp, _I, _I]),
     "cp_batch_run": (_I, [_vp, _I, ctypes.POINTER(CpBatchReport)]),
     "cp_batch_autotune": (_I, [_vp, _I, ctypes.POINTER(CpBatchReport)]),
+    "cp_thermal_params_default": (None, [ctypes.POINTER(CpThermalParams)]),
+    "cp_thermal_create": (_I, [ctypes.POINTER(CpThermalParams), ctypes.POINTER(_vp)]),
+    "cp_thermal_destroy": (_I, [_vp]),
+    "cp_thermal_set_inputs": (_I, [_vp, _dp, _dp, _dp, _dp]),
+    "cp_thermal_solve": (_I, [_vp, ctypes.POINTER(CpThermalReport)]),
+    "cp_thermal_get_T": (_I, [_vp, _dp]),
+    "cp_thermal_objective": (_I, [_vp, _D, _dp, _dp]),
+    "cp_thermal_pnorm_gradient": (_I, [_vp, _D, _dp, _dp, ctypes.POINTER(CpThermalReport)]),
     "cp_history_columns": (_I, []),
     "cp_get_history": (_I, [_vp, _dp, _I, _ip]),
     "cp_status_string": (ctypes.c_char_p, [_I]),

@@ -8,14 +8,15 @@ PKG_DIR = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG_DIR)          # coldplate-solver_b200/
 CSRC = os.path.join(ROOT, "csrc")
 OUT = os.path.join(ROOT, "libcoldplate.so")
-SOURCES = ["cp_solver.cu"]
+SOURCES = ["cp_solver.cu", "cp_thermal.cu"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
               "-Xcompiler", "-fPIC", "-shared", "--expt-relaxed-constexpr"]
 
 
 def _sources_mtime() -> float:
     files = [os.path.join(CSRC, f) for f in os.listdir(CSRC)]
-    files.append(os.path.join(os.path.dirname(ROOT), "include", "cp_simple.h"))
+    inc = os.path.join(os.path.dirname(ROOT), "include")
+    files += [os.path.join(inc, f) for f in os.listdir(inc)]
     return max(os.path.getmtime(f) for f in files if os.path.exists(f))
 
 

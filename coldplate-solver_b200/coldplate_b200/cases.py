@@ -19,6 +19,8 @@ Workloads
                     fluid so the pressure drop is defined
   batch             density fields of random sizes (Nx 256-1024, Ny 128-512)
                     and inlet velocities (0.2-1.0 m/s)
+  THERMAL_3D,       the 3-D conjugate-heat-transfer settings on the flow's
+  power_map         plane (8 + 4 layers) and a hotspot heat-flux map
 
 Values are rounded to float32 so the reference's float and double builds
 read identical geometries from the text files.
@@ -218,6 +220,26 @@ def batch(n: int = 64, seed: int = 0, **over) -> list[Case]:
         c.name = f"batch{k}"
         out.append(c)
     return out
+
+
+# the conjugate-heat-transfer workload on a converged density flow: 8 base
+# plate and 4 channel layers, water, T_in 25 C, 200 um channels on a 0.5 mm plate
+THERMAL_3D = dict(nz_solid=8, nz_fluid=4, k_s=400.0, k_f=0.6, rho=1000.0, Cp=4180.0, T_inlet=25.0,
+                  H_t=2e-4, H_b=5e-4)
+
+
+def power_map(Ny: int, Nx: int, seed: int) -> np.ndarray:
+    """Heat flux [W/cm^2] (the unit of the reference's power_map.txt): 20
+    W/cm^2 background plus 4-12 Gaussian hotspots with sigma U[20, 80] cells
+    and peak U[50, 300] W/cm^2 at uniformly drawn centres."""
+    rng = np.random.default_rng(seed)
+    q = np.full((Ny, Nx), 20.0)
+    y, x = np.mgrid[0:Ny, 0:Nx]
+    for _ in range(int(rng.integers(4, 13))):
+        cy, cx = rng.uniform(0, Ny), rng.uniform(0, Nx)
+        sig, peak = rng.uniform(20.0, 80.0), rng.uniform(50.0, 300.0)
+        q += peak * np.exp(-((x - cx) ** 2 + (y - cy) ** 2) / (2.0 * sig * sig))
+    return q
 
 
 WORKLOADS = {

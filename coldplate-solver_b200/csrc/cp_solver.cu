@@ -41,6 +41,16 @@ cp_status fail(cp_status s, const char* fmt, ...) {
     return s;
 }
 
+}  // namespace
+
+// The error string of the other translation units (cp_thermal.cu).
+__attribute__((visibility("hidden"))) cp_status cp_internal_set_error(cp_status s, const char* msg) {
+    g_err = msg;
+    return s;
+}
+
+namespace {
+
 #define CK(call)                                                                                   \
     do {                                                                                           \
         cudaError_t e_ = (call);                                                                   \

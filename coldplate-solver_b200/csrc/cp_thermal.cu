@@ -1,0 +1,778 @@
+// B200 3-D conjugate-heat-transfer solve (C ABI in include/cp_thermal.h).
+//
+// The reference (ThermalSolver/thermal_solver.cpp) assembles a 7-point
+// finite-volume system on Nx x Ny x Nz cells into CSR on the host and solves
+// it with AMGCL's IDR(s) (thermal_solver.cpp:417-553).  Here:
+//   k_th_assemble   one thread per cell computes the reference's row in FP64
+//                   (same formulas and summation order, thermal_solver.cpp:
+//                   420-520) into seven coefficient arrays and b;
+//   k_th_lu         factors the tridiagonal z-block of every (i, j) column
+//                   (the strongly coupled direction: thin layers);
+//   k_th_bicgstab   persistent cooperative BiCGStab, right-preconditioned by
+//                   exact solves of the z-columns.  The column phases fuse
+//                   the vector update with the column solve; five bounded
+//                   grid barriers per iteration; deterministic block sums;
+//                   AMGCL's stop test ||r|| <= rtol ||b||.  The same kernel
+//                   solves A^T x = rhs for the p-norm adjoint;
+//   k_th_sens       dJ/dgamma from the adjoint field, one thread per column.
+// Layout: every array is indexed k Nx Ny + j Nx + i (i contiguous), so the
+// stencil loads of a warp are coalesced and a column thread walks k with
+// stride Nx Ny.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "../../include/cp_thermal.h"
+#include "cp_device.cuh"
+
+// error string of the library (cp_solver.cu)
+cp_status cp_internal_set_error(cp_status s, const char* msg);
+
+namespace {
+
+cp_status tfail(cp_status s, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    return cp_internal_set_error(s, buf);
+}
+
+#define TCK(call)                                                                                  \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess)                                                                     \
+            return tfail(CP_ERR_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_),      \
+                         __FILE__, __LINE__);                                                      \
+    } while (0)
+
+constexpr int kThThreads = 256;
+constexpr int kThMaxNz = 64;
+
+}  // namespace
+
+namespace cp {
+
+struct ThK {
+    int Nx, Ny, Nz, nzS, nzF, mode;
+    long long n, ncol;
+    double dx, dy, dzS, dzF, Ht, kS, kF, rhoCp, Tin, qk;
+};
+
+struct ThSys {
+    double *aP, *aW, *aE, *aS, *aN, *aB, *aT, *b;
+};
+
+struct ThStatus {
+    int iterations, converged, err, pad;
+    double residual;
+};
+
+__device__ __forceinline__ double th_dz(const ThK& k, int kk) { return kk < k.nzS ? k.dzS : k.dzF; }
+
+// thermal_solver.cpp:271-305 (gamma clamped to [0, 1]); k_s in the base plate
+__device__ __forceinline__ double th_kval(const ThK& k, const double* gamma, int i, int j, int kk) {
+    if (kk < k.nzS) return k.kS;
+    double g = gamma[(size_t)j * k.Nx + i];
+    g = fmax(0.0, fmin(1.0, g));
+    if (k.mode == 1) {
+        const double num = 1.0 - g;
+        const double den = 1.0 + __dmul_rn(k.qk, g);
+        return k.kF + (k.kS - k.kF) * num / den;
+    }
+    if (k.mode == 2) return k.kS * k.kF / (__dmul_rn(1.0 - g, k.kF) + __dmul_rn(g, k.kS) + 1e-30);
+    return __dmul_rn(k.kS, 1.0 - g) + __dmul_rn(k.kF, g);
+}
+
+// 1 = fluid: above the base plate with gamma > 0.01 (thermal_solver.cpp:240-244)
+__device__ __forceinline__ bool th_fluid(const ThK& k, const double* gamma, int i, int j, int kk) {
+    if (kk < k.nzS) return false;
+    return gamma[(size_t)j * k.Nx + i] > 0.01;
+}
+
+// Poiseuille factor of a fluid layer (thermal_solver.cpp:323-327)
+__device__ __forceinline__ double th_pois(const ThK& k, int kk) {
+    if (kk < k.nzS) return 0.0;
+    const double z = (kk - k.nzS + 0.5) * k.dzF / k.Ht;
+    return 4.0 * z * (1 - z);
+}
+
+__device__ __forceinline__ double th_harm(double a, double b) { return 2 * a * b / (a + b + 1e-30); }
+
+// One row of the reference's system, in its summation order
+// (thermal_solver.cpp:420-520).  Every product that feeds a sum is rounded
+// on its own (__dmul_rn) so that no multiply-add is fused and the row has the
+// reference's bits.  Off-diagonal entries are the matrix values (negative);
+// the reference's two entries for one neighbour (diffusion and upwind
+// advection) are summed like its CSR conversion sums them.
+__global__ void k_th_assemble(ThK k, const double* gamma, const double* u_xy, const double* v_xy, const double* q0,
+                              ThSys S) {
+    const int Nx = k.Nx, Ny = k.Ny, Nz = k.Nz;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < k.n;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int kk = (int)(t / ((long long)Nx * Ny));
+        const int rem = (int)(t - (long long)kk * Nx * Ny);
+        const int j = rem / Nx, i = rem % Nx;
+        const double dx = k.dx, dy = k.dy, rhoCp = k.rhoCp, T_in = k.Tin;
+        const double dz_k = th_dz(k, kk), Ax = dy * dz_k, Ay = dx * dz_k, Az_cell = dx * dy;
+        double diag = 0, bb = 0;
+        const double kP = th_kval(k, gamma, i, j, kk), po = th_pois(k, kk);
+        double g = (kk < k.nzS) ? 0.0 : gamma[(size_t)j * Nx + i];
+        g = fmax(0.0, fmin(1.0, g));
+        const double uP = (g > 0.01) ? __dmul_rn(u_xy[(size_t)j * Nx + i], po) : 0.0;
+        const double vP = (g > 0.01) ? __dmul_rn(v_xy[(size_t)j * Nx + i], po) : 0.0;
+        const bool regP = th_fluid(k, gamma, i, j, kk);
+        double aW = 0, aE = 0, aS = 0, aN = 0, aB = 0, aT = 0;
+        // x faces
+        if (i > 0) {
+            const double kf = th_harm(kP, th_kval(k, gamma, i - 1, j, kk)), D = kf * Ax / dx;
+            diag += D;
+            aW = -D;
+            if (regP && th_fluid(k, gamma, i - 1, j, kk)) {
+                const double uW = __dmul_rn(u_xy[(size_t)j * Nx + i - 1], po), F = rhoCp * 0.5 * (uP + uW) * Ax;
+                diag += fmax(-F, 0.0);
+                aW = aW + (-fmax(F, 0.0));
+            }
+        } else if (regP) {
+            const double D_bc = 2.0 * kP * Ax / dx, F_bc = __dmul_rn(rhoCp * uP, Ax);
+            diag += D_bc;
+            bb += __dmul_rn(D_bc, T_in);
+            if (F_bc > 0) bb += __dmul_rn(F_bc, T_in);
+            else diag += -F_bc;
+        }
+        if (i < Nx - 1) {
+            const double kf = th_harm(kP, th_kval(k, gamma, i + 1, j, kk)), D = kf * Ax / dx;
+            diag += D;
+            aE = -D;
+            if (regP && th_fluid(k, gamma, i + 1, j, kk)) {
+                const double uE = __dmul_rn(u_xy[(size_t)j * Nx + i + 1], po), F = rhoCp * 0.5 * (uP + uE) * Ax;
+                diag += fmax(F, 0.0);
+                aE = aE + (-fmax(-F, 0.0));
+            }
+        } else if (regP && uP > 0) {
+            diag += __dmul_rn(rhoCp * uP, Ax);
+        }
+        // y faces
+        if (j > 0) {
+            const double kf = th_harm(kP, th_kval(k, gamma, i, j - 1, kk)), D = kf * Ay / dy;
+            diag += D;
+            aS = -D;
+            if (regP && th_fluid(k, gamma, i, j - 1, kk)) {
+                const double vS = __dmul_rn(v_xy[(size_t)(j - 1) * Nx + i], po), F = rhoCp * 0.5 * (vP + vS) * Ay;
+                diag += fmax(-F, 0.0);
+                aS = aS + (-fmax(F, 0.0));
+            }
+        }
+        if (j < Ny - 1) {
+            const double kf = th_harm(kP, th_kval(k, gamma, i, j + 1, kk)), D = kf * Ay / dy;
+            diag += D;
+            aN = -D;
+            if (regP && th_fluid(k, gamma, i, j + 1, kk)) {
+                const double vN = __dmul_rn(v_xy[(size_t)(j + 1) * Nx + i], po), F = rhoCp * 0.5 * (vP + vN) * Ay;
+                diag += fmax(F, 0.0);
+                aN = aN + (-fmax(-F, 0.0));
+            }
+        } else if (regP && vP > 0) {
+            diag += __dmul_rn(rhoCp * vP, Ay);
+        }
+        // z faces (diffusion only)
+        if (kk > 0) {
+            const double kN = th_kval(k, gamma, i, j, kk - 1), dz_P = dz_k, dz_N = th_dz(k, kk - 1);
+            const double kf = (dz_P + dz_N) / (dz_P / kP + dz_N / kN);
+            const double D = kf * Az_cell / (0.5 * (dz_P + dz_N));
+            diag += D;
+            aB = -D;
+        } else {
+            bb += __dmul_rn(q0[(size_t)j * Nx + i], Az_cell);
+        }
+        if (kk < Nz - 1) {
+            const double kN = th_kval(k, gamma, i, j, kk + 1), dz_P = dz_k, dz_N = th_dz(k, kk + 1);
+            const double kf = (dz_P + dz_N) / (dz_P / kP + dz_N / kN);
+            const double D = kf * Az_cell / (0.5 * (dz_P + dz_N));
+            diag += D;
+            aT = -D;
+        }
+        S.aP[t] = diag + 1e-12;
+        S.aW[t] = aW; S.aE[t] = aE; S.aS[t] = aS; S.aN[t] = aN; S.aB[t] = aB; S.aT[t] = aT;
+        S.b[t] = bb;
+    }
+}
+
+// z-coupling of row q of A (Tr = false) or of A^T (Tr = true): the entry
+// towards k-1 and towards k+1.  Row q of A^T holds column q of A, so its
+// k-1 entry is A's aT of the cell below and its k+1 entry A's aB above.
+template <bool Tr>
+__device__ __forceinline__ double th_sub(const ThSys& S, long long q, long long L) {
+    return Tr ? S.aT[q - L] : S.aB[q];
+}
+template <bool Tr>
+__device__ __forceinline__ double th_sup(const ThSys& S, long long q, long long L) {
+    return Tr ? S.aB[q + L] : S.aT[q];
+}
+
+// Thomas factors of each column's tridiagonal z-block: inv_k = 1 / (d_k -
+// sub_k c_{k-1}), c_k = sup_k inv_k
+template <bool Tr>
+__global__ void k_th_lu(ThK k, ThSys S, double* lc, double* linv) {
+    const long long L = (long long)k.Nx * k.Ny;
+    for (long long col = (long long)blockIdx.x * blockDim.x + threadIdx.x; col < k.ncol;
+         col += (long long)gridDim.x * blockDim.x) {
+        double cprev = 0.0;
+        for (int kk = 0; kk < k.Nz; ++kk) {
+            const long long q = kk * L + col;
+            const double den = S.aP[q] - (kk > 0 ? th_sub<Tr>(S, q, L) * cprev : 0.0);
+            const double inv = 1.0 / den;
+            const double c = (kk < k.Nz - 1 ? th_sup<Tr>(S, q, L) : 0.0) * inv;
+            linv[q] = inv;
+            lc[q] = c;
+            cprev = c;
+        }
+    }
+}
+
+// (A x)_P (Tr = false) or (A^T x)_P (Tr = true) from the stored rows: row P
+// of A^T takes each neighbour's coefficient towards P
+template <bool Tr>
+__device__ __forceinline__ double th_ax(const ThK& k, const ThSys& S, const double* x, long long q, int i, int j,
+                                        int kk) {
+    const long long L = (long long)k.Nx * k.Ny;
+    double s = S.aP[q] * x[q];
+    if (i > 0) s += (Tr ? S.aE[q - 1] : S.aW[q]) * x[q - 1];
+    if (i < k.Nx - 1) s += (Tr ? S.aW[q + 1] : S.aE[q]) * x[q + 1];
+    if (j > 0) s += (Tr ? S.aN[q - k.Nx] : S.aS[q]) * x[q - k.Nx];
+    if (j < k.Ny - 1) s += (Tr ? S.aS[q + k.Nx] : S.aN[q]) * x[q + k.Nx];
+    if (kk > 0) s += (Tr ? S.aT[q - L] : S.aB[q]) * x[q - L];
+    if (kk < k.Nz - 1) s += (Tr ? S.aB[q + L] : S.aT[q]) * x[q + L];
+    return s;
+}
+
+struct ThVecs {
+    double *x, *r, *rh, *p, *v, *s, *t, *ph, *sh;
+};
+
+// BiCGStab (van der Vorst), right-preconditioned by the z-column solves, for
+// A x = rhs (Tr = false) or A^T x = rhs (Tr = true), from the x in V.x
+template <bool Tr>
+__global__ void __launch_bounds__(kThThreads) k_th_bicgstab(ThK k, ThSys S, const double* rhs, const double* lc,
+                                                           const double* linv, ThVecs V, double* part,
+                                                           unsigned* bar, ThStatus* st, int maxiter, double rtol) {
+    __shared__ double sm[96];
+    const int G = gridDim.x;
+    const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x, nth = (long long)G * blockDim.x;
+    const long long L = (long long)k.Nx * k.Ny;
+    unsigned target = 0;
+    double* pA = part;             // [G][2]
+    double* pB = part + 2 * G;     // [G][2]
+    double* pC = part + 4 * G;     // [G][2]
+    auto sync = [&]() -> bool {
+        target += G;
+        return grid_barrier(bar, target, &st->err);
+    };
+    auto cells = [&](auto&& fn) {
+        for (long long q = tid; q < k.n; q += nth) {
+            const int kk = (int)(q / L);
+            const long long rem = q - kk * L;
+            fn(q, (int)(rem % k.Nx), (int)(rem / k.Nx), kk);
+        }
+    };
+    // column solve: out = M^-1 (in_k), in_k computed by inf(q) along the column
+    auto column_solve = [&](long long col, auto&& inf, double* out) {
+        double yprev = 0.0;
+        for (int kk = 0; kk < k.Nz; ++kk) {
+            const long long q = kk * L + col;
+            const double in = inf(q);
+            const double y = (in - (kk > 0 ? th_sub<Tr>(S, q, L) * yprev : 0.0)) * linv[q];
+            out[q] = y;
+            yprev = y;
+        }
+        double xnext = 0.0;
+        for (int kk = k.Nz - 1; kk >= 0; --kk) {
+            const long long q = kk * L + col;
+            const double xv = out[q] - (kk < k.Nz - 1 ? lc[q] * xnext : 0.0);
+            out[q] = xv;
+            xnext = xv;
+        }
+    };
+    // ---- r = rhs - op x, rh = r, p = v = 0; ||rhs||^2, ||r||^2
+    {
+        double acc[2] = {0.0, 0.0};
+        cells([&](long long q, int i, int j, int kk) {
+            const double r = rhs[q] - th_ax<Tr>(k, S, V.x, q, i, j, kk);
+            V.r[q] = r;
+            V.rh[q] = r;
+            V.p[q] = 0.0;
+            V.v[q] = 0.0;
+            acc[0] += rhs[q] * rhs[q];
+            acc[1] += r * r;
+        });
+        block_sum<2>(acc, sm);
+        if (threadIdx.x == 0) { pC[2 * blockIdx.x] = acc[0]; pC[2 * blockIdx.x + 1] = acc[1]; }
+    }
+    if (!sync()) return;
+    double tot[2];
+    sum_partials<2>(pC, G, 2, tot, sm);
+    const double bnorm = sqrt(tot[0]) > 0.0 ? sqrt(tot[0]) : 1.0;
+    double res = sqrt(tot[1]) / bnorm;
+    double rho = 1.0, alpha = 1.0, omega = 1.0, rho1 = tot[1];
+    int it = 0;
+    bool conv = res <= rtol;
+    for (; it < maxiter && !conv; ++it) {
+        if (rho1 == 0.0) break;
+        const double beta = (rho1 / rho) * (alpha / omega);
+        // ---- p = r + beta (p - omega v); ph = M^-1 p
+        for (long long col = tid; col < k.ncol; col += nth)
+            column_solve(col, [&](long long q) {
+                const double pv = V.r[q] + beta * (V.p[q] - omega * V.v[q]);
+                V.p[q] = pv;
+                return pv;
+            }, V.ph);
+        if (!sync()) return;
+        // ---- v = op ph; (rh, v)
+        {
+            double acc[2] = {0.0, 0.0};
+            cells([&](long long q, int i, int j, int kk) {
+                const double vv = th_ax<Tr>(k, S, V.ph, q, i, j, kk);
+                V.v[q] = vv;
+                acc[0] += V.rh[q] * vv;
+            });
+            block_sum<2>(acc, sm);
+            if (threadIdx.x == 0) pA[2 * blockIdx.x] = acc[0];
+        }
+        if (!sync()) return;
+        double rv[2];
+        sum_partials<2>(pA, G, 2, rv, sm);
+        if (rv[0] == 0.0) break;
+        alpha = rho1 / rv[0];
+        // ---- s = r - alpha v; sh = M^-1 s
+        for (long long col = tid; col < k.ncol; col += nth)
+            column_solve(col, [&](long long q) {
+                const double sv = V.r[q] - alpha * V.v[q];
+                V.s[q] = sv;
+                return sv;
+            }, V.sh);
+        if (!sync()) return;
+        // ---- t = op sh; (t, s), (t, t)
+        {
+            double acc[2] = {0.0, 0.0};
+            cells([&](long long q, int i, int j, int kk) {
+                const double tv = th_ax<Tr>(k, S, V.sh, q, i, j, kk);
+                V.t[q] = tv;
+                acc[0] += tv * V.s[q];
+                acc[1] += tv * tv;
+            });
+            block_sum<2>(acc, sm);
+            if (threadIdx.x == 0) { pB[2 * blockIdx.x] = acc[0]; pB[2 * blockIdx.x + 1] = acc[1]; }
+        }
+        if (!sync()) return;
+        double ts[2];
+        sum_partials<2>(pB, G, 2, ts, sm);
+        omega = ts[1] > 0.0 ? ts[0] / ts[1] : 0.0;
+        // ---- x += alpha ph + omega sh; r = s - omega t; (r, r), (rh, r)
+        {
+            double acc[2] = {0.0, 0.0};
+            cells([&](long long q, int, int, int) {
+                V.x[q] += alpha * V.ph[q] + omega * V.sh[q];
+                const double r = V.s[q] - omega * V.t[q];
+                V.r[q] = r;
+                acc[0] += r * r;
+                acc[1] += V.rh[q] * r;
+            });
+            block_sum<2>(acc, sm);
+            if (threadIdx.x == 0) { pC[2 * blockIdx.x] = acc[0]; pC[2 * blockIdx.x + 1] = acc[1]; }
+        }
+        if (!sync()) return;
+        sum_partials<2>(pC, G, 2, tot, sm);
+        res = sqrt(tot[0]) / bnorm;
+        rho = rho1;
+        rho1 = tot[1];
+        if (!(res == res)) {
+            if (blockIdx.x == 0 && threadIdx.x == 0) atomicCAS(&st->err, 0, (int)CP_ERR_NONFINITE);
+            return;
+        }
+        if (res <= rtol) { conv = true; ++it; break; }
+        if (omega == 0.0) { ++it; break; }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        st->iterations = it;
+        st->converged = conv ? 1 : 0;
+        st->residual = res;
+    }
+}
+
+// bottom layer: partials of max T and sum T^p
+__global__ void k_th_pnorm(ThK k, const double* T, double pexp, double* part) {
+    __shared__ double sm[64];
+    __shared__ double smx[32];
+    double mx = -1e300, s[1] = {0.0};
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < k.ncol;
+         q += (long long)gridDim.x * blockDim.x) {
+        const double t = T[q];
+        mx = fmax(mx, t);
+        s[0] += pow(t, pexp);
+    }
+    block_sum<1>(s, sm);
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if ((threadIdx.x & 31) == 0) smx[threadIdx.x >> 5] = mx;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double m = -1e300;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, smx[w]);
+        part[2 * blockIdx.x] = m;
+        part[2 * blockIdx.x + 1] = s[0];
+    }
+}
+
+__global__ void k_th_fill(double* x, long long n, double v) {
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+        x[q] = v;
+}
+
+// dJ/dT of J = (mean over the bottom layer of T^p)^(1/p):
+// (T / J)^(p-1) / (Nx Ny) on k = 0, zero above
+__global__ void k_th_adj_rhs(ThK k, const double* T, double J, double pexp, double* rhs) {
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < k.n;
+         q += (long long)gridDim.x * blockDim.x)
+        rhs[q] = q < k.ncol ? pow(T[q] / J, pexp - 1.0) / (double)k.ncol : 0.0;
+}
+
+// dk/dgamma of a cell above the base plate at the clamped gamma; for RAMP
+// the reference's dk_dgamma (thermal_solver.cpp:317-321)
+__device__ __forceinline__ double th_dkdg(const ThK& k, double g) {
+    g = fmax(0.0, fmin(1.0, g));
+    if (k.mode == 1) {
+        const double den = 1.0 + k.qk * g;
+        return (k.kS - k.kF) * (-(1.0 + k.qk)) / (den * den);
+    }
+    if (k.mode == 2) {
+        const double den = (1.0 - g) * k.kF + g * k.kS + 1e-30;
+        return -k.kS * k.kF * (k.kS - k.kF) / (den * den);
+    }
+    return k.kF - k.kS;
+}
+
+// d harm(a, b) / da for harm = 2ab / (a + b + 1e-30)
+__device__ __forceinline__ double th_dharm(double a, double b) {
+    const double s = a + b + 1e-30;
+    return 2.0 * b * (b + 1e-30) / (s * s);
+}
+
+// dJ/dgamma(i, j) = -lambda^T dR/dgamma(i, j) for R = A(gamma) T - b(gamma),
+// one thread per column.  gamma(i, j) sets k of every cell of the column
+// above the base plate, which enters the x/y face conductances (harmonic
+// means), the inlet conductance 2 k Ax / dx and the z conductances
+// (thickness-weighted); the velocities and the fluid/solid masks are held
+// fixed (the mask is a step at gamma = 0.01 without a derivative).  A face
+// of conductance D between P and N contributes (l_P - l_N)(T_P - T_N) dD.
+__global__ void k_th_sens(ThK k, const double* gamma, const double* T, const double* lam, double* grad) {
+    const long long L = (long long)k.Nx * k.Ny;
+    const double dx = k.dx, dy = k.dy;
+    for (long long col = (long long)blockIdx.x * blockDim.x + threadIdx.x; col < k.ncol;
+         col += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(col % k.Nx), j = (int)(col / k.Nx);
+        double acc = 0.0;
+        for (int kk = k.nzS; kk < k.Nz; ++kk) {
+            const long long q = kk * L + col;
+            const double kP = th_kval(k, gamma, i, j, kk), dz = th_dz(k, kk);
+            const double Ax = dy * dz, Ay = dx * dz, lP = lam[q], TP = T[q];
+            if (i > 0)
+                acc += (lP - lam[q - 1]) * (TP - T[q - 1]) * th_dharm(kP, th_kval(k, gamma, i - 1, j, kk)) * Ax / dx;
+            if (i < k.Nx - 1)
+                acc += (lP - lam[q + 1]) * (TP - T[q + 1]) * th_dharm(kP, th_kval(k, gamma, i + 1, j, kk)) * Ax / dx;
+            if (j > 0)
+                acc += (lP - lam[q - k.Nx]) * (TP - T[q - k.Nx]) * th_dharm(kP, th_kval(k, gamma, i, j - 1, kk)) *
+                       Ay / dy;
+            if (j < k.Ny - 1)
+                acc += (lP - lam[q + k.Nx]) * (TP - T[q + k.Nx]) * th_dharm(kP, th_kval(k, gamma, i, j + 1, kk)) *
+                       Ay / dy;
+            if (i == 0 && th_fluid(k, gamma, i, j, kk)) acc += lP * (TP - k.Tin) * 2.0 * Ax / dx;
+        }
+        // z faces (kk, kk + 1) with a cell above the base plate
+        for (int kk = k.nzS - 1; kk < k.Nz - 1; ++kk) {
+            const long long q = kk * L + col;
+            const double kL = th_kval(k, gamma, i, j, kk), kU = th_kval(k, gamma, i, j, kk + 1);
+            const double dL = th_dz(k, kk), dU = th_dz(k, kk + 1), den = dL / kL + dU / kU;
+            double dkf = (dL + dU) * (dU / (kU * kU)) / (den * den);
+            if (kk >= k.nzS) dkf += (dL + dU) * (dL / (kL * kL)) / (den * den);
+            acc += (lam[q] - lam[q + L]) * (T[q] - T[q + L]) * dkf * (dx * dy) / (0.5 * (dL + dU));
+        }
+        grad[col] = -th_dkdg(k, gamma[col]) * acc;
+    }
+}
+
+}  // namespace cp
+
+using namespace cp;
+
+struct cp_thermal {
+    cp_thermal_params prm{};
+    ThK k{};
+    int dev = 0, numSMs = 0, grid = 0, gElem = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    double *gamma = nullptr, *u = nullptr, *v = nullptr, *q0 = nullptr;
+    ThSys S{};
+    double *lc = nullptr, *linv = nullptr, *lam = nullptr, *rhs = nullptr, *grad = nullptr;
+    ThVecs V{};
+    double* part = nullptr;
+    unsigned* bar = nullptr;
+    ThStatus* st = nullptr;
+    bool hasInputs = false, solved = false;
+    std::vector<void*> allocs;
+};
+
+namespace {
+
+cp_status th_alloc(cp_thermal* t, double** p, size_t n) {
+    void* q = nullptr;
+    TCK(cudaMalloc(&q, std::max<size_t>(n, 1) * sizeof(double)));
+    t->allocs.push_back(q);
+    TCK(cudaMemsetAsync(q, 0, std::max<size_t>(n, 1) * sizeof(double), t->stream));
+    *p = static_cast<double*>(q);
+    return CP_OK;
+}
+
+cp_status th_objective(cp_thermal* t, double p, double* Tb_max, double* Tb_pnorm) {
+    k_th_pnorm<<<t->gElem, kThThreads, 0, t->stream>>>(t->k, t->V.x, p, t->part);
+    TCK(cudaGetLastError());
+    std::vector<double> h((size_t)2 * t->gElem);
+    TCK(cudaMemcpyAsync(h.data(), t->part, h.size() * 8, cudaMemcpyDeviceToHost, t->stream));
+    TCK(cudaStreamSynchronize(t->stream));
+    double mx = -1e300, s = 0.0;
+    for (int b = 0; b < t->gElem; ++b) {
+        mx = std::max(mx, h[2 * b]);
+        s += h[2 * b + 1];
+    }
+    if (Tb_max) *Tb_max = mx;
+    if (Tb_pnorm) *Tb_pnorm = std::pow(s / (double)t->k.ncol, 1.0 / p);
+    return CP_OK;
+}
+
+// Column factorisation and the persistent BiCGStab for op x = rhs, op = A or
+// A^T, from V.x; records ev1 after the solve and reads the status back.
+template <bool Tr>
+cp_status th_krylov(cp_thermal* t, const double* rhs, const ThVecs& V, ThStatus* hs) {
+    const ThK& k = t->k;
+    k_th_lu<Tr><<<t->gElem, kThThreads, 0, t->stream>>>(k, t->S, t->lc, t->linv);
+    TCK(cudaGetLastError());
+    TCK(cudaMemsetAsync(t->bar, 0, sizeof(unsigned), t->stream));
+    TCK(cudaMemsetAsync(t->st, 0, sizeof(ThStatus), t->stream));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(t->grid);
+    cfg.blockDim = dim3(kThThreads);
+    cfg.stream = t->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    TCK(cudaLaunchKernelEx(&cfg, k_th_bicgstab<Tr>, k, t->S, rhs, (const double*)t->lc, (const double*)t->linv, V,
+                           t->part, t->bar, t->st, t->prm.maxiter, t->prm.rtol));
+    TCK(cudaEventRecord(t->ev1, t->stream));
+    TCK(cudaMemcpyAsync(hs, t->st, sizeof *hs, cudaMemcpyDeviceToHost, t->stream));
+    TCK(cudaStreamSynchronize(t->stream));
+    if (hs->err)
+        return tfail((cp_status)hs->err, "device reported %s in the thermal %s solve",
+                     cp_status_string((cp_status)hs->err), Tr ? "adjoint" : "forward");
+    return CP_OK;
+}
+
+void th_report(cp_thermal* t, const ThStatus& hs, cp_thermal_report* rep) {
+    if (!rep) return;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, t->ev0, t->ev1);
+    rep->iterations = hs.iterations;
+    rep->converged = hs.converged;
+    rep->residual = hs.residual;
+    rep->device_ms = ms;
+}
+
+}  // namespace
+
+extern "C" {
+
+void cp_thermal_params_default(cp_thermal_params* p) {
+    if (!p) return;
+    memset(p, 0, sizeof(*p));
+    p->nz_solid = 2;
+    p->nz_fluid = 7;
+    p->H_b = 0.0005;
+    p->H_t = 0.004;
+    p->k_s = 400.0;
+    p->k_f = 0.6;
+    p->rho = 998.0;
+    p->Cp = 4180.0;
+    p->T_inlet = 30.0;
+    p->rtol = 1e-6;
+    p->maxiter = 1000;
+    p->k_interp_mode = 1;
+    p->qk = 1.0;
+}
+
+cp_status cp_thermal_create(const cp_thermal_params* p, cp_thermal** out) {
+    if (!p || !out) return tfail(CP_ERR_BAD_PARAM, "NULL argument");
+    *out = nullptr;
+    if (p->Nx < 2 || p->Ny < 2 || p->nz_solid < 1 || p->nz_fluid < 1 || p->nz_solid + p->nz_fluid > kThMaxNz)
+        return tfail(CP_ERR_BAD_PARAM, "grid %d x %d x (%d + %d): need Nx, Ny >= 2, nz_solid, nz_fluid >= 1 "
+                     "and Nz <= %d", p->Nx, p->Ny, p->nz_solid, p->nz_fluid, kThMaxNz);
+    const double pos[] = {p->dx, p->dy, p->H_b, p->H_t, p->k_s, p->k_f, p->rho, p->Cp};
+    for (double x : pos)
+        if (!(x > 0.0) || !std::isfinite(x)) return tfail(CP_ERR_BAD_PARAM, "dx, dy, H_b, H_t, k, rho, Cp must be > 0");
+    if (!std::isfinite(p->T_inlet) || !(p->rtol >= 0.0) || p->maxiter < 0 || p->k_interp_mode < 0 ||
+        p->k_interp_mode > 2 || !std::isfinite(p->qk))
+        return tfail(CP_ERR_BAD_PARAM, "T_inlet, rtol, maxiter, k_interp_mode or qk out of range");
+    cp_thermal* t = new cp_thermal();
+    t->prm = *p;
+    auto bail = [&](cp_status s) {
+        cp_thermal_destroy(t);
+        return s;
+    };
+    if (cudaGetDevice(&t->dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&t->numSMs, cudaDevAttrMultiProcessorCount, t->dev) != cudaSuccess) {
+        cudaGetLastError();
+        delete t;
+        return tfail(CP_ERR_CUDA, "no CUDA device");
+    }
+    if (cudaStreamCreateWithFlags(&t->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&t->ev0) != cudaSuccess || cudaEventCreate(&t->ev1) != cudaSuccess)
+        return bail(tfail(CP_ERR_CUDA, "stream / events"));
+    ThK& k = t->k;
+    k.Nx = p->Nx; k.Ny = p->Ny; k.nzS = p->nz_solid; k.nzF = p->nz_fluid; k.Nz = k.nzS + k.nzF;
+    k.mode = p->k_interp_mode;
+    k.ncol = (long long)k.Nx * k.Ny;
+    k.n = k.ncol * k.Nz;
+    // the reference keeps the domain length and divides it again (thermal_solver.cpp:186-187, 729)
+    k.dx = (k.Nx * p->dx) / k.Nx;
+    k.dy = (k.Ny * p->dy) / k.Ny;
+    k.dzS = p->H_b / p->nz_solid;
+    k.dzF = p->H_t / p->nz_fluid;
+    k.Ht = p->H_t; k.kS = p->k_s; k.kF = p->k_f; k.rhoCp = p->rho * p->Cp; k.Tin = p->T_inlet; k.qk = p->qk;
+    const size_t n = (size_t)k.n, nc = (size_t)k.ncol;
+    cp_status s;
+    double** planes[] = {&t->gamma, &t->u, &t->v, &t->q0, &t->grad};
+    for (double** q : planes)
+        if ((s = th_alloc(t, q, nc)) != CP_OK) return bail(s);
+    double** vols[] = {&t->S.aP, &t->S.aW, &t->S.aE, &t->S.aS, &t->S.aN, &t->S.aB, &t->S.aT, &t->S.b,
+                       &t->lc,   &t->linv, &t->V.x,  &t->V.r,  &t->V.rh, &t->V.p,  &t->V.v,  &t->V.s,
+                       &t->V.t,  &t->V.ph, &t->V.sh, &t->lam,  &t->rhs};
+    for (double** q : vols)
+        if ((s = th_alloc(t, q, n)) != CP_OK) return bail(s);
+    // the forward and the adjoint kernel run on the same grid: every block resident
+    int nb = 0, nbT = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_th_bicgstab<false>, kThThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nbT, k_th_bicgstab<true>, kThThreads, 0);
+    nb = std::min(nb, nbT);
+    if (nb < 1) return bail(tfail(CP_ERR_CUDA, "the thermal solver kernel does not fit on an SM"));
+    t->grid = t->numSMs * std::min(nb, 4);
+    t->gElem = t->numSMs * 4;
+    if ((s = th_alloc(t, &t->part, (size_t)6 * kMaxBlocks)) != CP_OK) return bail(s);
+    void* q = nullptr;
+    if (cudaMalloc(&q, 64) != cudaSuccess) return bail(tfail(CP_ERR_CUDA, "cudaMalloc"));
+    t->allocs.push_back(q);
+    t->bar = static_cast<unsigned*>(q);
+    if (cudaMalloc(&q, sizeof(ThStatus)) != cudaSuccess) return bail(tfail(CP_ERR_CUDA, "cudaMalloc"));
+    t->allocs.push_back(q);
+    t->st = static_cast<ThStatus*>(q);
+    if (cudaStreamSynchronize(t->stream) != cudaSuccess) return bail(tfail(CP_ERR_CUDA, "stream"));
+    *out = t;
+    return CP_OK;
+}
+
+cp_status cp_thermal_destroy(cp_thermal* t) {
+    if (!t) return CP_OK;
+    if (t->stream) cudaStreamSynchronize(t->stream);
+    for (void* q : t->allocs) cudaFree(q);
+    if (t->ev0) cudaEventDestroy(t->ev0);
+    if (t->ev1) cudaEventDestroy(t->ev1);
+    if (t->stream) cudaStreamDestroy(t->stream);
+    delete t;
+    return CP_OK;
+}
+
+cp_status cp_thermal_set_inputs(cp_thermal* t, const double* gamma, const double* u, const double* v,
+                                const double* q0) {
+    if (!t || !gamma || !u || !v || !q0) return tfail(CP_ERR_BAD_PARAM, "NULL argument");
+    const size_t nc = (size_t)t->k.ncol;
+    const double* src[] = {gamma, u, v, q0};
+    for (const double* a : src)
+        for (size_t q = 0; q < nc; ++q)
+            if (!std::isfinite(a[q])) return tfail(CP_ERR_NONFINITE, "non-finite input at %zu", q);
+    TCK(cudaMemcpyAsync(t->gamma, gamma, nc * 8, cudaMemcpyHostToDevice, t->stream));
+    TCK(cudaMemcpyAsync(t->u, u, nc * 8, cudaMemcpyHostToDevice, t->stream));
+    TCK(cudaMemcpyAsync(t->v, v, nc * 8, cudaMemcpyHostToDevice, t->stream));
+    TCK(cudaMemcpyAsync(t->q0, q0, nc * 8, cudaMemcpyHostToDevice, t->stream));
+    TCK(cudaStreamSynchronize(t->stream));
+    t->hasInputs = true;
+    t->solved = false;
+    return CP_OK;
+}
+
+cp_status cp_thermal_solve(cp_thermal* t, cp_thermal_report* rep) {
+    if (!t) return tfail(CP_ERR_BAD_PARAM, "NULL argument");
+    if (!t->hasInputs) return tfail(CP_ERR_STATE, "cp_thermal_set_inputs first");
+    const ThK& k = t->k;
+    t->solved = false;
+    TCK(cudaEventRecord(t->ev0, t->stream));
+    k_th_assemble<<<t->gElem, kThThreads, 0, t->stream>>>(k, t->gamma, t->u, t->v, t->q0, t->S);
+    TCK(cudaGetLastError());
+    // initial guess T = T_inlet
+    k_th_fill<<<t->gElem, kThThreads, 0, t->stream>>>(t->V.x, k.n, t->prm.T_inlet);
+    TCK(cudaGetLastError());
+    ThStatus hs;
+    cp_status s = th_krylov<false>(t, t->S.b, t->V, &hs);
+    if (s != CP_OK) return s;
+    t->solved = true;
+    th_report(t, hs, rep);
+    return CP_OK;
+}
+
+cp_status cp_thermal_get_T(cp_thermal* t, double* T) {
+    if (!t || !T) return tfail(CP_ERR_BAD_PARAM, "NULL argument");
+    if (!t->solved) return tfail(CP_ERR_STATE, "no solution yet (cp_thermal_solve)");
+    TCK(cudaMemcpyAsync(T, t->V.x, (size_t)t->k.n * 8, cudaMemcpyDeviceToHost, t->stream));
+    TCK(cudaStreamSynchronize(t->stream));
+    return CP_OK;
+}
+
+cp_status cp_thermal_objective(cp_thermal* t, double p, double* Tb_max, double* Tb_pnorm) {
+    if (!t) return tfail(CP_ERR_BAD_PARAM, "NULL argument");
+    if (!t->solved) return tfail(CP_ERR_STATE, "no solution yet (cp_thermal_solve)");
+    if (!(p > 0.0) || !std::isfinite(p)) return tfail(CP_ERR_BAD_PARAM, "p must be > 0");
+    return th_objective(t, p, Tb_max, Tb_pnorm);
+}
+
+cp_status cp_thermal_pnorm_gradient(cp_thermal* t, double p, double* J, double* dJ_dgamma, cp_thermal_report* rep) {
+    if (!t || !dJ_dgamma) return tfail(CP_ERR_BAD_PARAM, "NULL argument");
+    if (!t->solved) return tfail(CP_ERR_STATE, "no solution yet (cp_thermal_solve)");
+    if (!(p >= 1.0) || !std::isfinite(p)) return tfail(CP_ERR_BAD_PARAM, "p must be >= 1");
+    const ThK& k = t->k;
+    double Jv = 0.0;
+    cp_status s = th_objective(t, p, nullptr, &Jv);
+    if (s != CP_OK) return s;
+    if (!(Jv > 0.0) || !std::isfinite(Jv))
+        return tfail(CP_ERR_NONFINITE, "the p-norm of the bottom temperatures is %g", Jv);
+    TCK(cudaEventRecord(t->ev0, t->stream));
+    k_th_adj_rhs<<<t->gElem, kThThreads, 0, t->stream>>>(k, t->V.x, Jv, p, t->rhs);
+    TCK(cudaGetLastError());
+    TCK(cudaMemsetAsync(t->lam, 0, (size_t)k.n * 8, t->stream));
+    ThVecs W = t->V;
+    W.x = t->lam;
+    ThStatus hs;
+    s = th_krylov<true>(t, t->rhs, W, &hs);
+    if (s != CP_OK) return s;
+    k_th_sens<<<t->gElem, kThThreads, 0, t->stream>>>(k, t->gamma, t->V.x, t->lam, t->grad);
+    TCK(cudaGetLastError());
+    TCK(cudaEventRecord(t->ev1, t->stream));
+    TCK(cudaMemcpyAsync(dJ_dgamma, t->grad, (size_t)k.ncol * 8, cudaMemcpyDeviceToHost, t->stream));
+    TCK(cudaStreamSynchronize(t->stream));
+    if (J) *J = Jv;
+    th_report(t, hs, rep);
+    return CP_OK;
+}
+
+}  // extern "C"

@@ -234,6 +234,71 @@ def pnorm(T: np.ndarray, pexp: float) -> float:
     return float(np.power(np.sum(np.power(Tb, pexp)) / Tb.size, 1.0 / pexp))
 
 
+def dk_dgamma(p: ThermalParams, g: np.ndarray) -> np.ndarray:
+    """dk/dgamma above the base plate at the clamped gamma; for RAMP the
+    reference's dk_dgamma (thermal_solver.cpp:317-321)."""
+    g = np.clip(g, 0.0, 1.0)
+    if p.k_interp_mode == 1:
+        den = 1.0 + p.qk * g
+        return (p.k_s - p.k_f) * (-(1.0 + p.qk)) / (den * den)
+    if p.k_interp_mode == 2:
+        den = (1.0 - g) * p.k_f + g * p.k_s + 1e-30
+        return -p.k_s * p.k_f * (p.k_s - p.k_f) / (den * den)
+    return np.full_like(g, p.k_f - p.k_s)
+
+
+def pnorm_gradient(p: ThermalParams, gamma, u_xy, v_xy, q0, pexp: float):
+    """(J, dJ/dgamma (Ny x Nx), T, lambda) of J = (mean over the bottom
+    layer of T^p)^(1/p) by the discrete adjoint of the assembled system:
+    A^T lambda = dJ/dT, dJ/dgamma = -lambda^T dR/dgamma for R = A T - b,
+    with velocities and fluid masks fixed.  gamma enters through the
+    conductivity of the cells above the base plate: the x/y face
+    conductances harm(k_P, k_N) A / h, the inlet conductance 2 k Ax / dx and
+    the z conductances.  The reference computes no sensitivity
+    (thermal_solver.cpp:377-378 fills zeros), so this is pinned by central
+    finite differences of J (tests/test_thermal_oracle.py)."""
+    import scipy.sparse.linalg as spl
+    Nx, Ny, Nz, nzS = p.Nx, p.Ny, p.Nz, p.nz_solid
+    A, b = assemble(p, gamma, u_xy, v_xy, q0)
+    T = spl.spsolve(A.tocsc(), b)
+    Tb = T[:Nx * Ny]
+    J = float(np.power(np.sum(np.power(Tb, pexp)) / Tb.size, 1.0 / pexp))
+    rhs = np.zeros_like(T)
+    rhs[:Nx * Ny] = np.power(Tb / J, pexp - 1.0) / (Nx * Ny)
+    lam = spl.spsolve(A.T.tocsc(), rhs)
+    T3, L3 = T.reshape(Nz, Ny, Nx), lam.reshape(Nz, Ny, Nx)
+    dx, dy = (Nx * p.dx) / Nx, (Ny * p.dy) / Ny
+    dz = np.array([p.H_b / p.nz_solid] * p.nz_solid + [p.H_t / p.nz_fluid] * p.nz_fluid)
+    gam = np.asarray(gamma, dtype=np.float64)
+    K = np.empty((Nz, Ny, Nx))
+    K[:nzS] = p.k_s
+    K[nzS:] = kval_layer(p, gam)
+    fluid = gam > 0.01
+
+    def dharm(a, c):            # d/da of 2ac / (a + c + 1e-30)
+        s_ = a + c + 1e-30
+        return 2.0 * c * (c + 1e-30) / (s_ * s_)
+
+    acc = np.zeros((Ny, Nx))
+    for k in range(nzS, Nz):
+        t, lm, kk = T3[k], L3[k], K[k]
+        gx = dy * dz[k] / dx       # Ax / dx
+        gy = dx * dz[k] / dy       # Ay / dy
+        acc[:, 1:] += (lm[:, 1:] - lm[:, :-1]) * (t[:, 1:] - t[:, :-1]) * dharm(kk[:, 1:], kk[:, :-1]) * gx
+        acc[:, :-1] += (lm[:, :-1] - lm[:, 1:]) * (t[:, :-1] - t[:, 1:]) * dharm(kk[:, :-1], kk[:, 1:]) * gx
+        acc[1:, :] += (lm[1:, :] - lm[:-1, :]) * (t[1:, :] - t[:-1, :]) * dharm(kk[1:, :], kk[:-1, :]) * gy
+        acc[:-1, :] += (lm[:-1, :] - lm[1:, :]) * (t[:-1, :] - t[1:, :]) * dharm(kk[:-1, :], kk[1:, :]) * gy
+        acc[:, 0] += np.where(fluid[:, 0], lm[:, 0] * (t[:, 0] - p.T_inlet) * 2.0 * gx, 0.0)
+    for k in range(nzS - 1, Nz - 1):
+        kL, kU, dL, dU = K[k], K[k + 1], dz[k], dz[k + 1]
+        den = dL / kL + dU / kU
+        dkf = (dL + dU) * (dU / (kU * kU)) / (den * den)
+        if k >= nzS:
+            dkf = dkf + (dL + dU) * (dL / (kL * kL)) / (den * den)
+        acc += (L3[k] - L3[k + 1]) * (T3[k] - T3[k + 1]) * dkf * (dx * dy) / (0.5 * (dL + dU))
+    return J, -dk_dgamma(p, gam) * acc, T3, L3
+
+
 def read_dump(path: str):
     """n, CSR (ptr, col, val), b, x written by the AMGCL stand-in."""
     import scipy.sparse as sp

@@ -1,6 +1,7 @@
 """The C ABI library without a GPU: it builds, loads, exports every function
-include/cp_simple.h declares, and the ctypes structs match the C layout."""
+the headers in include/ declare, and the ctypes structs match the C layout."""
 import ctypes
+import glob
 import os
 import re
 import subprocess
@@ -9,21 +10,23 @@ import tempfile
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-HEADER = os.path.join(ROOT, "include", "cp_simple.h")
+HEADERS = sorted(glob.glob(os.path.join(ROOT, "include", "*.h")))
 
 
 def declared_functions():
-    src = open(HEADER).read()
-    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
-    names = re.findall(r"^\s*(?:const\s+)?[a-z_]+\s*\*?\s*(cp_[a-z0-9_]+)\s*\(", src, flags=re.M)
-    return sorted(set(names))
+    names = set()
+    for h in HEADERS:
+        src = re.sub(r"/\*.*?\*/", "", open(h).read(), flags=re.S)
+        names.update(re.findall(r"^\s*(?:const\s+)?[a-z_]+\s*\*?\s*(cp_[a-z0-9_]+)\s*\(", src, flags=re.M))
+    return sorted(names)
 
 
 def test_header_declares_the_boundary():
     names = declared_functions()
     for must in ("cp_create", "cp_destroy", "cp_step", "cp_run", "cp_momentum_u", "cp_momentum_v",
                  "cp_pressure", "cp_get_field", "cp_set_field", "cp_get_history", "cp_params_default",
-                 "cp_last_error_string"):
+                 "cp_last_error_string", "cp_pressure_noalloc", "cp_batch_run", "cp_thermal_solve",
+                 "cp_thermal_pnorm_gradient"):
         assert must in names
 
 
@@ -52,7 +55,7 @@ def test_defaults_are_the_reference_defaults(built_lib):
 
 
 def _c_offsets(struct_name, fields):
-    prog = ["#include <stdio.h>", "#include <stddef.h>", f'#include "{HEADER}"', "int main(void){"]
+    prog = ["#include <stdio.h>", "#include <stddef.h>"] + [f'#include "{h}"' for h in HEADERS] + ["int main(void){"]
     prog.append(f'printf("%zu\\n", sizeof({struct_name}));')
     for f in fields:
         prog.append(f'printf("%zu\\n", offsetof({struct_name}, {f}));')
@@ -66,13 +69,15 @@ def _c_offsets(struct_name, fields):
     return [int(x) for x in out]
 
 
-@pytest.mark.parametrize("which", ["params", "report", "adjoint", "batch", "timing"])
+@pytest.mark.parametrize("which", ["params", "report", "adjoint", "batch", "timing", "thermal", "thermal_report"])
 def test_ctypes_layout_matches_c(which):
     from coldplate_b200 import _native as nat
     cls, name = {"params": (nat.CpParams, "cp_params"), "report": (nat.CpIterReport, "cp_iter_report"),
                  "adjoint": (nat.CpAdjointReport, "cp_adjoint_report"),
                  "batch": (nat.CpBatchReport, "cp_batch_report"),
-                 "timing": (nat.CpKernelTiming, "cp_kernel_timing")}[which]
+                 "timing": (nat.CpKernelTiming, "cp_kernel_timing"),
+                 "thermal": (nat.CpThermalParams, "cp_thermal_params"),
+                 "thermal_report": (nat.CpThermalReport, "cp_thermal_report")}[which]
     fields = cls._fields_
     c = _c_offsets(name, [f for f, _ in fields])
     assert c[0] == ctypes.sizeof(cls)
