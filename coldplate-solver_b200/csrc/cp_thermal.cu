@@ -2,18 +2,26 @@
 //
 // The reference (ThermalSolver/thermal_solver.cpp) assembles a 7-point
 // finite-volume system on Nx x Ny x Nz cells into CSR on the host and solves
-// it with AMGCL's IDR(s) (thermal_solver.cpp:417-553).  Here:
+// it with AMGCL's IDR(s) preconditioned by smoothed-aggregation AMG
+// (thermal_solver.cpp:417-553).  Here:
 //   k_th_assemble   one thread per cell computes the reference's row in FP64
 //                   (same formulas and summation order, thermal_solver.cpp:
 //                   420-520) into seven coefficient arrays and b;
-//   k_th_lu         factors the tridiagonal z-block of every (i, j) column
-//                   (the strongly coupled direction: thin layers);
-//   k_th_bicgstab   persistent cooperative BiCGStab, right-preconditioned by
-//                   exact solves of the z-columns.  The column phases fuse
-//                   the vector update with the column solve; five bounded
-//                   grid barriers per iteration; deterministic block sums;
-//                   AMGCL's stop test ||r|| <= rtol ||b||.  The same kernel
-//                   solves A^T x = rhs for the p-norm adjoint;
+//   k_th_coarsen    Galerkin coarse operators P^T A P of a hierarchy that
+//                   aggregates 2 x 2 columns (all z-layers kept) down to one
+//                   column; P piecewise constant, so every level keeps the
+//                   7-point form and the levels of A^T are the transposes;
+//   k_th_lu         Thomas factors of every column's tridiagonal z-block, per
+//                   level (z is the direction a column thread owns);
+//   k_th_bicgstab   persistent cooperative BiCGStab right-preconditioned by
+//                   one V-cycle: damped z-line Jacobi smoothing (one sweep
+//                   down, one up; exact on the one-column level), residual
+//                   restriction fused with the 2 x 2 sums, prolongation fused
+//                   with the post-smoothing sweep; levels of at most
+//                   kThCtaCols columns run in block 0 alone.  Bounded grid
+//                   barriers, deterministic block sums, AMGCL's stop test
+//                   ||r|| <= rtol ||b||.  The same kernel solves A^T x = rhs
+//                   for the p-norm adjoint;
 //   k_th_sens       dJ/dgamma from the adjoint field, one thread per column.
 // Layout: every array is indexed k Nx Ny + j Nx + i (i contiguous), so the
 // stencil loads of a warp are coalesced and a column thread walks k with
@@ -24,6 +32,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -54,6 +63,10 @@ cp_status tfail(cp_status s, const char* fmt, ...) {
 
 constexpr int kThThreads = 256;
 constexpr int kThMaxNz = 64;
+constexpr int kThMaxLevels = 16;          // 2 x 2 aggregation from up to 2^15 columns per side
+constexpr long long kThCtaCols = 1024;    // levels of at most this many columns: block 0 alone
+constexpr double kThOmega = 0.8;          // z-line Jacobi damping
+constexpr double kThScale = 1.3;          // coarse-correction factor
 
 }  // namespace
 
@@ -204,9 +217,28 @@ __global__ void k_th_assemble(ThK k, const double* gamma, const double* u_xy, co
     }
 }
 
-// z-coupling of row q of A (Tr = false) or of A^T (Tr = true): the entry
-// towards k-1 and towards k+1.  Row q of A^T holds column q of A, so its
-// k-1 entry is A's aT of the cell below and its k+1 entry A's aB above.
+// One level of the hierarchy (level 0: the assembled system).  x holds the
+// pre-smoothed iterate, b the restricted residual and y the post-smoothed
+// iterate of a coarse level.
+struct ThLevel {
+    int nx, ny;
+    long long ncol, n;
+    ThSys S;
+    double *lc, *linv;
+    double *b, *x, *y;
+};
+
+// Entries of row q of A (Tr = false) or of A^T (Tr = true) towards the
+// west, east, south, north, lower and upper neighbour.  Row q of A^T holds
+// column q of A: its west entry is the east coefficient of the west cell.
+template <bool Tr>
+__device__ __forceinline__ double th_cW(const ThSys& S, long long q) { return Tr ? S.aE[q - 1] : S.aW[q]; }
+template <bool Tr>
+__device__ __forceinline__ double th_cE(const ThSys& S, long long q) { return Tr ? S.aW[q + 1] : S.aE[q]; }
+template <bool Tr>
+__device__ __forceinline__ double th_cS(const ThSys& S, long long q, int nx) { return Tr ? S.aN[q - nx] : S.aS[q]; }
+template <bool Tr>
+__device__ __forceinline__ double th_cN(const ThSys& S, long long q, int nx) { return Tr ? S.aS[q + nx] : S.aN[q]; }
 template <bool Tr>
 __device__ __forceinline__ double th_sub(const ThSys& S, long long q, long long L) {
     return Tr ? S.aT[q - L] : S.aB[q];
@@ -216,94 +248,322 @@ __device__ __forceinline__ double th_sup(const ThSys& S, long long q, long long 
     return Tr ? S.aB[q + L] : S.aT[q];
 }
 
-// Thomas factors of each column's tridiagonal z-block: inv_k = 1 / (d_k -
-// sub_k c_{k-1}), c_k = sup_k inv_k
+// (op x)_q on a level, op = A or A^T
 template <bool Tr>
-__global__ void k_th_lu(ThK k, ThSys S, double* lc, double* linv) {
-    const long long L = (long long)k.Nx * k.Ny;
-    for (long long col = (long long)blockIdx.x * blockDim.x + threadIdx.x; col < k.ncol;
+__device__ __forceinline__ double th_ax(const ThLevel& F, int Nz, const double* x, long long q, int i, int j,
+                                        int kk) {
+    const long long L = F.ncol;
+    double s = F.S.aP[q] * x[q];
+    if (i > 0) s += th_cW<Tr>(F.S, q) * x[q - 1];
+    if (i < F.nx - 1) s += th_cE<Tr>(F.S, q) * x[q + 1];
+    if (j > 0) s += th_cS<Tr>(F.S, q, F.nx) * x[q - F.nx];
+    if (j < F.ny - 1) s += th_cN<Tr>(F.S, q, F.nx) * x[q + F.nx];
+    if (kk > 0) s += th_sub<Tr>(F.S, q, L) * x[q - L];
+    if (kk < Nz - 1) s += th_sup<Tr>(F.S, q, L) * x[q + L];
+    return s;
+}
+
+// Galerkin coarse operator P^T A P of 2 x 2 column aggregates, P piecewise
+// constant: couplings inside an aggregate fold into the diagonal, couplings
+// across an aggregate edge add up into the coarse neighbour's entry.
+__global__ void k_th_coarsen(int Nz, ThLevel F, ThLevel C) {
+    for (long long qc = (long long)blockIdx.x * blockDim.x + threadIdx.x; qc < C.n;
+         qc += (long long)gridDim.x * blockDim.x) {
+        const int kk = (int)(qc / C.ncol);
+        const long long rem = qc - kk * C.ncol;
+        const int I = (int)(rem % C.nx), J = (int)(rem / C.nx);
+        double aP = 0, aW = 0, aE = 0, aS = 0, aN = 0, aB = 0, aT = 0;
+        for (int dj = 0; dj < 2; ++dj) {
+            const int j = 2 * J + dj;
+            if (j >= F.ny) break;
+            for (int di = 0; di < 2; ++di) {
+                const int i = 2 * I + di;
+                if (i >= F.nx) break;
+                const long long q = kk * F.ncol + (long long)j * F.nx + i;
+                aP += F.S.aP[q];
+                aB += F.S.aB[q];
+                aT += F.S.aT[q];
+                if (di == 1) aP += F.S.aW[q]; else aW += F.S.aW[q];
+                if (di == 0 && i + 1 < F.nx) aP += F.S.aE[q]; else aE += F.S.aE[q];
+                if (dj == 1) aP += F.S.aS[q]; else aS += F.S.aS[q];
+                if (dj == 0 && j + 1 < F.ny) aP += F.S.aN[q]; else aN += F.S.aN[q];
+            }
+        }
+        C.S.aP[qc] = aP; C.S.aW[qc] = aW; C.S.aE[qc] = aE; C.S.aS[qc] = aS; C.S.aN[qc] = aN;
+        C.S.aB[qc] = aB; C.S.aT[qc] = aT;
+    }
+}
+
+// Thomas factors of each column's tridiagonal z-block of a level:
+// inv_k = 1 / (d_k - sub_k c_{k-1}), c_k = sup_k inv_k
+template <bool Tr>
+__global__ void k_th_lu(int Nz, ThLevel F) {
+    const long long L = F.ncol;
+    for (long long col = (long long)blockIdx.x * blockDim.x + threadIdx.x; col < F.ncol;
          col += (long long)gridDim.x * blockDim.x) {
         double cprev = 0.0;
-        for (int kk = 0; kk < k.Nz; ++kk) {
+        for (int kk = 0; kk < Nz; ++kk) {
             const long long q = kk * L + col;
-            const double den = S.aP[q] - (kk > 0 ? th_sub<Tr>(S, q, L) * cprev : 0.0);
+            const double den = F.S.aP[q] - (kk > 0 ? th_sub<Tr>(F.S, q, L) * cprev : 0.0);
             const double inv = 1.0 / den;
-            const double c = (kk < k.Nz - 1 ? th_sup<Tr>(S, q, L) : 0.0) * inv;
-            linv[q] = inv;
-            lc[q] = c;
+            const double c = (kk < Nz - 1 ? th_sup<Tr>(F.S, q, L) : 0.0) * inv;
+            F.linv[q] = inv;
+            F.lc[q] = c;
             cprev = c;
         }
     }
 }
 
-// (A x)_P (Tr = false) or (A^T x)_P (Tr = true) from the stored rows: row P
-// of A^T takes each neighbour's coefficient towards P
-template <bool Tr>
-__device__ __forceinline__ double th_ax(const ThK& k, const ThSys& S, const double* x, long long q, int i, int j,
-                                        int kk) {
-    const long long L = (long long)k.Nx * k.Ny;
-    double s = S.aP[q] * x[q];
-    if (i > 0) s += (Tr ? S.aE[q - 1] : S.aW[q]) * x[q - 1];
-    if (i < k.Nx - 1) s += (Tr ? S.aW[q + 1] : S.aE[q]) * x[q + 1];
-    if (j > 0) s += (Tr ? S.aN[q - k.Nx] : S.aS[q]) * x[q - k.Nx];
-    if (j < k.Ny - 1) s += (Tr ? S.aS[q + k.Nx] : S.aN[q]) * x[q + k.Nx];
-    if (kk > 0) s += (Tr ? S.aT[q - L] : S.aB[q]) * x[q - L];
-    if (kk < k.Nz - 1) s += (Tr ? S.aB[q + L] : S.aT[q]) * x[q + L];
-    return s;
+// Pre-smoothing from zero: x = omega Mz^-1 b over the columns of a level,
+// b_k given by bin(q) (so the caller can fuse the vector update that makes
+// b; with bout set, b is also stored there).  The column is walked in
+// chunks of kThChunk layers whose loads are issued together before the
+// recurrence runs over them, so a column costs a few memory latencies
+// rather than one per layer.
+template <bool Tr, int kThChunk, typename Bin>
+__device__ __forceinline__ void th_presmooth(const ThLevel& F, int Nz, Bin&& bin, double* bout, double* x,
+                                             double omega, long long t0, long long nt) {
+    const long long L = F.ncol;
+    for (long long col = t0; col < F.ncol; col += nt) {
+        double yprev = 0.0;
+        for (int k0 = 0; k0 < Nz; k0 += kThChunk) {
+            double bv[kThChunk], sub[kThChunk], li[kThChunk];
+#pragma unroll
+            for (int u = 0; u < kThChunk; ++u) {
+                const int kk = k0 + u;
+                if (kk < Nz) {
+                    const long long q = kk * L + col;
+                    bv[u] = bin(q);
+                    sub[u] = kk > 0 ? th_sub<Tr>(F.S, q, L) : 0.0;
+                    li[u] = F.linv[q];
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kThChunk; ++u) {
+                const int kk = k0 + u;
+                if (kk < Nz) {
+                    const long long q = kk * L + col;
+                    yprev = (bv[u] - sub[u] * yprev) * li[u];
+                    x[q] = yprev;
+                    if (bout) bout[q] = bv[u];
+                }
+            }
+        }
+        double xn = 0.0;
+        for (int k0 = ((Nz - 1) / kThChunk) * kThChunk; k0 >= 0; k0 -= kThChunk) {
+            double yv[kThChunk], lcv[kThChunk];
+#pragma unroll
+            for (int u = 0; u < kThChunk; ++u) {
+                const int kk = k0 + u;
+                if (kk < Nz) {
+                    const long long q = kk * L + col;
+                    yv[u] = x[q];
+                    lcv[u] = F.lc[q];
+                }
+            }
+#pragma unroll
+            for (int u = kThChunk - 1; u >= 0; --u) {
+                const int kk = k0 + u;
+                if (kk < Nz) {
+                    const double xv = yv[u] - (kk < Nz - 1 ? lcv[u] * xn : 0.0);
+                    x[kk * L + col] = omega * xv;
+                    xn = xv;
+                }
+            }
+        }
+    }
 }
+
+// Residual restriction: bC = sum over the 2 x 2 aggregate of (bF - op xF)
+template <bool Tr>
+__device__ __forceinline__ void th_restrict(const ThLevel& F, const ThLevel& C, int Nz, const double* bF,
+                                            const double* xF, double* bC, long long t0, long long nt) {
+    for (long long qc = t0; qc < C.n; qc += nt) {
+        const int kk = (int)(qc / C.ncol);
+        const long long rem = qc - kk * C.ncol;
+        const int I = (int)(rem % C.nx), J = (int)(rem / C.nx);
+        double s = 0.0;
+        for (int dj = 0; dj < 2; ++dj) {
+            const int j = 2 * J + dj;
+            if (j >= F.ny) break;
+            for (int di = 0; di < 2; ++di) {
+                const int i = 2 * I + di;
+                if (i >= F.nx) break;
+                const long long q = kk * F.ncol + (long long)j * F.nx + i;
+                s += bF[q] - th_ax<Tr>(F, Nz, xF, q, i, j, kk);
+            }
+        }
+        bC[qc] = s;
+    }
+}
+
+// Prolongation and post-smoothing in one sweep over the fine columns:
+// xp = xF + scale P xC (formed on the fly, neighbours included), then
+// out = xp + omega Mz^-1 (bF - op xp); chunks of kThChunkPost layers
+// (about 16 loads a layer) as in th_presmooth
+template <bool Tr, int kThChunkPost>
+__device__ __forceinline__ void th_postsmooth(const ThLevel& F, const ThLevel& C, int Nz, const double* bF,
+                                              const double* xF, const double* xC, double scale, double omega,
+                                              double* out, long long t0, long long nt) {
+    const long long L = F.ncol, LC = C.ncol;
+    for (long long col = t0; col < F.ncol; col += nt) {
+        const int i = (int)(col % F.nx), j = (int)(col / F.nx);
+        const long long c0 = (long long)(j >> 1) * C.nx + (i >> 1);
+        const long long cw = i > 0 ? (long long)(j >> 1) * C.nx + ((i - 1) >> 1) : c0;
+        const long long ce = i < F.nx - 1 ? (long long)(j >> 1) * C.nx + ((i + 1) >> 1) : c0;
+        const long long cs = j > 0 ? (long long)((j - 1) >> 1) * C.nx + (i >> 1) : c0;
+        const long long cn = j < F.ny - 1 ? (long long)((j + 1) >> 1) * C.nx + (i >> 1) : c0;
+        double yprev = 0.0, xm = 0.0;
+        for (int k0 = 0; k0 < Nz; k0 += kThChunkPost) {
+            double xp[kThChunkPost + 1], rr[kThChunkPost], sub[kThChunkPost], li[kThChunkPost];
+#pragma unroll
+            for (int u = 0; u <= kThChunkPost; ++u) {
+                const int kk = k0 + u;
+                xp[u] = kk < Nz ? xF[kk * L + col] + scale * xC[kk * LC + c0] : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < kThChunkPost; ++u) {
+                const int kk = k0 + u;
+                if (kk < Nz) {
+                    const long long q = kk * L + col, kc = kk * LC;
+                    double ax = F.S.aP[q] * xp[u];
+                    if (i > 0) ax += th_cW<Tr>(F.S, q) * (xF[q - 1] + scale * xC[kc + cw]);
+                    if (i < F.nx - 1) ax += th_cE<Tr>(F.S, q) * (xF[q + 1] + scale * xC[kc + ce]);
+                    if (j > 0) ax += th_cS<Tr>(F.S, q, F.nx) * (xF[q - F.nx] + scale * xC[kc + cs]);
+                    if (j < F.ny - 1) ax += th_cN<Tr>(F.S, q, F.nx) * (xF[q + F.nx] + scale * xC[kc + cn]);
+                    sub[u] = kk > 0 ? th_sub<Tr>(F.S, q, L) : 0.0;
+                    if (kk < Nz - 1) ax += th_sup<Tr>(F.S, q, L) * xp[u + 1];
+                    rr[u] = bF[q] - ax;
+                    li[u] = F.linv[q];
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kThChunkPost; ++u) {
+                const int kk = k0 + u;
+                if (kk < Nz) {
+                    const double r = rr[u] - (kk > 0 ? sub[u] * xm : 0.0);
+                    xm = xp[u];
+                    yprev = (r - sub[u] * yprev) * li[u];
+                    out[kk * L + col] = yprev;
+                }
+            }
+        }
+        double cnext = 0.0;
+        for (int k0 = ((Nz - 1) / kThChunkPost) * kThChunkPost; k0 >= 0; k0 -= kThChunkPost) {
+            double yv[kThChunkPost], lcv[kThChunkPost], xv[kThChunkPost];
+#pragma unroll
+            for (int u = 0; u < kThChunkPost; ++u) {
+                const int kk = k0 + u;
+                if (kk < Nz) {
+                    const long long q = kk * L + col;
+                    yv[u] = out[q];
+                    lcv[u] = F.lc[q];
+                    xv[u] = xF[q] + scale * xC[kk * LC + c0];
+                }
+            }
+#pragma unroll
+            for (int u = kThChunkPost - 1; u >= 0; --u) {
+                const int kk = k0 + u;
+                if (kk < Nz) {
+                    const double corr = yv[u] - (kk < Nz - 1 ? lcv[u] * cnext : 0.0);
+                    out[kk * L + col] = xv[u] + omega * corr;
+                    cnext = corr;
+                }
+            }
+        }
+    }
+}
+
+struct ThHier {
+    int L, cta;             // levels; first level run by block 0 alone (L: none)
+    double omega, scale;
+    const ThLevel* lv;      // device array of L levels
+};
 
 struct ThVecs {
     double *x, *r, *rh, *p, *v, *s, *t, *ph, *sh;
 };
 
-// BiCGStab (van der Vorst), right-preconditioned by the z-column solves, for
-// A x = rhs (Tr = false) or A^T x = rhs (Tr = true), from the x in V.x
-template <bool Tr>
-__global__ void __launch_bounds__(kThThreads) k_th_bicgstab(ThK k, ThSys S, const double* rhs, const double* lc,
-                                                           const double* linv, ThVecs V, double* part,
-                                                           unsigned* bar, ThStatus* st, int maxiter, double rtol) {
+// BiCGStab (van der Vorst), right-preconditioned by one V-cycle, for
+// A x = rhs (Tr = false) or A^T x = rhs (Tr = true), from the x in V.x.
+// CH / CHP: layers per load chunk of the smoothing sweeps; CH = 1 is built
+// for two blocks an SM (128 registers), CH = 2 for one (no spills at 252).
+template <bool Tr, int CH, int CHP>
+__global__ void __launch_bounds__(kThThreads, CH == 1 ? 2 : 1) k_th_bicgstab(ThK k, ThHier H, const double* rhs, ThVecs V,
+                                                           double* part, unsigned* bar, ThStatus* st, int maxiter,
+                                                           double rtol) {
     __shared__ double sm[96];
-    const int G = gridDim.x;
+    const int G = gridDim.x, Nz = k.Nz;
     const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x, nth = (long long)G * blockDim.x;
-    const long long L = (long long)k.Nx * k.Ny;
     unsigned target = 0;
     double* pA = part;             // [G][2]
     double* pB = part + 2 * G;     // [G][2]
     double* pC = part + 4 * G;     // [G][2]
+    const ThLevel& F0 = H.lv[0];
     auto sync = [&]() -> bool {
         target += G;
         return grid_barrier(bar, target, &st->err);
     };
     auto cells = [&](auto&& fn) {
         for (long long q = tid; q < k.n; q += nth) {
-            const int kk = (int)(q / L);
-            const long long rem = q - kk * L;
+            const int kk = (int)(q / k.ncol);
+            const long long rem = q - kk * k.ncol;
             fn(q, (int)(rem % k.Nx), (int)(rem / k.Nx), kk);
         }
     };
-    // column solve: out = M^-1 (in_k), in_k computed by inf(q) along the column
-    auto column_solve = [&](long long col, auto&& inf, double* out) {
-        double yprev = 0.0;
-        for (int kk = 0; kk < k.Nz; ++kk) {
-            const long long q = kk * L + col;
-            const double in = inf(q);
-            const double y = (in - (kk > 0 ? th_sub<Tr>(S, q, L) * yprev : 0.0)) * linv[q];
-            out[q] = y;
-            yprev = y;
+    // The V-cycle after the level-0 pre-smoothing (F0.x = omega Mz^-1 b0):
+    // out0 = M^-1 b0.  Ends with a grid barrier.
+    auto vcycle = [&](const double* b0, double* out0) -> bool {
+        const int L = H.L;
+        int l = 0;
+        for (; l + 1 < L && l + 1 < H.cta; ++l) {
+            const ThLevel &F = H.lv[l], &C = H.lv[l + 1];
+            th_restrict<Tr>(F, C, Nz, l == 0 ? b0 : F.b, F.x, C.b, tid, nth);
+            if (!sync()) return false;
+            const double* cb = C.b;
+            th_presmooth<Tr, CH>(C, Nz, [&](long long q) { return cb[q]; }, nullptr, C.x, l + 2 == L ? 1.0 : H.omega,
+                             tid, nth);
+            if (!sync()) return false;
         }
-        double xnext = 0.0;
-        for (int kk = k.Nz - 1; kk >= 0; --kk) {
-            const long long q = kk * L + col;
-            const double xv = out[q] - (kk < k.Nz - 1 ? lc[q] * xnext : 0.0);
-            out[q] = xv;
-            xnext = xv;
+        if (l + 1 < L) {
+            // levels l+1 .. L-1 are small: restrict to l+1 grid-wide, then block 0
+            th_restrict<Tr>(H.lv[l], H.lv[l + 1], Nz, l == 0 ? b0 : H.lv[l].b, H.lv[l].x, H.lv[l + 1].b, tid, nth);
+            if (!sync()) return false;
+            if (blockIdx.x == 0) {
+                const long long bt = threadIdx.x, bn = blockDim.x;
+                for (int m = l + 1;; ++m) {
+                    const ThLevel& C = H.lv[m];
+                    const double* cb = C.b;
+                    th_presmooth<Tr, CH>(C, Nz, [&](long long q) { return cb[q]; }, nullptr, C.x,
+                                     m + 1 == L ? 1.0 : H.omega, bt, bn);
+                    __syncthreads();
+                    if (m + 1 == L) break;
+                    th_restrict<Tr>(C, H.lv[m + 1], Nz, C.b, C.x, H.lv[m + 1].b, bt, bn);
+                    __syncthreads();
+                }
+                for (int m = L - 2; m >= l + 1; --m) {
+                    const ThLevel &F = H.lv[m], &C = H.lv[m + 1];
+                    th_postsmooth<Tr, CHP>(F, C, Nz, F.b, F.x, m + 2 == L ? C.x : C.y, H.scale, H.omega, F.y, bt, bn);
+                    __syncthreads();
+                }
+            }
+            if (!sync()) return false;
+        } else {
+            l = L - 2;   // every level grid-wide: the ascent starts above the bottom
         }
+        for (int m = l; m >= 0; --m) {
+            const ThLevel &F = H.lv[m], &C = H.lv[m + 1];
+            th_postsmooth<Tr, CHP>(F, C, Nz, m == 0 ? b0 : F.b, F.x, m + 2 == L ? C.x : C.y, H.scale, H.omega,
+                              m == 0 ? out0 : F.y, tid, nth);
+            if (!sync()) return false;
+        }
+        return true;
     };
     // ---- r = rhs - op x, rh = r, p = v = 0; ||rhs||^2, ||r||^2
     {
         double acc[2] = {0.0, 0.0};
         cells([&](long long q, int i, int j, int kk) {
-            const double r = rhs[q] - th_ax<Tr>(k, S, V.x, q, i, j, kk);
+            const double r = rhs[q] - th_ax<Tr>(F0, Nz, V.x, q, i, j, kk);
             V.r[q] = r;
             V.rh[q] = r;
             V.p[q] = 0.0;
@@ -325,19 +585,16 @@ __global__ void __launch_bounds__(kThThreads) k_th_bicgstab(ThK k, ThSys S, cons
     for (; it < maxiter && !conv; ++it) {
         if (rho1 == 0.0) break;
         const double beta = (rho1 / rho) * (alpha / omega);
-        // ---- p = r + beta (p - omega v); ph = M^-1 p
-        for (long long col = tid; col < k.ncol; col += nth)
-            column_solve(col, [&](long long q) {
-                const double pv = V.r[q] + beta * (V.p[q] - omega * V.v[q]);
-                V.p[q] = pv;
-                return pv;
-            }, V.ph);
+        // ---- p = r + beta (p - omega v), fused with the level-0 pre-smoothing; ph = M^-1 p
+        th_presmooth<Tr, CH>(F0, Nz, [&](long long q) { return V.r[q] + beta * (V.p[q] - omega * V.v[q]); }, V.p,
+                         F0.x, H.omega, tid, nth);
         if (!sync()) return;
+        if (!vcycle(V.p, V.ph)) return;
         // ---- v = op ph; (rh, v)
         {
             double acc[2] = {0.0, 0.0};
             cells([&](long long q, int i, int j, int kk) {
-                const double vv = th_ax<Tr>(k, S, V.ph, q, i, j, kk);
+                const double vv = th_ax<Tr>(F0, Nz, V.ph, q, i, j, kk);
                 V.v[q] = vv;
                 acc[0] += V.rh[q] * vv;
             });
@@ -349,19 +606,16 @@ __global__ void __launch_bounds__(kThThreads) k_th_bicgstab(ThK k, ThSys S, cons
         sum_partials<2>(pA, G, 2, rv, sm);
         if (rv[0] == 0.0) break;
         alpha = rho1 / rv[0];
-        // ---- s = r - alpha v; sh = M^-1 s
-        for (long long col = tid; col < k.ncol; col += nth)
-            column_solve(col, [&](long long q) {
-                const double sv = V.r[q] - alpha * V.v[q];
-                V.s[q] = sv;
-                return sv;
-            }, V.sh);
+        // ---- s = r - alpha v, fused with the level-0 pre-smoothing; sh = M^-1 s
+        th_presmooth<Tr, CH>(F0, Nz, [&](long long q) { return V.r[q] - alpha * V.v[q]; }, V.s, F0.x, H.omega, tid,
+                         nth);
         if (!sync()) return;
+        if (!vcycle(V.s, V.sh)) return;
         // ---- t = op sh; (t, s), (t, t)
         {
             double acc[2] = {0.0, 0.0};
             cells([&](long long q, int i, int j, int kk) {
-                const double tv = th_ax<Tr>(k, S, V.sh, q, i, j, kk);
+                const double tv = th_ax<Tr>(F0, Nz, V.sh, q, i, j, kk);
                 V.t[q] = tv;
                 acc[0] += tv * V.s[q];
                 acc[1] += tv * tv;
@@ -517,8 +771,12 @@ struct cp_thermal {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     double *gamma = nullptr, *u = nullptr, *v = nullptr, *q0 = nullptr;
     ThSys S{};
-    double *lc = nullptr, *linv = nullptr, *lam = nullptr, *rhs = nullptr, *grad = nullptr;
+    double *lc = nullptr, *linv = nullptr, *z0 = nullptr, *lam = nullptr, *rhs = nullptr, *grad = nullptr;
     ThVecs V{};
+    int variant = 1;                  // 0: chunks 1/1, two blocks an SM; 1: chunks 2/2, one block
+    std::vector<ThLevel> lv;          // the hierarchy (level 0: S, lc, linv, z0)
+    ThLevel* dlv = nullptr;           // its device copy
+    ThHier H{};
     double* part = nullptr;
     unsigned* bar = nullptr;
     ThStatus* st = nullptr;
@@ -534,6 +792,60 @@ cp_status th_alloc(cp_thermal* t, double** p, size_t n) {
     t->allocs.push_back(q);
     TCK(cudaMemsetAsync(q, 0, std::max<size_t>(n, 1) * sizeof(double), t->stream));
     *p = static_cast<double*>(q);
+    return CP_OK;
+}
+
+// Levels of 2 x 2 column aggregates down to a single column, all z-layers
+// kept; level 0 is the assembled system.  CP_TH_OMEGA, CP_TH_SCALE and
+// CP_TH_CTA_COLS override the smoothing weight, the coarse-correction
+// factor and the size below which block 0 runs a level alone.
+cp_status th_build_hierarchy(cp_thermal* t) {
+    const ThK& k = t->k;
+    ThLevel f0{};
+    f0.nx = k.Nx;
+    f0.ny = k.Ny;
+    f0.ncol = k.ncol;
+    f0.n = k.n;
+    f0.S = t->S;
+    f0.lc = t->lc;
+    f0.linv = t->linv;
+    f0.x = t->z0;
+    t->lv.assign(1, f0);
+    while (t->lv.back().nx > 1 || t->lv.back().ny > 1) {
+        if ((int)t->lv.size() == kThMaxLevels)
+            return tfail(CP_ERR_BAD_PARAM, "grid %d x %d needs more than %d levels", k.Nx, k.Ny, kThMaxLevels);
+        const ThLevel& F = t->lv.back();
+        ThLevel C{};
+        C.nx = (F.nx + 1) / 2;
+        C.ny = (F.ny + 1) / 2;
+        C.ncol = (long long)C.nx * C.ny;
+        C.n = C.ncol * k.Nz;
+        double** arr[] = {&C.S.aP, &C.S.aW, &C.S.aE, &C.S.aS, &C.S.aN, &C.S.aB, &C.S.aT,
+                          &C.lc,   &C.linv, &C.b,    &C.x,    &C.y};
+        for (double** q : arr) {
+            cp_status s = th_alloc(t, q, (size_t)C.n);
+            if (s != CP_OK) return s;
+        }
+        t->lv.push_back(C);
+    }
+    const int L = (int)t->lv.size();
+    long long ctaCols = kThCtaCols;
+    if (const char* e = getenv("CP_TH_CTA_COLS")) ctaCols = std::max(atoll(e), 1LL);
+    int cta = L;
+    for (int l = 1; l < L; ++l)
+        if (t->lv[l].ncol <= ctaCols) { cta = l; break; }
+    void* q = nullptr;
+    TCK(cudaMalloc(&q, sizeof(ThLevel) * L));
+    t->allocs.push_back(q);
+    t->dlv = static_cast<ThLevel*>(q);
+    TCK(cudaMemcpyAsync(t->dlv, t->lv.data(), sizeof(ThLevel) * L, cudaMemcpyHostToDevice, t->stream));
+    t->H.L = L;
+    t->H.cta = cta;
+    t->H.omega = kThOmega;
+    t->H.scale = kThScale;
+    if (const char* e = getenv("CP_TH_OMEGA")) t->H.omega = atof(e);
+    if (const char* e = getenv("CP_TH_SCALE")) t->H.scale = atof(e);
+    t->H.lv = t->dlv;
     return CP_OK;
 }
 
@@ -558,8 +870,11 @@ cp_status th_objective(cp_thermal* t, double p, double* Tb_max, double* Tb_pnorm
 template <bool Tr>
 cp_status th_krylov(cp_thermal* t, const double* rhs, const ThVecs& V, ThStatus* hs) {
     const ThK& k = t->k;
-    k_th_lu<Tr><<<t->gElem, kThThreads, 0, t->stream>>>(k, t->S, t->lc, t->linv);
-    TCK(cudaGetLastError());
+    for (const ThLevel& F : t->lv) {
+        const int g = (int)std::min<long long>(t->gElem, (F.ncol + kThThreads - 1) / kThThreads);
+        k_th_lu<Tr><<<g, kThThreads, 0, t->stream>>>(k.Nz, F);
+        TCK(cudaGetLastError());
+    }
     TCK(cudaMemsetAsync(t->bar, 0, sizeof(unsigned), t->stream));
     TCK(cudaMemsetAsync(t->st, 0, sizeof(ThStatus), t->stream));
     cudaLaunchConfig_t cfg = {};
@@ -571,8 +886,12 @@ cp_status th_krylov(cp_thermal* t, const double* rhs, const ThVecs& V, ThStatus*
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    TCK(cudaLaunchKernelEx(&cfg, k_th_bicgstab<Tr>, k, t->S, rhs, (const double*)t->lc, (const double*)t->linv, V,
-                           t->part, t->bar, t->st, t->prm.maxiter, t->prm.rtol));
+    if (t->variant == 0)
+        TCK(cudaLaunchKernelEx(&cfg, k_th_bicgstab<Tr, 1, 1>, k, t->H, rhs, V, t->part, t->bar, t->st,
+                               t->prm.maxiter, t->prm.rtol));
+    else
+        TCK(cudaLaunchKernelEx(&cfg, k_th_bicgstab<Tr, 2, 2>, k, t->H, rhs, V, t->part, t->bar, t->st,
+                               t->prm.maxiter, t->prm.rtol));
     TCK(cudaEventRecord(t->ev1, t->stream));
     TCK(cudaMemcpyAsync(hs, t->st, sizeof *hs, cudaMemcpyDeviceToHost, t->stream));
     TCK(cudaStreamSynchronize(t->stream));
@@ -659,16 +978,23 @@ cp_status cp_thermal_create(const cp_thermal_params* p, cp_thermal** out) {
         if ((s = th_alloc(t, q, nc)) != CP_OK) return bail(s);
     double** vols[] = {&t->S.aP, &t->S.aW, &t->S.aE, &t->S.aS, &t->S.aN, &t->S.aB, &t->S.aT, &t->S.b,
                        &t->lc,   &t->linv, &t->V.x,  &t->V.r,  &t->V.rh, &t->V.p,  &t->V.v,  &t->V.s,
-                       &t->V.t,  &t->V.ph, &t->V.sh, &t->lam,  &t->rhs};
+                       &t->V.t,  &t->V.ph, &t->V.sh, &t->lam,  &t->rhs, &t->z0};
     for (double** q : vols)
         if ((s = th_alloc(t, q, n)) != CP_OK) return bail(s);
     // the forward and the adjoint kernel run on the same grid: every block resident
+    if (const char* e = getenv("CP_TH_VARIANT")) t->variant = atoi(e) == 0 ? 0 : 1;
     int nb = 0, nbT = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_th_bicgstab<false>, kThThreads, 0);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nbT, k_th_bicgstab<true>, kThThreads, 0);
+    if (t->variant == 0) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_th_bicgstab<false, 1, 1>, kThThreads, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nbT, k_th_bicgstab<true, 1, 1>, kThThreads, 0);
+    } else {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_th_bicgstab<false, 2, 2>, kThThreads, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nbT, k_th_bicgstab<true, 2, 2>, kThThreads, 0);
+    }
     nb = std::min(nb, nbT);
     if (nb < 1) return bail(tfail(CP_ERR_CUDA, "the thermal solver kernel does not fit on an SM"));
     t->grid = t->numSMs * std::min(nb, 4);
+    if ((s = th_build_hierarchy(t)) != CP_OK) return bail(s);
     t->gElem = t->numSMs * 4;
     if ((s = th_alloc(t, &t->part, (size_t)6 * kMaxBlocks)) != CP_OK) return bail(s);
     void* q = nullptr;
@@ -723,6 +1049,12 @@ cp_status cp_thermal_solve(cp_thermal* t, cp_thermal_report* rep) {
     // initial guess T = T_inlet
     k_th_fill<<<t->gElem, kThThreads, 0, t->stream>>>(t->V.x, k.n, t->prm.T_inlet);
     TCK(cudaGetLastError());
+    for (size_t l = 0; l + 1 < t->lv.size(); ++l) {
+        const ThLevel& C = t->lv[l + 1];
+        const int g = (int)std::min<long long>(t->gElem, (C.n + kThThreads - 1) / kThThreads);
+        k_th_coarsen<<<g, kThThreads, 0, t->stream>>>(k.Nz, t->lv[l], C);
+        TCK(cudaGetLastError());
+    }
     ThStatus hs;
     cp_status s = th_krylov<false>(t, t->S.b, t->V, &hs);
     if (s != CP_OK) return s;
