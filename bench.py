@@ -321,10 +321,13 @@ def thermal_leg(Simple, torch, args) -> dict:
     t_a = max(r["device_ms"] for r in adj) / 1e3
     its_f = max(r["iterations"] for r in fwd)
     its_a = max(r["iterations"] for r in adj)
-    # algorithmic bytes per cell and BiCGStab iteration: 43 FP64 words (two
-    # column phases of 8 and 7 words, two operator phases of 10, the update
-    # phase of 8: every vector and coefficient once per phase that needs it)
-    bytes_iter = 43 * 8 * n
+    # algorithmic bytes per cell and BiCGStab iteration, FP64 words, every
+    # vector and coefficient once per phase that needs it: level 0 85.5 (the
+    # two vector updates fused with pre-smoothing, 8 and 7; two residual
+    # restrictions, 9.25 each; two prolongation + post-smoothing sweeps, 12
+    # each; two operator applications, 10 each; the solution update, 8) and
+    # the coarse levels 18.7 (27.25 / 4 per V-cycle, twice, times 4/3)
+    bytes_iter = 104 * 8 * n
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
