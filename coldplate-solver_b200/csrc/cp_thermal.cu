@@ -26,6 +26,7 @@
 // Layout: every array is indexed k Nx Ny + j Nx + i (i contiguous), so the
 // stencil loads of a warp are coalesced and a column thread walks k with
 // stride Nx Ny.
+#include <cuda_pipeline.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -62,7 +63,11 @@ cp_status tfail(cp_status s, const char* fmt, ...) {
     } while (0)
 
 constexpr int kThThreads = 256;
-constexpr int kThMaxNz = 64;
+constexpr int kThZ = 16;                  // most layers (a column's sweep is kept in shared memory)
+constexpr int kThMaxNz = kThZ;
+constexpr int kThStage = 6;               // layers per asynchronous staging chunk
+constexpr int kThStageArr = 5;            // arrays staged per layer at most
+constexpr size_t kThSmemBytes = (size_t)(kThZ + kThStageArr * kThStage) * kThThreads * sizeof(double);
 constexpr int kThMaxLevels = 16;          // 2 x 2 aggregation from up to 2^15 columns per side
 constexpr long long kThCtaCols = 1024;    // levels of at most this many columns: block 0 alone
 constexpr double kThOmega = 0.8;          // z-line Jacobi damping
@@ -314,61 +319,70 @@ __global__ void k_th_lu(int Nz, ThLevel F) {
     }
 }
 
-// Pre-smoothing from zero: x = omega Mz^-1 b over the columns of a level,
-// b_k given by bin(q) (so the caller can fuse the vector update that makes
-// b; with bout set, b is also stored there).  The column is walked in
-// chunks of kThChunk layers whose loads are issued together before the
-// recurrence runs over them, so a column costs a few memory latencies
-// rather than one per layer.
-template <bool Tr, int kThChunk, typename Bin>
-__device__ __forceinline__ void th_presmooth(const ThLevel& F, int Nz, Bin&& bin, double* bout, double* x,
-                                             double omega, long long t0, long long nt) {
+// Shared memory of the column sweeps (doubles): ys[kThZ][blockDim] holds a
+// column's forward sweep, st[kThStageArr][kThStage][blockDim] the staged
+// inputs of kThStage layers.  Each thread uses only its own slots, so no
+// block barrier is needed around them.
+struct ThSm {
+    double* ys;
+    double* st;
+    __device__ __forceinline__ double& y(int kk) const { return ys[kk * blockDim.x + threadIdx.x]; }
+    __device__ __forceinline__ double& s(int a, int u) const {
+        return st[(a * kThStage + u) * blockDim.x + threadIdx.x];
+    }
+};
+
+__device__ __forceinline__ void th_stage(double* dst, const double* src) { __pipeline_memcpy_async(dst, src, 8); }
+
+// Pre-smoothing from zero over the columns of a level: b = A0 + c1 A1 +
+// c2 A2 (A1, A2 optional; stored to bout when set), x = omega Mz^-1 b.  The
+// inputs of kThStage layers are copied to shared memory asynchronously, all
+// in flight together, and the Thomas recurrence runs from shared memory.
+template <bool Tr>
+__device__ __forceinline__ void th_presmooth(const ThLevel& F, int Nz, const double* A0, const double* A1, double c1,
+                                             const double* A2, double c2, double* bout, double* x, double omega,
+                                             long long t0, long long nt, const ThSm& sm) {
     const long long L = F.ncol;
     for (long long col = t0; col < F.ncol; col += nt) {
         double yprev = 0.0;
-        for (int k0 = 0; k0 < Nz; k0 += kThChunk) {
-            double bv[kThChunk], sub[kThChunk], li[kThChunk];
-#pragma unroll
-            for (int u = 0; u < kThChunk; ++u) {
+        for (int k0 = 0; k0 < Nz; k0 += kThStage) {
+            const int nu = min(kThStage, Nz - k0);
+            for (int u = 0; u < nu; ++u) {
                 const int kk = k0 + u;
-                if (kk < Nz) {
-                    const long long q = kk * L + col;
-                    bv[u] = bin(q);
-                    sub[u] = kk > 0 ? th_sub<Tr>(F.S, q, L) : 0.0;
-                    li[u] = F.linv[q];
-                }
+                const long long q = kk * L + col;
+                th_stage(&sm.s(0, u), A0 + q);
+                if (A1) th_stage(&sm.s(1, u), A1 + q);
+                if (A2) th_stage(&sm.s(2, u), A2 + q);
+                if (kk > 0) th_stage(&sm.s(3, u), Tr ? F.S.aT + (q - L) : F.S.aB + q);
+                th_stage(&sm.s(4, u), F.linv + q);
             }
-#pragma unroll
-            for (int u = 0; u < kThChunk; ++u) {
+            __pipeline_commit();
+            __pipeline_wait_prior(0);
+            for (int u = 0; u < nu; ++u) {
                 const int kk = k0 + u;
-                if (kk < Nz) {
-                    const long long q = kk * L + col;
-                    yprev = (bv[u] - sub[u] * yprev) * li[u];
-                    x[q] = yprev;
-                    if (bout) bout[q] = bv[u];
-                }
+                double b = sm.s(0, u);
+                if (A1) b += c1 * sm.s(1, u);
+                if (A2) b += c2 * sm.s(2, u);
+                if (bout) bout[kk * L + col] = b;
+                const double sub = kk > 0 ? sm.s(3, u) : 0.0;
+                yprev = (b - sub * yprev) * sm.s(4, u);
+                sm.y(kk) = yprev;
             }
         }
         double xn = 0.0;
-        for (int k0 = ((Nz - 1) / kThChunk) * kThChunk; k0 >= 0; k0 -= kThChunk) {
-            double yv[kThChunk], lcv[kThChunk];
-#pragma unroll
-            for (int u = 0; u < kThChunk; ++u) {
+        for (int k0 = ((Nz - 1) / kThStage) * kThStage; k0 >= 0; k0 -= kThStage) {
+            const int nu = min(kThStage, Nz - k0);
+            for (int u = 0; u < nu; ++u) {
                 const int kk = k0 + u;
-                if (kk < Nz) {
-                    const long long q = kk * L + col;
-                    yv[u] = x[q];
-                    lcv[u] = F.lc[q];
-                }
+                if (kk < Nz - 1) th_stage(&sm.s(0, u), F.lc + (kk * L + col));
             }
-#pragma unroll
-            for (int u = kThChunk - 1; u >= 0; --u) {
+            __pipeline_commit();
+            __pipeline_wait_prior(0);
+            for (int u = nu - 1; u >= 0; --u) {
                 const int kk = k0 + u;
-                if (kk < Nz) {
-                    const double xv = yv[u] - (kk < Nz - 1 ? lcv[u] * xn : 0.0);
-                    x[kk * L + col] = omega * xv;
-                    xn = xv;
-                }
+                const double xv = sm.y(kk) - (kk < Nz - 1 ? sm.s(0, u) * xn : 0.0);
+                x[kk * L + col] = omega * xv;
+                xn = xv;
             }
         }
     }
@@ -397,78 +411,77 @@ __device__ __forceinline__ void th_restrict(const ThLevel& F, const ThLevel& C, 
     }
 }
 
-// Prolongation and post-smoothing in one sweep over the fine columns:
-// xp = xF + scale P xC (formed on the fly, neighbours included), then
-// out = xp + omega Mz^-1 (bF - op xp); chunks of kThChunkPost layers
-// (about 16 loads a layer) as in th_presmooth
-template <bool Tr, int kThChunkPost>
-__device__ __forceinline__ void th_postsmooth(const ThLevel& F, const ThLevel& C, int Nz, const double* bF,
-                                              const double* xF, const double* xC, double scale, double omega,
-                                              double* out, long long t0, long long nt) {
+// Post-smoothing, first half (cells): out = bF - op xp with the prolonged
+// iterate xp = xF + scale P xC formed on the fly at every stencil point
+template <bool Tr>
+__device__ __forceinline__ void th_post_resid(const ThLevel& F, const ThLevel& C, int Nz, const double* bF,
+                                              const double* xF, const double* xC, double scale, double* out,
+                                              long long t0, long long nt) {
+    const long long L = F.ncol, LC = C.ncol;
+    for (long long q = t0; q < F.n; q += nt) {
+        const int kk = (int)(q / L);
+        const long long col = q - kk * L;
+        const int i = (int)(col % F.nx), j = (int)(col / F.nx);
+        const long long kc = kk * LC, cj = (long long)(j >> 1) * C.nx;
+        double ax = F.S.aP[q] * (xF[q] + scale * xC[kc + cj + (i >> 1)]);
+        if (i > 0) ax += th_cW<Tr>(F.S, q) * (xF[q - 1] + scale * xC[kc + cj + ((i - 1) >> 1)]);
+        if (i < F.nx - 1) ax += th_cE<Tr>(F.S, q) * (xF[q + 1] + scale * xC[kc + cj + ((i + 1) >> 1)]);
+        if (j > 0)
+            ax += th_cS<Tr>(F.S, q, F.nx) * (xF[q - F.nx] + scale * xC[kc + (long long)((j - 1) >> 1) * C.nx + (i >> 1)]);
+        if (j < F.ny - 1)
+            ax += th_cN<Tr>(F.S, q, F.nx) * (xF[q + F.nx] + scale * xC[kc + (long long)((j + 1) >> 1) * C.nx + (i >> 1)]);
+        if (kk > 0) ax += th_sub<Tr>(F.S, q, L) * (xF[q - L] + scale * xC[kc - LC + cj + (i >> 1)]);
+        if (kk < Nz - 1) ax += th_sup<Tr>(F.S, q, L) * (xF[q + L] + scale * xC[kc + LC + cj + (i >> 1)]);
+        out[q] = bF[q] - ax;
+    }
+}
+
+// Post-smoothing, second half (columns): out = xp + omega Mz^-1 out, in
+// place (each column reads its residual before writing the result)
+template <bool Tr>
+__device__ __forceinline__ void th_post_cols(const ThLevel& F, const ThLevel& C, int Nz, const double* xF,
+                                             const double* xC, double scale, double omega, double* out,
+                                             long long t0, long long nt, const ThSm& sm) {
     const long long L = F.ncol, LC = C.ncol;
     for (long long col = t0; col < F.ncol; col += nt) {
         const int i = (int)(col % F.nx), j = (int)(col / F.nx);
         const long long c0 = (long long)(j >> 1) * C.nx + (i >> 1);
-        const long long cw = i > 0 ? (long long)(j >> 1) * C.nx + ((i - 1) >> 1) : c0;
-        const long long ce = i < F.nx - 1 ? (long long)(j >> 1) * C.nx + ((i + 1) >> 1) : c0;
-        const long long cs = j > 0 ? (long long)((j - 1) >> 1) * C.nx + (i >> 1) : c0;
-        const long long cn = j < F.ny - 1 ? (long long)((j + 1) >> 1) * C.nx + (i >> 1) : c0;
-        double yprev = 0.0, xm = 0.0;
-        for (int k0 = 0; k0 < Nz; k0 += kThChunkPost) {
-            double xp[kThChunkPost + 1], rr[kThChunkPost], sub[kThChunkPost], li[kThChunkPost];
-#pragma unroll
-            for (int u = 0; u <= kThChunkPost; ++u) {
+        double yprev = 0.0;
+        for (int k0 = 0; k0 < Nz; k0 += kThStage) {
+            const int nu = min(kThStage, Nz - k0);
+            for (int u = 0; u < nu; ++u) {
                 const int kk = k0 + u;
-                xp[u] = kk < Nz ? xF[kk * L + col] + scale * xC[kk * LC + c0] : 0.0;
+                const long long q = kk * L + col;
+                th_stage(&sm.s(0, u), out + q);
+                if (kk > 0) th_stage(&sm.s(1, u), Tr ? F.S.aT + (q - L) : F.S.aB + q);
+                th_stage(&sm.s(2, u), F.linv + q);
             }
-#pragma unroll
-            for (int u = 0; u < kThChunkPost; ++u) {
+            __pipeline_commit();
+            __pipeline_wait_prior(0);
+            for (int u = 0; u < nu; ++u) {
                 const int kk = k0 + u;
-                if (kk < Nz) {
-                    const long long q = kk * L + col, kc = kk * LC;
-                    double ax = F.S.aP[q] * xp[u];
-                    if (i > 0) ax += th_cW<Tr>(F.S, q) * (xF[q - 1] + scale * xC[kc + cw]);
-                    if (i < F.nx - 1) ax += th_cE<Tr>(F.S, q) * (xF[q + 1] + scale * xC[kc + ce]);
-                    if (j > 0) ax += th_cS<Tr>(F.S, q, F.nx) * (xF[q - F.nx] + scale * xC[kc + cs]);
-                    if (j < F.ny - 1) ax += th_cN<Tr>(F.S, q, F.nx) * (xF[q + F.nx] + scale * xC[kc + cn]);
-                    sub[u] = kk > 0 ? th_sub<Tr>(F.S, q, L) : 0.0;
-                    if (kk < Nz - 1) ax += th_sup<Tr>(F.S, q, L) * xp[u + 1];
-                    rr[u] = bF[q] - ax;
-                    li[u] = F.linv[q];
-                }
-            }
-#pragma unroll
-            for (int u = 0; u < kThChunkPost; ++u) {
-                const int kk = k0 + u;
-                if (kk < Nz) {
-                    const double r = rr[u] - (kk > 0 ? sub[u] * xm : 0.0);
-                    xm = xp[u];
-                    yprev = (r - sub[u] * yprev) * li[u];
-                    out[kk * L + col] = yprev;
-                }
+                const double sub = kk > 0 ? sm.s(1, u) : 0.0;
+                yprev = (sm.s(0, u) - sub * yprev) * sm.s(2, u);
+                sm.y(kk) = yprev;
             }
         }
         double cnext = 0.0;
-        for (int k0 = ((Nz - 1) / kThChunkPost) * kThChunkPost; k0 >= 0; k0 -= kThChunkPost) {
-            double yv[kThChunkPost], lcv[kThChunkPost], xv[kThChunkPost];
-#pragma unroll
-            for (int u = 0; u < kThChunkPost; ++u) {
+        for (int k0 = ((Nz - 1) / kThStage) * kThStage; k0 >= 0; k0 -= kThStage) {
+            const int nu = min(kThStage, Nz - k0);
+            for (int u = 0; u < nu; ++u) {
                 const int kk = k0 + u;
-                if (kk < Nz) {
-                    const long long q = kk * L + col;
-                    yv[u] = out[q];
-                    lcv[u] = F.lc[q];
-                    xv[u] = xF[q] + scale * xC[kk * LC + c0];
-                }
+                const long long q = kk * L + col;
+                if (kk < Nz - 1) th_stage(&sm.s(0, u), F.lc + q);
+                th_stage(&sm.s(1, u), xF + q);
+                th_stage(&sm.s(2, u), xC + (kk * LC + c0));
             }
-#pragma unroll
-            for (int u = kThChunkPost - 1; u >= 0; --u) {
+            __pipeline_commit();
+            __pipeline_wait_prior(0);
+            for (int u = nu - 1; u >= 0; --u) {
                 const int kk = k0 + u;
-                if (kk < Nz) {
-                    const double corr = yv[u] - (kk < Nz - 1 ? lcv[u] * cnext : 0.0);
-                    out[kk * L + col] = xv[u] + omega * corr;
-                    cnext = corr;
-                }
+                const double corr = sm.y(kk) - (kk < Nz - 1 ? sm.s(0, u) * cnext : 0.0);
+                out[kk * L + col] = sm.s(1, u) + scale * sm.s(2, u) + omega * corr;
+                cnext = corr;
             }
         }
     }
@@ -486,13 +499,14 @@ struct ThVecs {
 
 // BiCGStab (van der Vorst), right-preconditioned by one V-cycle, for
 // A x = rhs (Tr = false) or A^T x = rhs (Tr = true), from the x in V.x.
-// CH / CHP: layers per load chunk of the smoothing sweeps; CH = 1 is built
-// for two blocks an SM (128 registers), CH = 2 for one (no spills at 252).
-template <bool Tr, int CH, int CHP>
-__global__ void __launch_bounds__(kThThreads, CH == 1 ? 2 : 1) k_th_bicgstab(ThK k, ThHier H, const double* rhs, ThVecs V,
-                                                           double* part, unsigned* bar, ThStatus* st, int maxiter,
-                                                           double rtol) {
+// Dynamic shared memory: kThSmemBytes (the column sweeps' staging).
+template <bool Tr>
+__global__ void __launch_bounds__(kThThreads, 2) k_th_bicgstab(ThK k, ThHier H, const double* rhs, ThVecs V,
+                                                              double* part, unsigned* bar, ThStatus* st, int maxiter,
+                                                              double rtol) {
     __shared__ double sm[96];
+    extern __shared__ double th_dyn[];
+    const ThSm cs{th_dyn, th_dyn + kThZ * blockDim.x};
     const int G = gridDim.x, Nz = k.Nz;
     const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x, nth = (long long)G * blockDim.x;
     unsigned target = 0;
@@ -520,9 +534,8 @@ __global__ void __launch_bounds__(kThThreads, CH == 1 ? 2 : 1) k_th_bicgstab(ThK
             const ThLevel &F = H.lv[l], &C = H.lv[l + 1];
             th_restrict<Tr>(F, C, Nz, l == 0 ? b0 : F.b, F.x, C.b, tid, nth);
             if (!sync()) return false;
-            const double* cb = C.b;
-            th_presmooth<Tr, CH>(C, Nz, [&](long long q) { return cb[q]; }, nullptr, C.x, l + 2 == L ? 1.0 : H.omega,
-                             tid, nth);
+            th_presmooth<Tr>(C, Nz, C.b, nullptr, 0.0, nullptr, 0.0, nullptr, C.x, l + 2 == L ? 1.0 : H.omega, tid,
+                             nth, cs);
             if (!sync()) return false;
         }
         if (l + 1 < L) {
@@ -533,9 +546,8 @@ __global__ void __launch_bounds__(kThThreads, CH == 1 ? 2 : 1) k_th_bicgstab(ThK
                 const long long bt = threadIdx.x, bn = blockDim.x;
                 for (int m = l + 1;; ++m) {
                     const ThLevel& C = H.lv[m];
-                    const double* cb = C.b;
-                    th_presmooth<Tr, CH>(C, Nz, [&](long long q) { return cb[q]; }, nullptr, C.x,
-                                     m + 1 == L ? 1.0 : H.omega, bt, bn);
+                    th_presmooth<Tr>(C, Nz, C.b, nullptr, 0.0, nullptr, 0.0, nullptr, C.x,
+                                     m + 1 == L ? 1.0 : H.omega, bt, bn, cs);
                     __syncthreads();
                     if (m + 1 == L) break;
                     th_restrict<Tr>(C, H.lv[m + 1], Nz, C.b, C.x, H.lv[m + 1].b, bt, bn);
@@ -543,7 +555,10 @@ __global__ void __launch_bounds__(kThThreads, CH == 1 ? 2 : 1) k_th_bicgstab(ThK
                 }
                 for (int m = L - 2; m >= l + 1; --m) {
                     const ThLevel &F = H.lv[m], &C = H.lv[m + 1];
-                    th_postsmooth<Tr, CHP>(F, C, Nz, F.b, F.x, m + 2 == L ? C.x : C.y, H.scale, H.omega, F.y, bt, bn);
+                    const double* xc = m + 2 == L ? C.x : C.y;
+                    th_post_resid<Tr>(F, C, Nz, F.b, F.x, xc, H.scale, F.y, bt, bn);
+                    __syncthreads();
+                    th_post_cols<Tr>(F, C, Nz, F.x, xc, H.scale, H.omega, F.y, bt, bn, cs);
                     __syncthreads();
                 }
             }
@@ -553,8 +568,11 @@ __global__ void __launch_bounds__(kThThreads, CH == 1 ? 2 : 1) k_th_bicgstab(ThK
         }
         for (int m = l; m >= 0; --m) {
             const ThLevel &F = H.lv[m], &C = H.lv[m + 1];
-            th_postsmooth<Tr, CHP>(F, C, Nz, m == 0 ? b0 : F.b, F.x, m + 2 == L ? C.x : C.y, H.scale, H.omega,
-                              m == 0 ? out0 : F.y, tid, nth);
+            const double* xc = m + 2 == L ? C.x : C.y;
+            double* out = m == 0 ? out0 : F.y;
+            th_post_resid<Tr>(F, C, Nz, m == 0 ? b0 : F.b, F.x, xc, H.scale, out, tid, nth);
+            if (!sync()) return false;
+            th_post_cols<Tr>(F, C, Nz, F.x, xc, H.scale, H.omega, out, tid, nth, cs);
             if (!sync()) return false;
         }
         return true;
@@ -585,9 +603,8 @@ __global__ void __launch_bounds__(kThThreads, CH == 1 ? 2 : 1) k_th_bicgstab(ThK
     for (; it < maxiter && !conv; ++it) {
         if (rho1 == 0.0) break;
         const double beta = (rho1 / rho) * (alpha / omega);
-        // ---- p = r + beta (p - omega v), fused with the level-0 pre-smoothing; ph = M^-1 p
-        th_presmooth<Tr, CH>(F0, Nz, [&](long long q) { return V.r[q] + beta * (V.p[q] - omega * V.v[q]); }, V.p,
-                         F0.x, H.omega, tid, nth);
+        // ---- p = r + beta p - beta omega v, fused with the level-0 pre-smoothing; ph = M^-1 p
+        th_presmooth<Tr>(F0, Nz, V.r, V.p, beta, V.v, -beta * omega, V.p, F0.x, H.omega, tid, nth, cs);
         if (!sync()) return;
         if (!vcycle(V.p, V.ph)) return;
         // ---- v = op ph; (rh, v)
@@ -607,8 +624,7 @@ __global__ void __launch_bounds__(kThThreads, CH == 1 ? 2 : 1) k_th_bicgstab(ThK
         if (rv[0] == 0.0) break;
         alpha = rho1 / rv[0];
         // ---- s = r - alpha v, fused with the level-0 pre-smoothing; sh = M^-1 s
-        th_presmooth<Tr, CH>(F0, Nz, [&](long long q) { return V.r[q] - alpha * V.v[q]; }, V.s, F0.x, H.omega, tid,
-                         nth);
+        th_presmooth<Tr>(F0, Nz, V.r, V.v, -alpha, nullptr, 0.0, V.s, F0.x, H.omega, tid, nth, cs);
         if (!sync()) return;
         if (!vcycle(V.s, V.sh)) return;
         // ---- t = op sh; (t, s), (t, t)
@@ -773,7 +789,6 @@ struct cp_thermal {
     ThSys S{};
     double *lc = nullptr, *linv = nullptr, *z0 = nullptr, *lam = nullptr, *rhs = nullptr, *grad = nullptr;
     ThVecs V{};
-    int variant = 0;                  // 0: chunks 1/1, two blocks an SM; 1: chunks 2/2, one block
     std::vector<ThLevel> lv;          // the hierarchy (level 0: S, lc, linv, z0)
     ThLevel* dlv = nullptr;           // its device copy
     ThHier H{};
@@ -886,12 +901,9 @@ cp_status th_krylov(cp_thermal* t, const double* rhs, const ThVecs& V, ThStatus*
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    if (t->variant == 0)
-        TCK(cudaLaunchKernelEx(&cfg, k_th_bicgstab<Tr, 1, 1>, k, t->H, rhs, V, t->part, t->bar, t->st,
-                               t->prm.maxiter, t->prm.rtol));
-    else
-        TCK(cudaLaunchKernelEx(&cfg, k_th_bicgstab<Tr, 2, 2>, k, t->H, rhs, V, t->part, t->bar, t->st,
-                               t->prm.maxiter, t->prm.rtol));
+    cfg.dynamicSmemBytes = kThSmemBytes;
+    TCK(cudaLaunchKernelEx(&cfg, k_th_bicgstab<Tr>, k, t->H, rhs, V, t->part, t->bar, t->st, t->prm.maxiter,
+                           t->prm.rtol));
     TCK(cudaEventRecord(t->ev1, t->stream));
     TCK(cudaMemcpyAsync(hs, t->st, sizeof *hs, cudaMemcpyDeviceToHost, t->stream));
     TCK(cudaStreamSynchronize(t->stream));
@@ -982,16 +994,14 @@ cp_status cp_thermal_create(const cp_thermal_params* p, cp_thermal** out) {
     for (double** q : vols)
         if ((s = th_alloc(t, q, n)) != CP_OK) return bail(s);
     // the forward and the adjoint kernel run on the same grid: every block resident
-    // two blocks an SM measured faster (2.4 vs 3.8 ms an iteration at 1024 x 512 x 12)
-    if (const char* e = getenv("CP_TH_VARIANT")) t->variant = atoi(e) == 0 ? 0 : 1;
     int nb = 0, nbT = 0;
-    if (t->variant == 0) {
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_th_bicgstab<false, 1, 1>, kThThreads, 0);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nbT, k_th_bicgstab<true, 1, 1>, kThThreads, 0);
-    } else {
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_th_bicgstab<false, 2, 2>, kThThreads, 0);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nbT, k_th_bicgstab<true, 2, 2>, kThThreads, 0);
-    }
+    if (cudaFuncSetAttribute(k_th_bicgstab<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kThSmemBytes) !=
+            cudaSuccess ||
+        cudaFuncSetAttribute(k_th_bicgstab<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kThSmemBytes) !=
+            cudaSuccess)
+        return bail(tfail(CP_ERR_CUDA, "the thermal solver kernel's shared memory (%zu bytes)", kThSmemBytes));
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_th_bicgstab<false>, kThThreads, kThSmemBytes);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nbT, k_th_bicgstab<true>, kThThreads, kThSmemBytes);
     nb = std::min(nb, nbT);
     if (nb < 1) return bail(tfail(CP_ERR_CUDA, "the thermal solver kernel does not fit on an SM"));
     t->grid = t->numSMs * std::min(nb, 4);

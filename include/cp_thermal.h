@@ -4,7 +4,8 @@
  * cp_status (include/cp_simple.h); cp_last_error_string() explains it.
  *
  * Grid: Nx x Ny cells in the plane (the CFD's cropped thermal domain) and
- * Nz = nz_solid + nz_fluid layers (k = 0 the bottom of the base plate);
+ * Nz = nz_solid + nz_fluid layers (k = 0 the bottom of the base plate,
+ * Nz <= 16; the reference's default is 9);
  * temperatures are indexed k * Nx * Ny + j * Nx + i as in the reference. */
 #ifndef CP_THERMAL_H
 #define CP_THERMAL_H
