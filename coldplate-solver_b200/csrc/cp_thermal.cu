@@ -69,7 +69,7 @@ constexpr int kThStage = 6;               // layers per asynchronous staging chu
 constexpr int kThStageArr = 5;            // arrays staged per layer at most
 constexpr size_t kThSmemBytes = (size_t)(kThZ + kThStageArr * kThStage) * kThThreads * sizeof(double);
 constexpr int kThMaxLevels = 16;          // 2 x 2 aggregation from up to 2^15 columns per side
-constexpr long long kThCtaCols = 1024;    // levels of at most this many columns: block 0 alone
+constexpr long long kThCtaCols = 64;      // levels of at most this many columns: block 0 alone
 constexpr double kThOmega = 0.8;          // z-line Jacobi damping
 constexpr double kThScale = 1.4;          // coarse-correction factor (1.2-1.4 within 10 % at 1024 x 512)
 
@@ -237,20 +237,24 @@ struct ThLevel {
 // west, east, south, north, lower and upper neighbour.  Row q of A^T holds
 // column q of A: its west entry is the east coefficient of the west cell.
 template <bool Tr>
-__device__ __forceinline__ double th_cW(const ThSys& S, long long q) { return Tr ? S.aE[q - 1] : S.aW[q]; }
+__device__ __forceinline__ double th_cW(const ThSys& S, long long q) { return __ldg(Tr ? S.aE + (q - 1) : S.aW + q); }
 template <bool Tr>
-__device__ __forceinline__ double th_cE(const ThSys& S, long long q) { return Tr ? S.aW[q + 1] : S.aE[q]; }
+__device__ __forceinline__ double th_cE(const ThSys& S, long long q) { return __ldg(Tr ? S.aW + (q + 1) : S.aE + q); }
 template <bool Tr>
-__device__ __forceinline__ double th_cS(const ThSys& S, long long q, int nx) { return Tr ? S.aN[q - nx] : S.aS[q]; }
+__device__ __forceinline__ double th_cS(const ThSys& S, long long q, int nx) {
+    return __ldg(Tr ? S.aN + (q - nx) : S.aS + q);
+}
 template <bool Tr>
-__device__ __forceinline__ double th_cN(const ThSys& S, long long q, int nx) { return Tr ? S.aS[q + nx] : S.aN[q]; }
+__device__ __forceinline__ double th_cN(const ThSys& S, long long q, int nx) {
+    return __ldg(Tr ? S.aS + (q + nx) : S.aN + q);
+}
 template <bool Tr>
 __device__ __forceinline__ double th_sub(const ThSys& S, long long q, long long L) {
-    return Tr ? S.aT[q - L] : S.aB[q];
+    return __ldg(Tr ? S.aT + (q - L) : S.aB + q);
 }
 template <bool Tr>
 __device__ __forceinline__ double th_sup(const ThSys& S, long long q, long long L) {
-    return Tr ? S.aB[q + L] : S.aT[q];
+    return __ldg(Tr ? S.aB + (q + L) : S.aT + q);
 }
 
 // (op x)_q on a level, op = A or A^T
@@ -258,7 +262,7 @@ template <bool Tr>
 __device__ __forceinline__ double th_ax(const ThLevel& F, int Nz, const double* x, long long q, int i, int j,
                                         int kk) {
     const long long L = F.ncol;
-    double s = F.S.aP[q] * x[q];
+    double s = __ldg(F.S.aP + q) * x[q];
     if (i > 0) s += th_cW<Tr>(F.S, q) * x[q - 1];
     if (i < F.nx - 1) s += th_cE<Tr>(F.S, q) * x[q + 1];
     if (j > 0) s += th_cS<Tr>(F.S, q, F.nx) * x[q - F.nx];
@@ -388,52 +392,65 @@ __device__ __forceinline__ void th_presmooth(const ThLevel& F, int Nz, const dou
     }
 }
 
-// Residual restriction: bC = sum over the 2 x 2 aggregate of (bF - op xF)
+// Residual restriction: bC = sum over the 2 x 2 aggregate of (bF - op xF).
+// The four fine residuals are independent, so their loads are in flight
+// together; index math in 32 bits (levels hold fewer than 2^31 cells).
 template <bool Tr>
 __device__ __forceinline__ void th_restrict(const ThLevel& F, const ThLevel& C, int Nz, const double* bF,
                                             const double* xF, double* bC, long long t0, long long nt) {
-    for (long long qc = t0; qc < C.n; qc += nt) {
-        const int kk = (int)(qc / C.ncol);
-        const long long rem = qc - kk * C.ncol;
-        const int I = (int)(rem % C.nx), J = (int)(rem / C.nx);
-        double s = 0.0;
-        for (int dj = 0; dj < 2; ++dj) {
-            const int j = 2 * J + dj;
-            if (j >= F.ny) break;
-            for (int di = 0; di < 2; ++di) {
-                const int i = 2 * I + di;
-                if (i >= F.nx) break;
-                const long long q = kk * F.ncol + (long long)j * F.nx + i;
-                s += bF[q] - th_ax<Tr>(F, Nz, xF, q, i, j, kk);
-            }
+    const unsigned LC = (unsigned)C.ncol, cnx = (unsigned)C.nx, LF = (unsigned)F.ncol;
+    for (unsigned qc = (unsigned)t0; qc < (unsigned)C.n; qc += (unsigned)nt) {
+        const unsigned kk = qc / LC, rem = qc - kk * LC, J = rem / cnx, I = rem - J * cnx;
+        // fine cells past an odd edge are clamped onto the edge and masked,
+        // so no branch separates the four stencils
+        double r[4];
+#pragma unroll
+        for (int d = 0; d < 4; ++d) {
+            const int i0 = 2 * (int)I + (d & 1), j0 = 2 * (int)J + (d >> 1);
+            const int i = min(i0, F.nx - 1), j = min(j0, F.ny - 1);
+            const long long q = (long long)kk * LF + (long long)j * F.nx + i;
+            const double v = bF[q] - th_ax<Tr>(F, Nz, xF, q, i, j, (int)kk);
+            r[d] = (i0 == i && j0 == j) ? v : 0.0;
         }
-        bC[qc] = s;
+        bC[qc] = ((r[0] + r[1]) + r[2]) + r[3];
     }
 }
 
 // Post-smoothing, first half (cells): out = bF - op xp with the prolonged
-// iterate xp = xF + scale P xC formed on the fly at every stencil point
+// iterate xp = xF + scale P xC formed on the fly at every stencil point.
+// Two cells a thread per step (their loads in flight together), 32-bit
+// index math.
+template <bool Tr>
+__device__ __forceinline__ double th_post_res1(const ThLevel& F, const ThLevel& C, int Nz, const double* bF,
+                                               const double* xF, const double* xC, double scale, unsigned q) {
+    const unsigned L = (unsigned)F.ncol, LC = (unsigned)C.ncol, nx = (unsigned)F.nx, cnx = (unsigned)C.nx;
+    const unsigned kk = q / L, col = q - kk * L, ju = col / nx, iu = col - ju * nx;
+    const int i = (int)iu, j = (int)ju;
+    const unsigned kc = kk * LC, cj = (ju >> 1) * cnx;
+    double ax = __ldg(F.S.aP + q) * (xF[q] + scale * xC[kc + cj + (iu >> 1)]);
+    if (i > 0) ax += th_cW<Tr>(F.S, q) * (xF[q - 1] + scale * xC[kc + cj + ((iu - 1) >> 1)]);
+    if (i < F.nx - 1) ax += th_cE<Tr>(F.S, q) * (xF[q + 1] + scale * xC[kc + cj + ((iu + 1) >> 1)]);
+    if (j > 0) ax += th_cS<Tr>(F.S, q, F.nx) * (xF[q - nx] + scale * xC[kc + ((ju - 1) >> 1) * cnx + (iu >> 1)]);
+    if (j < F.ny - 1)
+        ax += th_cN<Tr>(F.S, q, F.nx) * (xF[q + nx] + scale * xC[kc + ((ju + 1) >> 1) * cnx + (iu >> 1)]);
+    if (kk > 0) ax += th_sub<Tr>(F.S, q, L) * (xF[q - L] + scale * xC[kc - LC + cj + (iu >> 1)]);
+    if ((int)kk < Nz - 1) ax += th_sup<Tr>(F.S, q, L) * (xF[q + L] + scale * xC[kc + LC + cj + (iu >> 1)]);
+    return bF[q] - ax;
+}
+
 template <bool Tr>
 __device__ __forceinline__ void th_post_resid(const ThLevel& F, const ThLevel& C, int Nz, const double* bF,
                                               const double* xF, const double* xC, double scale, double* out,
                                               long long t0, long long nt) {
-    const long long L = F.ncol, LC = C.ncol;
-    for (long long q = t0; q < F.n; q += nt) {
-        const int kk = (int)(q / L);
-        const long long col = q - kk * L;
-        const int i = (int)(col % F.nx), j = (int)(col / F.nx);
-        const long long kc = kk * LC, cj = (long long)(j >> 1) * C.nx;
-        double ax = F.S.aP[q] * (xF[q] + scale * xC[kc + cj + (i >> 1)]);
-        if (i > 0) ax += th_cW<Tr>(F.S, q) * (xF[q - 1] + scale * xC[kc + cj + ((i - 1) >> 1)]);
-        if (i < F.nx - 1) ax += th_cE<Tr>(F.S, q) * (xF[q + 1] + scale * xC[kc + cj + ((i + 1) >> 1)]);
-        if (j > 0)
-            ax += th_cS<Tr>(F.S, q, F.nx) * (xF[q - F.nx] + scale * xC[kc + (long long)((j - 1) >> 1) * C.nx + (i >> 1)]);
-        if (j < F.ny - 1)
-            ax += th_cN<Tr>(F.S, q, F.nx) * (xF[q + F.nx] + scale * xC[kc + (long long)((j + 1) >> 1) * C.nx + (i >> 1)]);
-        if (kk > 0) ax += th_sub<Tr>(F.S, q, L) * (xF[q - L] + scale * xC[kc - LC + cj + (i >> 1)]);
-        if (kk < Nz - 1) ax += th_sup<Tr>(F.S, q, L) * (xF[q + L] + scale * xC[kc + LC + cj + (i >> 1)]);
-        out[q] = bF[q] - ax;
+    const unsigned n = (unsigned)F.n, st = (unsigned)nt;
+    unsigned q = (unsigned)t0;
+    for (; q + st < n; q += 2 * st) {
+        const double r0 = th_post_res1<Tr>(F, C, Nz, bF, xF, xC, scale, q);
+        const double r1 = th_post_res1<Tr>(F, C, Nz, bF, xF, xC, scale, q + st);
+        out[q] = r0;
+        out[q + st] = r1;
     }
+    if (q < n) out[q] = th_post_res1<Tr>(F, C, Nz, bF, xF, xC, scale, q);
 }
 
 // Post-smoothing, second half (columns): out = xp + omega Mz^-1 out, in
@@ -491,6 +508,15 @@ struct ThHier {
     int L, cta;             // levels; first level run by block 0 alone (L: none)
     double omega, scale;
     const ThLevel* lv;      // device array of L levels
+    unsigned long long* prof;  // per-phase nanoseconds (CP_TH_PROFILE), or null
+};
+
+// phase slots of the profile: the BiCGStab phases, then 16 slots per
+// V-cycle phase kind indexed by level
+enum ThProfSlot {
+    TH_P_INIT = 0, TH_P_PRE_P = 1, TH_P_MATVEC_V = 2, TH_P_PRE_S = 3, TH_P_MATVEC_T = 4, TH_P_UPDATE = 5,
+    TH_P_BLOCK0 = 6, TH_P_RESTRICT = 16, TH_P_PRESMOOTH = 32, TH_P_POSTRES = 48, TH_P_POSTCOL = 64,
+    TH_P_COUNT = 80
 };
 
 struct ThVecs {
@@ -514,9 +540,18 @@ __global__ void __launch_bounds__(kThThreads, 2) k_th_bicgstab(ThK k, ThHier H, 
     double* pB = part + 2 * G;     // [G][2]
     double* pC = part + 4 * G;     // [G][2]
     const ThLevel& F0 = H.lv[0];
-    auto sync = [&]() -> bool {
+    unsigned long long tprev = (H.prof && blockIdx.x == 0 && threadIdx.x == 0) ? globaltimer_ns() : 0ull;
+    // grid barrier; with the profile on, block 0 books the time since the
+    // previous barrier to the phase slot
+    auto sync = [&](int slot) -> bool {
         target += G;
-        return grid_barrier(bar, target, &st->err);
+        const bool ok = grid_barrier(bar, target, &st->err);
+        if (H.prof && blockIdx.x == 0 && threadIdx.x == 0) {
+            const unsigned long long t = globaltimer_ns();
+            H.prof[slot] += t - tprev;
+            tprev = t;
+        }
+        return ok;
     };
     auto cells = [&](auto&& fn) {
         for (long long q = tid; q < k.n; q += nth) {
@@ -524,6 +559,24 @@ __global__ void __launch_bounds__(kThThreads, 2) k_th_bicgstab(ThK k, ThHier H, 
             const long long rem = q - kk * k.ncol;
             fn(q, (int)(rem % k.Nx), (int)(rem / k.Nx), kk);
         }
+    };
+    // Two cells a thread per step: compute(q, i, j, kk) only loads and
+    // computes (its loads for both cells in flight together), commit(q, v)
+    // stores and accumulates; 32-bit index math.
+    auto cells2 = [&](auto&& compute, auto&& commit) {
+        const unsigned n = (unsigned)k.n, L = (unsigned)k.ncol, nx = (unsigned)k.Nx, stp = (unsigned)nth;
+        auto at = [&](unsigned q) {
+            const unsigned kk = q / L, rem = q - kk * L, j = rem / nx;
+            return compute((long long)q, (int)(rem - j * nx), (int)j, (int)kk);
+        };
+        unsigned q = (unsigned)tid;
+        for (; q + stp < n; q += 2 * stp) {
+            const auto a = at(q);
+            const auto b = at(q + stp);
+            commit((long long)q, a);
+            commit((long long)(q + stp), b);
+        }
+        if (q < n) commit((long long)q, at(q));
     };
     // The V-cycle after the level-0 pre-smoothing (F0.x = omega Mz^-1 b0):
     // out0 = M^-1 b0.  Ends with a grid barrier.
@@ -533,15 +586,15 @@ __global__ void __launch_bounds__(kThThreads, 2) k_th_bicgstab(ThK k, ThHier H, 
         for (; l + 1 < L && l + 1 < H.cta; ++l) {
             const ThLevel &F = H.lv[l], &C = H.lv[l + 1];
             th_restrict<Tr>(F, C, Nz, l == 0 ? b0 : F.b, F.x, C.b, tid, nth);
-            if (!sync()) return false;
+            if (!sync(TH_P_RESTRICT + l)) return false;
             th_presmooth<Tr>(C, Nz, C.b, nullptr, 0.0, nullptr, 0.0, nullptr, C.x, l + 2 == L ? 1.0 : H.omega, tid,
                              nth, cs);
-            if (!sync()) return false;
+            if (!sync(TH_P_PRESMOOTH + l + 1)) return false;
         }
         if (l + 1 < L) {
             // levels l+1 .. L-1 are small: restrict to l+1 grid-wide, then block 0
             th_restrict<Tr>(H.lv[l], H.lv[l + 1], Nz, l == 0 ? b0 : H.lv[l].b, H.lv[l].x, H.lv[l + 1].b, tid, nth);
-            if (!sync()) return false;
+            if (!sync(TH_P_RESTRICT + l)) return false;
             if (blockIdx.x == 0) {
                 const long long bt = threadIdx.x, bn = blockDim.x;
                 for (int m = l + 1;; ++m) {
@@ -562,7 +615,7 @@ __global__ void __launch_bounds__(kThThreads, 2) k_th_bicgstab(ThK k, ThHier H, 
                     __syncthreads();
                 }
             }
-            if (!sync()) return false;
+            if (!sync(TH_P_BLOCK0)) return false;
         } else {
             l = L - 2;   // every level grid-wide: the ascent starts above the bottom
         }
@@ -571,9 +624,9 @@ __global__ void __launch_bounds__(kThThreads, 2) k_th_bicgstab(ThK k, ThHier H, 
             const double* xc = m + 2 == L ? C.x : C.y;
             double* out = m == 0 ? out0 : F.y;
             th_post_resid<Tr>(F, C, Nz, m == 0 ? b0 : F.b, F.x, xc, H.scale, out, tid, nth);
-            if (!sync()) return false;
+            if (!sync(TH_P_POSTRES + m)) return false;
             th_post_cols<Tr>(F, C, Nz, F.x, xc, H.scale, H.omega, out, tid, nth, cs);
-            if (!sync()) return false;
+            if (!sync(TH_P_POSTCOL + m)) return false;
         }
         return true;
     };
@@ -592,7 +645,7 @@ __global__ void __launch_bounds__(kThThreads, 2) k_th_bicgstab(ThK k, ThHier H, 
         block_sum<2>(acc, sm);
         if (threadIdx.x == 0) { pC[2 * blockIdx.x] = acc[0]; pC[2 * blockIdx.x + 1] = acc[1]; }
     }
-    if (!sync()) return;
+    if (!sync(TH_P_INIT)) return;
     double tot[2];
     sum_partials<2>(pC, G, 2, tot, sm);
     const double bnorm = sqrt(tot[0]) > 0.0 ? sqrt(tot[0]) : 1.0;
@@ -605,58 +658,61 @@ __global__ void __launch_bounds__(kThThreads, 2) k_th_bicgstab(ThK k, ThHier H, 
         const double beta = (rho1 / rho) * (alpha / omega);
         // ---- p = r + beta p - beta omega v, fused with the level-0 pre-smoothing; ph = M^-1 p
         th_presmooth<Tr>(F0, Nz, V.r, V.p, beta, V.v, -beta * omega, V.p, F0.x, H.omega, tid, nth, cs);
-        if (!sync()) return;
+        if (!sync(TH_P_PRE_P)) return;
         if (!vcycle(V.p, V.ph)) return;
         // ---- v = op ph; (rh, v)
         {
             double acc[2] = {0.0, 0.0};
-            cells([&](long long q, int i, int j, int kk) {
-                const double vv = th_ax<Tr>(F0, Nz, V.ph, q, i, j, kk);
-                V.v[q] = vv;
-                acc[0] += V.rh[q] * vv;
+            cells2([&](long long q, int i, int j, int kk) {
+                return make_double2(th_ax<Tr>(F0, Nz, V.ph, q, i, j, kk), V.rh[q]);
+            }, [&](long long q, double2 a) {
+                V.v[q] = a.x;
+                acc[0] += a.y * a.x;
             });
             block_sum<2>(acc, sm);
             if (threadIdx.x == 0) pA[2 * blockIdx.x] = acc[0];
         }
-        if (!sync()) return;
+        if (!sync(TH_P_MATVEC_V)) return;
         double rv[2];
         sum_partials<2>(pA, G, 2, rv, sm);
         if (rv[0] == 0.0) break;
         alpha = rho1 / rv[0];
         // ---- s = r - alpha v, fused with the level-0 pre-smoothing; sh = M^-1 s
         th_presmooth<Tr>(F0, Nz, V.r, V.v, -alpha, nullptr, 0.0, V.s, F0.x, H.omega, tid, nth, cs);
-        if (!sync()) return;
+        if (!sync(TH_P_PRE_S)) return;
         if (!vcycle(V.s, V.sh)) return;
         // ---- t = op sh; (t, s), (t, t)
         {
             double acc[2] = {0.0, 0.0};
-            cells([&](long long q, int i, int j, int kk) {
-                const double tv = th_ax<Tr>(F0, Nz, V.sh, q, i, j, kk);
-                V.t[q] = tv;
-                acc[0] += tv * V.s[q];
-                acc[1] += tv * tv;
+            cells2([&](long long q, int i, int j, int kk) {
+                return make_double2(th_ax<Tr>(F0, Nz, V.sh, q, i, j, kk), V.s[q]);
+            }, [&](long long q, double2 a) {
+                V.t[q] = a.x;
+                acc[0] += a.x * a.y;
+                acc[1] += a.x * a.x;
             });
             block_sum<2>(acc, sm);
             if (threadIdx.x == 0) { pB[2 * blockIdx.x] = acc[0]; pB[2 * blockIdx.x + 1] = acc[1]; }
         }
-        if (!sync()) return;
+        if (!sync(TH_P_MATVEC_T)) return;
         double ts[2];
         sum_partials<2>(pB, G, 2, ts, sm);
         omega = ts[1] > 0.0 ? ts[0] / ts[1] : 0.0;
         // ---- x += alpha ph + omega sh; r = s - omega t; (r, r), (rh, r)
         {
             double acc[2] = {0.0, 0.0};
-            cells([&](long long q, int, int, int) {
-                V.x[q] += alpha * V.ph[q] + omega * V.sh[q];
-                const double r = V.s[q] - omega * V.t[q];
-                V.r[q] = r;
-                acc[0] += r * r;
-                acc[1] += V.rh[q] * r;
+            cells2([&](long long q, int, int, int) {
+                return make_double3(V.x[q] + alpha * V.ph[q] + omega * V.sh[q], V.s[q] - omega * V.t[q], V.rh[q]);
+            }, [&](long long q, double3 a) {
+                V.x[q] = a.x;
+                V.r[q] = a.y;
+                acc[0] += a.y * a.y;
+                acc[1] += a.z * a.y;
             });
             block_sum<2>(acc, sm);
             if (threadIdx.x == 0) { pC[2 * blockIdx.x] = acc[0]; pC[2 * blockIdx.x + 1] = acc[1]; }
         }
-        if (!sync()) return;
+        if (!sync(TH_P_UPDATE)) return;
         sum_partials<2>(pC, G, 2, tot, sm);
         res = sqrt(tot[0]) / bnorm;
         rho = rho1;
@@ -861,7 +917,31 @@ cp_status th_build_hierarchy(cp_thermal* t) {
     if (const char* e = getenv("CP_TH_OMEGA")) t->H.omega = atof(e);
     if (const char* e = getenv("CP_TH_SCALE")) t->H.scale = atof(e);
     t->H.lv = t->dlv;
+    t->H.prof = nullptr;
+    if (getenv("CP_TH_PROFILE")) {
+        TCK(cudaMalloc(&q, sizeof(unsigned long long) * TH_P_COUNT));
+        t->allocs.push_back(q);
+        t->H.prof = static_cast<unsigned long long*>(q);
+    }
     return CP_OK;
+}
+
+// CP_TH_PROFILE: the phase times of the last solve, to stderr
+void th_print_profile(cp_thermal* t, bool Tr, int iters) {
+    unsigned long long h[TH_P_COUNT];
+    if (cudaMemcpy(h, t->H.prof, sizeof h, cudaMemcpyDeviceToHost) != cudaSuccess) return;
+    const double it = iters > 0 ? iters : 1;
+    fprintf(stderr, "thermal %s profile, us per iteration (%d iterations):\n", Tr ? "adjoint" : "forward", iters);
+    const char* top[] = {"init(total)", "update p + presmooth 0", "matvec v", "update s + presmooth 0", "matvec t",
+                         "update x, r", "block-0 levels"};
+    for (int i = 0; i <= TH_P_BLOCK0; ++i)
+        if (h[i]) fprintf(stderr, "  %-26s %9.1f\n", top[i], h[i] * 1e-3 / (i == TH_P_INIT ? 1.0 : it));
+    const char* kind[] = {"restrict from", "presmooth", "post residual", "post columns"};
+    for (int kd = 0; kd < 4; ++kd)
+        for (int l = 0; l < 16; ++l) {
+            const unsigned long long v = h[TH_P_RESTRICT + 16 * kd + l];
+            if (v) fprintf(stderr, "  %-16s level %2d %9.1f\n", kind[kd], l, v * 1e-3 / it);
+        }
 }
 
 cp_status th_objective(cp_thermal* t, double p, double* Tb_max, double* Tb_pnorm) {
@@ -902,6 +982,7 @@ cp_status th_krylov(cp_thermal* t, const double* rhs, const ThVecs& V, ThStatus*
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     cfg.dynamicSmemBytes = kThSmemBytes;
+    if (t->H.prof) TCK(cudaMemsetAsync(t->H.prof, 0, sizeof(unsigned long long) * TH_P_COUNT, t->stream));
     TCK(cudaLaunchKernelEx(&cfg, k_th_bicgstab<Tr>, k, t->H, rhs, V, t->part, t->bar, t->st, t->prm.maxiter,
                            t->prm.rtol));
     TCK(cudaEventRecord(t->ev1, t->stream));
@@ -910,6 +991,7 @@ cp_status th_krylov(cp_thermal* t, const double* rhs, const ThVecs& V, ThStatus*
     if (hs->err)
         return tfail((cp_status)hs->err, "device reported %s in the thermal %s solve",
                      cp_status_string((cp_status)hs->err), Tr ? "adjoint" : "forward");
+    if (t->H.prof) th_print_profile(t, Tr, hs->iterations);
     return CP_OK;
 }
 
@@ -983,6 +1065,8 @@ cp_status cp_thermal_create(const cp_thermal_params* p, cp_thermal** out) {
     k.dzS = p->H_b / p->nz_solid;
     k.dzF = p->H_t / p->nz_fluid;
     k.Ht = p->H_t; k.kS = p->k_s; k.kF = p->k_f; k.rhoCp = p->rho * p->Cp; k.Tin = p->T_inlet; k.qk = p->qk;
+    if (k.n >= (1LL << 31))
+        return bail(tfail(CP_ERR_BAD_PARAM, "%lld cells: the solver indexes fewer than 2^31", k.n));
     const size_t n = (size_t)k.n, nc = (size_t)k.ncol;
     cp_status s;
     double** planes[] = {&t->gamma, &t->u, &t->v, &t->q0, &t->grad};
