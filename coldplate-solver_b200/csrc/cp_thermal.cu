@@ -401,16 +401,15 @@ __device__ __forceinline__ void th_restrict(const ThLevel& F, const ThLevel& C, 
     const unsigned LC = (unsigned)C.ncol, cnx = (unsigned)C.nx, LF = (unsigned)F.ncol;
     for (unsigned qc = (unsigned)t0; qc < (unsigned)C.n; qc += (unsigned)nt) {
         const unsigned kk = qc / LC, rem = qc - kk * LC, J = rem / cnx, I = rem - J * cnx;
-        // fine cells past an odd edge are clamped onto the edge and masked,
-        // so no branch separates the four stencils
         double r[4];
 #pragma unroll
         for (int d = 0; d < 4; ++d) {
-            const int i0 = 2 * (int)I + (d & 1), j0 = 2 * (int)J + (d >> 1);
-            const int i = min(i0, F.nx - 1), j = min(j0, F.ny - 1);
-            const long long q = (long long)kk * LF + (long long)j * F.nx + i;
-            const double v = bF[q] - th_ax<Tr>(F, Nz, xF, q, i, j, (int)kk);
-            r[d] = (i0 == i && j0 == j) ? v : 0.0;
+            const int i = 2 * (int)I + (d & 1), j = 2 * (int)J + (d >> 1);
+            r[d] = 0.0;
+            if (i < F.nx && j < F.ny) {
+                const long long q = (long long)kk * LF + (long long)j * F.nx + i;
+                r[d] = bF[q] - th_ax<Tr>(F, Nz, xF, q, i, j, (int)kk);
+            }
         }
         bC[qc] = ((r[0] + r[1]) + r[2]) + r[3];
     }
