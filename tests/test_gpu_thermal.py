@@ -197,3 +197,22 @@ def test_case_directory_and_flow_inputs(tmp_path):
         T = th.T
     To = solve(oracle_params(**prm), inp["gamma"], inp["u_xy"], inp["v_xy"], inp["q0"])
     assert np.linalg.norm(T - To) <= 1e-9 * np.linalg.norm(To)
+
+
+def test_autograd_function_matches_the_adjoint_call():
+    import torch
+
+    from coldplate_b200 import Thermal, cases
+    from coldplate_b200.autograd import ThermalPNorm
+    Ny, Nx = 16, 32
+    gam, u, v, q0 = inputs(Ny, Nx, 6)
+    prm = dict(Nx=Nx, Ny=Ny, dx=1e-5, dy=1e-5, rtol=1e-12, maxiter=5000, **cases.THERMAL_3D)
+    g = torch.tensor(gam, dtype=torch.float64, requires_grad=True)
+    J = ThermalPNorm.apply(g, u, v, q0, prm, 8.0)
+    (2.0 * J).backward()
+    with Thermal(**prm) as th:
+        th.set_inputs(gam, u, v, q0)
+        th.solve()
+        Jr, gr, _ = th.pnorm_gradient(8)
+    assert float(J) == Jr
+    assert np.array_equal(g.grad.numpy(), 2.0 * gr)

@@ -15,7 +15,8 @@ def test_defaults_are_the_reference_defaults(built_lib):
         assert getattr(p, k) == pytest.approx(v), k
 
 
-@pytest.mark.parametrize("over", [dict(Nx=1), dict(Ny=0), dict(nz_solid=0), dict(nz_fluid=70), dict(dx=0.0),
+@pytest.mark.parametrize("over", [dict(Nx=1), dict(Ny=0), dict(nz_solid=0), dict(nz_fluid=70),
+                                  dict(nz_solid=8, nz_fluid=9), dict(dx=0.0),
                                   dict(k_f=-1.0), dict(k_interp_mode=3), dict(maxiter=-1),
                                   dict(rtol=float("nan")), dict(T_inlet=float("inf"))])
 def test_bad_parameters_are_rejected_before_any_device_work(built_lib, over):
