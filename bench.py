@@ -48,6 +48,10 @@ BENCH_KNOBS = dict(pressureSolverType=4, maxPressureIter=30, pTol=1e-6)
 # whose gradient is above 1% of the largest
 ADJ_TOL = 1e-6
 ADJ_MAX_ITER = 2000
+# ncu captures of the dominant kernels (profiles/): DRAM bytes read + written
+PCG_MG_CAPTURE_BYTES = (850.3 + 1406.4) * 1e6     # k_pcg_mg<float>, one launch
+PCG_MG_CAPTURE_ITERS = 30
+THERMAL_CAPTURE_BYTES_PER_CELL_ITER = 704.0        # k_th_bicgstab, 512 x 256 x 12 capture
 
 
 def parse():
@@ -344,6 +348,10 @@ def thermal_leg(Simple, torch, args) -> dict:
             "residual_forward": max(r["residual"] for r in fwd),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "kernel": "k_th_bicgstab<false> (assembly and factorisation inside the time)",
+                         "traffic": THERMAL_CAPTURE_BYTES_PER_CELL_ITER * n * its_f,
+                         "algorithmic_bytes": bytes_iter * its_f,
+                         "traffic_source": "ncu capture at 512x256x12 (10 iterations), scaled by cells x iterations; "
+                                           "L2 holds more of the smaller case, so this is a lower bound",
                          "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"},
             "e2e": {"value": float(np.mean(e2e)), "unit": "s", "h2d_bytes_per_step": int(4 * 8 * Nx * Ny),
                     "d2h_bytes_per_step": int(T.nbytes + 16)},
@@ -437,8 +445,13 @@ def main():
         pass
     peak = float(peaks.get("hbm_gbs", 6650.0))
     achieved = pcg_bytes / (pcg_ms * 1e-3) / 1e9
+    # DRAM traffic of one launch from the ncu capture of this kernel on this
+    # workload (profiles/k_pcg_mg_float_density_2048x1024.md: 850.3 + 1406.4 MB
+    # for a launch of 30 CG iterations), scaled to this line's CG iterations
+    traffic = PCG_MG_CAPTURE_BYTES * pcg_iters / PCG_MG_CAPTURE_ITERS
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": None, "kernel": "k_pcg_mg<float>",
+                "traffic": traffic, "algorithmic_bytes": pcg_bytes, "kernel": "k_pcg_mg<float>",
+                "traffic_source": "ncu capture (2048x1024, 30 CG iterations) scaled by CG iterations",
                 "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"}
 
     # ---- batched solves: 64 density fields of random size in one persistent kernel
