@@ -214,5 +214,5 @@ def test_autograd_function_matches_the_adjoint_call():
         th.set_inputs(gam, u, v, q0)
         th.solve()
         Jr, gr, _ = th.pnorm_gradient(8)
-    assert float(J) == Jr
+    assert float(J.detach()) == Jr
     assert np.array_equal(g.grad.numpy(), 2.0 * gr)
