@@ -113,6 +113,19 @@ class Thermal:
                                               ctypes.byref(r)))
         return J.value, g, _report(r)
 
+    def save_outputs(self, export_dir: str, gamma, pnorm_exp: float | None = None) -> list[str]:
+        """The reference's thermal result files from the current solution
+        (coldplate_b200.output.save_thermal_outputs): thermal_metrics.txt,
+        k_thermal.txt, T_bottom.txt, and with pnorm_exp given also
+        dJ_dgamma.txt from the adjoint, in the format the optimiser reads.
+        gamma is the field passed to set_inputs."""
+        from . import output
+        p = self.params
+        dz = [p.H_b / p.nz_solid] * p.nz_solid + [p.H_t / p.nz_fluid] * p.nz_fluid
+        g = self.pnorm_gradient(pnorm_exp)[1] if pnorm_exp is not None else None
+        return output.save_thermal_outputs(export_dir, self.T, gamma, p.dx, p.dy, dz, p.nz_solid, p.k_s, p.k_f,
+                                           p.qk, dJ_dgamma=g)
+
     def compute_optimization_results(self, pnorm_exp: float = 10) -> dict:
         """Tb_max, Tb_pnorm and dJ_dgamma (Ny x Nx) of the current solution."""
         mx, _ = self.objective(pnorm_exp)

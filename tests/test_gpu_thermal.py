@@ -216,3 +216,34 @@ def test_autograd_function_matches_the_adjoint_call():
         Jr, gr, _ = th.pnorm_gradient(8)
     assert float(J.detach()) == Jr
     assert np.array_equal(g.grad.numpy(), 2.0 * gr)
+
+
+def test_result_files_from_a_gpu_solve(tmp_path):
+    """The reference's thermal files written from a GPU solve agree with the
+    same files written from the oracle's temperature field (the solves
+    differ at their tolerance only), and dJ_dgamma.txt holds the gradient."""
+    from thermal_oracle import solve
+
+    from coldplate_b200 import Thermal, cases, output
+    Ny, Nx = 20, 40
+    gam, u, v, q0 = inputs(Ny, Nx, 7)
+    prm = dict(Nx=Nx, Ny=Ny, dx=1e-5, dy=1e-5, rtol=1e-12, maxiter=5000, **cases.THERMAL_3D)
+    with Thermal(**prm) as th:
+        th.set_inputs(gam, u, v, q0)
+        th.solve()
+        files = th.save_outputs(str(tmp_path / "gpu"), gam, pnorm_exp=8)
+        _, g, _ = th.pnorm_gradient(8)
+    assert files == ["thermal_metrics.txt", "k_thermal.txt", "T_bottom.txt", "dJ_dgamma.txt"]
+    To = solve(oracle_params(**prm), gam, u, v, q0)
+    p = oracle_params(**prm)
+    dz = [p.H_b / p.nz_solid] * p.nz_solid + [p.H_t / p.nz_fluid] * p.nz_fluid
+    output.save_thermal_outputs(str(tmp_path / "ora"), To, gam, 1e-5, 1e-5, dz, p.nz_solid, p.k_s, p.k_f, p.qk)
+    for name in ("k_thermal.txt", "T_bottom.txt"):
+        a = np.loadtxt(tmp_path / "gpu" / name)
+        b = np.loadtxt(tmp_path / "ora" / name)
+        assert np.allclose(a, b, rtol=0, atol=2e-4), name
+    assert np.allclose(np.loadtxt(tmp_path / "gpu" / "dJ_dgamma.txt"), g, rtol=1e-9, atol=0)
+    mg = {l.split()[0]: l.split()[1:] for l in open(tmp_path / "gpu" / "thermal_metrics.txt") if not l.startswith("#")}
+    mo = {l.split()[0]: l.split()[1:] for l in open(tmp_path / "ora" / "thermal_metrics.txt") if not l.startswith("#")}
+    assert mg.keys() == mo.keys()
+    assert abs(float(mg["T_avg_base"][0]) - float(mo["T_avg_base"][0])) <= 2e-4

@@ -95,3 +95,56 @@ def test_adjoint_gradient_matches_central_differences(kind, mode):
         gm[j, i] -= h
         fd = (Jof(gp) - Jof(gm)) / (2 * h)
         assert abs(fd - g[j, i]) <= 1e-5 * scale + 1e-4 * abs(fd), (j, i, fd, g[j, i])
+
+
+@pytest.mark.skipif(not os.path.exists(REF), reason="reference build (oracle/_ref) not present")
+@pytest.mark.parametrize("seed", [3, 8])
+def test_thermal_result_files_match_the_reference_byte_for_byte(tmp_path, seed):
+    """thermal_metrics.txt, k_thermal.txt and T_bottom.txt written by
+    coldplate_b200.output from the reference's own temperature field equal
+    the files the reference's main() wrote (thermal_output.cpp)."""
+    from thermal_oracle import read_dump, write_case
+
+    from coldplate_b200 import output
+    Ny, Nx, dx, dy, qf, Ht = 20, 44, 2e-5, 2e-5, 5.0e5, 2e-4
+    gam, u, v, pm = thermal_inputs(Ny, Nx, seed)
+    case = str(tmp_path / "case")
+    write_case(case, 1.0 - gam, u, v, dx, dy, qf, Ht, pm)
+    gam = 1.0 - (1.0 - gam)
+    dump = str(tmp_path / "dump.bin")
+    subprocess.run([REF, case], check=True, capture_output=True, text=True, timeout=600,
+                   env=dict(os.environ, CP_AMGCL_SHIM_DUMP=dump, OMP_NUM_THREADS="1"))
+    _, _, x_ref = read_dump(dump)
+    nzs, nzf, Hb = 2, 7, 5e-4
+    T = x_ref.reshape(nzs + nzf, Ny, Nx)
+    dz = [Hb / nzs] * nzs + [Ht / nzf] * nzf
+    mine = str(tmp_path / "mine")
+    files = output.save_thermal_outputs(mine, T, gam, dx, dy, dz, nzs, 400.0, 0.6, 1.0)
+    assert files == ["thermal_metrics.txt", "k_thermal.txt", "T_bottom.txt"]
+    for name in files:
+        a = open(os.path.join(mine, name), "rb").read()
+        b = open(os.path.join(case, name), "rb").read()
+        assert a == b, name
+
+
+def test_thermal_metrics_against_a_direct_restatement():
+    """The vectorised metrics against plain loops in the reference's order."""
+    from coldplate_b200 import output
+    rng = np.random.default_rng(2)
+    Nz, Ny, Nx, nzs = 5, 4, 6, 2
+    T = 30 + 10 * rng.random((Nz, Ny, Nx))
+    gam = (rng.random((Ny, Nx)) > 0.4).astype(float)
+    dz = [1e-4, 1e-4, 5e-5, 5e-5, 5e-5]
+    dx = dy = 1e-5
+    m = output.thermal_metrics(T, gam, dx, dy, dz, nzs)
+    s = sv = 0.0
+    for k in range(Nz):
+        for j in range(Ny):
+            for i in range(Nx):
+                if k >= nzs and gam[j, i] > 0.01:
+                    V = dx * dy * dz[k]
+                    s += T[k, j, i] * V
+                    sv += V
+    assert m["T_avg_fluid"] == s / sv
+    ext = [output.thermal_metrics(T, gam, dx, dy, dz, nzs)["grad_max_i"]]
+    assert 0 <= ext[0] < Nx
