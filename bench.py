@@ -296,6 +296,9 @@ def thermal_leg(Simple, torch, args) -> dict:
     q0 = cases.power_map(Ny, Nx, args.seed) * 1e4
     prm = dict(Nx=Nx, Ny=Ny, dx=c.hx, dy=c.hy, rtol=1e-6, maxiter=5000, **cases.THERMAL_3D)
     n = Nx * Ny * (prm["nz_solid"] + prm["nz_fluid"])
+    levels, a, b = 1, Nx, Ny              # 2 x 2 column aggregates down to one column
+    while a > 1 or b > 1:
+        a, b, levels = (a + 1) // 2, (b + 1) // 2, levels + 1
     fwd, adj = [], []
     with Thermal(**prm) as th:
         th.set_inputs(q0=q0, **fl)
@@ -355,7 +358,12 @@ def thermal_leg(Simple, torch, args) -> dict:
                          "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"},
             "e2e": {"value": float(np.mean(e2e)), "unit": "s", "h2d_bytes_per_step": int(4 * 8 * Nx * Ny),
                     "d2h_bytes_per_step": int(T.nbytes + 16)},
-            "gpu_launches_per_forward": 4, "gpu_launches_per_adjoint": 5}
+            # launches: assembly, fill, a Galerkin coarsening per coarse level, a
+            # z-factorisation per level, the persistent solver; the adjoint adds
+            # the p-norm, its right-hand side and the sensitivity
+            "multigrid_levels": levels,
+            "gpu_launches_per_forward": 2 + (levels - 1) + levels + 1,
+            "gpu_launches_per_adjoint": 2 + levels + 1 + 1}
 
 
 # ------------------------------------------------------------------ our arm
