@@ -71,7 +71,8 @@ constexpr size_t kThSmemBytes = (size_t)(kThZ + kThStageArr * kThStage) * kThThr
 constexpr int kThMaxLevels = 16;          // 2 x 2 aggregation from up to 2^15 columns per side
 constexpr long long kThCtaCols = 64;      // levels of at most this many columns: block 0 alone
 constexpr double kThOmega = 0.8;          // z-line Jacobi damping
-constexpr double kThScale = 1.4;          // coarse-correction factor (1.2-1.4 within 10 % at 1024 x 512)
+constexpr double kThScale0 = 1.4;         // coarse-correction factor into level 0
+constexpr double kThScale = 1.2;          // ... into the deeper levels
 
 }  // namespace
 
@@ -505,7 +506,7 @@ __device__ __forceinline__ void th_post_cols(const ThLevel& F, const ThLevel& C,
 
 struct ThHier {
     int L, cta;             // levels; first level run by block 0 alone (L: none)
-    double omega, scale;
+    double omega, scale0, scale;   // coarse-correction factor into level 0, into the deeper levels
     const ThLevel* lv;      // device array of L levels
     unsigned long long* prof;  // per-phase nanoseconds (CP_TH_PROFILE), or null
 };
@@ -610,7 +611,7 @@ __global__ void __launch_bounds__(kThThreads, 2) k_th_bicgstab(ThK k, ThHier H, 
                     const double* xc = m + 2 == L ? C.x : C.y;
                     th_post_resid<Tr>(F, C, Nz, F.b, F.x, xc, H.scale, F.y, bt, bn);
                     __syncthreads();
-                    th_post_cols<Tr>(F, C, Nz, F.x, xc, H.scale, H.omega, F.y, bt, bn, cs);
+                    th_post_cols<Tr>(F, C, Nz, F.x, xc, H.scale, H.omega, F.y, bt, bn, cs);   // m >= 1
                     __syncthreads();
                 }
             }
@@ -622,9 +623,10 @@ __global__ void __launch_bounds__(kThThreads, 2) k_th_bicgstab(ThK k, ThHier H, 
             const ThLevel &F = H.lv[m], &C = H.lv[m + 1];
             const double* xc = m + 2 == L ? C.x : C.y;
             double* out = m == 0 ? out0 : F.y;
-            th_post_resid<Tr>(F, C, Nz, m == 0 ? b0 : F.b, F.x, xc, H.scale, out, tid, nth);
+            const double sc = m == 0 ? H.scale0 : H.scale;
+            th_post_resid<Tr>(F, C, Nz, m == 0 ? b0 : F.b, F.x, xc, sc, out, tid, nth);
             if (!sync(TH_P_POSTRES + m)) return false;
-            th_post_cols<Tr>(F, C, Nz, F.x, xc, H.scale, H.omega, out, tid, nth, cs);
+            th_post_cols<Tr>(F, C, Nz, F.x, xc, sc, H.omega, out, tid, nth, cs);
             if (!sync(TH_P_POSTCOL + m)) return false;
         }
         return true;
@@ -866,9 +868,10 @@ cp_status th_alloc(cp_thermal* t, double** p, size_t n) {
 }
 
 // Levels of 2 x 2 column aggregates down to a single column, all z-layers
-// kept; level 0 is the assembled system.  CP_TH_OMEGA, CP_TH_SCALE and
-// CP_TH_CTA_COLS override the smoothing weight, the coarse-correction
-// factor and the size below which block 0 runs a level alone.
+// kept; level 0 is the assembled system.  CP_TH_OMEGA, CP_TH_SCALE0,
+// CP_TH_SCALE and CP_TH_CTA_COLS override the smoothing weight, the
+// coarse-correction factors into level 0 and into the deeper levels, and the
+// size below which block 0 runs a level alone.
 cp_status th_build_hierarchy(cp_thermal* t) {
     const ThK& k = t->k;
     ThLevel f0{};
@@ -912,8 +915,10 @@ cp_status th_build_hierarchy(cp_thermal* t) {
     t->H.L = L;
     t->H.cta = cta;
     t->H.omega = kThOmega;
+    t->H.scale0 = kThScale0;
     t->H.scale = kThScale;
     if (const char* e = getenv("CP_TH_OMEGA")) t->H.omega = atof(e);
+    if (const char* e = getenv("CP_TH_SCALE0")) t->H.scale0 = atof(e);
     if (const char* e = getenv("CP_TH_SCALE")) t->H.scale = atof(e);
     t->H.lv = t->dlv;
     t->H.prof = nullptr;
