@@ -72,7 +72,8 @@ constexpr int kThMaxLevels = 16;          // 2 x 2 aggregation from up to 2^15 c
 constexpr long long kThCtaCols = 64;      // levels of at most this many columns: block 0 alone
 constexpr double kThOmega = 0.8;          // z-line Jacobi damping
 constexpr double kThScale0 = 1.4;         // coarse-correction factor into level 0
-constexpr double kThScale = 1.2;          // ... into the deeper levels
+constexpr double kThScale = 1.4;          // ... into the deeper levels (1.2 / 1.1: 95 / more iterations
+                                          // at 1024 x 512 x 12, against 84)
 
 }  // namespace
 
