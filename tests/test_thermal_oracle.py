@@ -148,3 +148,36 @@ def test_thermal_metrics_against_a_direct_restatement():
     assert m["T_avg_fluid"] == s / sv
     ext = [output.thermal_metrics(T, gam, dx, dy, dz, nzs)["grad_max_i"]]
     assert 0 <= ext[0] < Nx
+
+
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+
+@pytest.mark.parametrize("name", ["thermal_uniform", "thermal_map"])
+def test_oracle_and_writers_against_the_golden_fixtures(tmp_path, name):
+    """The committed fixtures of the reference's thermal run
+    (tests/golden/make_thermal_golden.py): the oracle's assembly equals the
+    reference's matrix and right-hand side bit for bit, its solve matches the
+    reference's tight solution, and the result-file writers reproduce the
+    reference's files byte for byte from its temperature field.  Needs no
+    reference build."""
+    from thermal_oracle import ThermalParams, assemble, solve
+
+    from coldplate_b200 import output
+    z = np.load(os.path.join(GOLDEN, name + ".npz"))
+    Ny, Nx, dx, dy, qf, Ht = z["case"]
+    Ny, Nx = int(Ny), int(Nx)
+    gam = 1.0 - z["geometry"]                       # as the reference reads it
+    q0 = z["power_map"] * 10000.0 if z["power_map"].size else np.full((Ny, Nx), qf)
+    p = ThermalParams(Nx=Nx, Ny=Ny, dx=dx, dy=dy, H_t=Ht)
+    A, b = assemble(p, gam, z["u"], z["v"], q0)
+    assert np.array_equal(A.indptr, z["indptr"]) and np.array_equal(A.indices, z["indices"])
+    assert np.array_equal(A.data, z["data"])
+    assert np.array_equal(b, z["b"])
+    T = solve(p, gam, z["u"], z["v"], q0).ravel()
+    assert np.linalg.norm(T - z["x"]) <= 1e-10 * np.linalg.norm(z["x"])
+    dz = [p.H_b / p.nz_solid] * p.nz_solid + [p.H_t / p.nz_fluid] * p.nz_fluid
+    files = output.save_thermal_outputs(str(tmp_path), z["x"].reshape(p.Nz, Ny, Nx), gam, dx, dy, dz, p.nz_solid,
+                                        p.k_s, p.k_f, p.qk)
+    for f in files:
+        assert open(tmp_path / f, "rb").read() == z[f.replace(".txt", "")].tobytes(), f
