@@ -51,7 +51,7 @@ ADJ_MAX_ITER = 2000
 # ncu captures of the dominant kernels (profiles/): DRAM bytes read + written
 PCG_MG_CAPTURE_BYTES = (850.3 + 1406.4) * 1e6     # k_pcg_mg<float>, one launch
 PCG_MG_CAPTURE_ITERS = 30
-THERMAL_CAPTURE_BYTES_PER_CELL_ITER = 704.0        # k_th_bicgstab, 512 x 256 x 12 capture
+THERMAL_CAPTURE_BYTES_PER_CELL_ITER = 702.0        # k_th_bicgstab, 512 x 256 x 12 capture
 
 
 def parse():
