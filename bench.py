@@ -224,6 +224,24 @@ def reference_arm(args, case, rank: int):
     print(json.dumps(line))
 
 
+# ------------------------------------------------------------------ ranks
+def replica_seed(seed: int, rank: int) -> int:
+    """Each rank solves its own replica of the workload (the path does not
+    shard): the density field of seed + rank."""
+    return seed + rank
+
+
+def max_over_ranks(x: float, dist, device: str) -> float:
+    """The job's time is its slowest replica's: max of x over the ranks (one
+    all-reduce, which every rank calls at the same point)."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 # ------------------------------------------------------------------ batched solves
 BATCH_SINGLE_OUTER = 20
 
@@ -373,7 +391,7 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     from coldplate_b200 import cases
-    case = cases.density_field(args.ny, args.nx, seed=args.seed + rank, **BENCH_KNOBS)
+    case = cases.density_field(args.ny, args.nx, seed=replica_seed(args.seed, rank), **BENCH_KNOBS)
     if args.impl == "reference":
         return reference_arm(args, case, rank)
 
@@ -427,10 +445,7 @@ def main():
     clocks = clk.summary()
     t_mixed = max(t_mix)
     t_adj = max(r["device_ms"] for r in adj_reps) / 1e3
-    if dist:
-        tt = torch.tensor([t_mixed], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_mixed = float(tt.item())
+    t_mixed = max_over_ranks(t_mixed, dist, "cuda")
 
     # ---- per-kernel device times and the roofline of the dominant kernel
     prm = case.params(precision="mixed", maxIterations=100000, epsilon=1e-30, historyCapacity=100000)
