@@ -16,7 +16,9 @@ import pytest
 
 from oracle import HIST_COLS, Oracle, ref_available, run_reference, write_case
 
-GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz")))
+# the flow fixtures (the thermal ones, thermal_*.npz, belong to test_thermal_oracle.py)
+GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*_f32.npz")) +
+                glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*_f64.npz")))
 FIELDS = ("u", "v", "p", "uStar", "vStar", "pStar", "dE", "dN")
 
 
