@@ -318,8 +318,9 @@ constexpr int kTmaStages = 2;
 
 template <typename TV>
 struct TileSmem {
-    static constexpr int kBox = ((kBoxR * kBoxW * (int)sizeof(TV) + 127) / 128) * 128;
-    static constexpr int kCBox = ((kCBoxR * kCBoxW * (int)sizeof(TV) + 127) / 128) * 128;
+    typedef TileGeom<TV> G;
+    static constexpr int kBox = ((G::BoxR * G::BoxW * (int)sizeof(TV) + 127) / 128) * 128;
+    static constexpr int kCBox = ((G::CBoxR * G::CBoxW * (int)sizeof(TV) + 127) / 128) * 128;
     static constexpr int kStage = 6 * kBox;   // up to five fine boxes and a coarse one per stage
     static constexpr int kBytes = kTmaStages * kStage;
 };
@@ -451,6 +452,8 @@ __global__ void __launch_bounds__(512, 1) k_pcg_mg(KParams k, Status* st, const 
     unsigned long long tp = (H.prof && blockIdx.x == 0 && threadIdx.x == 0) ? globaltimer_ns() : 0ull;
 
     // ---- level-0 tile phases (TMA staged)
+    constexpr int kTileR = TileGeom<TV>::R, kTileC = TileGeom<TV>::C, kBoxR = TileGeom<TV>::BoxR,
+                  kBoxW = TileGeom<TV>::BoxW, kCBoxR = TileGeom<TV>::CBoxR, kCBoxW = TileGeom<TV>::CBoxW;
     const int nI0 = M - 1, nJ0 = w;
     const int tilesI = (nI0 + kTileR - 1) / kTileR, tilesJ = (nJ0 + kTileC - 1) / kTileC;
     const int ntiles = tilesI * tilesJ;

@@ -365,8 +365,10 @@ constexpr int kMgThreads = 512;
 // dynamic shared memory: the dense set-up workspace and, afterwards, the two
 // TMA tile stages (sized for double; the float kernel uses less of it)
 constexpr size_t kMgDenseSmem = sizeof(double) * (size_t)(kMgDense * 2 * kMgDense + kMgDense);
-constexpr size_t kMgDynSmem = kMgDenseSmem > (size_t)TileSmem<double>::kBytes ? kMgDenseSmem
-                                                                               : (size_t)TileSmem<double>::kBytes;
+constexpr size_t kMgTileSmem = (size_t)TileSmem<double>::kBytes > (size_t)TileSmem<float>::kBytes
+                                   ? (size_t)TileSmem<double>::kBytes
+                                   : (size_t)TileSmem<float>::kBytes;
+constexpr size_t kMgDynSmem = kMgDenseSmem > kMgTileSmem ? kMgDenseSmem : kMgTileSmem;
 
 // Level sizes: halve (rounding up) until at most kMgDense unknowns; levels
 // above kMgCtaCells unknowns (and always level 0) run grid-wide.
@@ -413,6 +415,11 @@ cp_status mg_build(cp_ctx* c) {
     // prolongation (y of a grid-wide level 1, x of a CTA level)
     {
         const int R0 = c->d.M + 2, P0 = c->d.P, es = c->es;
+        // the box shapes of the kernel instance for this element size
+        const int kBoxR = es == 4 ? TileGeom<float>::BoxR : TileGeom<double>::BoxR;
+        const int kBoxW = es == 4 ? TileGeom<float>::BoxW : TileGeom<double>::BoxW;
+        const int kCBoxR = es == 4 ? TileGeom<float>::CBoxR : TileGeom<double>::CBoxR;
+        const int kCBoxW = es == 4 ? TileGeom<float>::CBoxW : TileGeom<double>::CBoxW;
         void* a0[7] = {c->mgArr[0][5], c->pcg[5], c->pcg[6], c->pcg[4], c->pcg[2], c->pcg[0], c->pcg[1]};
         CUtensorMap* m0[7] = {&c->mgMaps.z, &c->mgMaps.pa, &c->mgMaps.pb, &c->mgMaps.r, &c->mgMaps.d,
                               &c->mgMaps.fE, &c->mgMaps.fN};

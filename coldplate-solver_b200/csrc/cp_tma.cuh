@@ -82,16 +82,26 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, i
         : "memory");
 }
 
-// Tile geometry of the level-0 stencil phases: TR x TC unknowns with a
-// one-cell halo, loaded as boxes of (TR + 2) x BW elements whose origin is
-// (x = TC * tJ, y = TR * tI) in array coordinates (the unknowns start at
-// i = j = 1, so the halo column/row sits exactly on a multiple of TC / TR).
-constexpr int kTileR = 16;
-constexpr int kTileC = 64;
-constexpr int kBoxR = kTileR + 2;   // 18
-constexpr int kBoxW = kTileC + 4;   // 68: >= TC + 2 and a multiple of 16 bytes for 4- and 8-byte types
-// coarse (level-1) box of the prolongation: rows 8 tI .. 8 tI + 9, cols 32 tJ .. 32 tJ + 35
-constexpr int kCBoxR = kTileR / 2 + 2;   // 10
-constexpr int kCBoxW = kTileC / 2 + 4;   // 36
+// Tile geometry of the level-0 stencil phases: R x C unknowns with a
+// one-cell halo, loaded as boxes of (R + 2) x BoxW elements whose origin is
+// (x = C * tJ, y = R * tI) in array coordinates (the unknowns start at
+// i = j = 1, so the halo column/row sits exactly on a multiple of C / R).
+// The coarse (level-1) box of the prolongation covers rows (R / 2) tI ..
+// (R / 2) tI + R / 2 + 1 and columns (C / 2) tJ .. (C / 2) tJ + C / 2 + 3.
+// Rows by element size: 32 for float (a CTA walks half as many tiles as with
+// 16, -6 % per CG iteration at 2048 x 1024, measured), 16 for double (32
+// rows fill 217 KB of shared memory for two stages and measured slower).
+#ifndef CP_TILE_R_FLOAT
+#define CP_TILE_R_FLOAT 32
+#endif
+template <typename TV>
+struct TileGeom {
+    static constexpr int R = sizeof(TV) == 4 ? CP_TILE_R_FLOAT : 16;
+    static constexpr int C = 64;
+    static constexpr int BoxR = R + 2;
+    static constexpr int BoxW = C + 4;        // >= C + 2 and a multiple of 16 bytes for 4- and 8-byte types
+    static constexpr int CBoxR = R / 2 + 2;
+    static constexpr int CBoxW = C / 2 + 4;
+};
 
 }  // namespace cp
