@@ -470,7 +470,9 @@ def main():
     achieved = pcg_bytes / (pcg_ms * 1e-3) / 1e9
     # DRAM traffic of one launch from the ncu capture of this kernel on this
     # workload (profiles/k_pcg_mg_float_density_2048x1024.md: 850.3 + 1406.4 MB
-    # for a launch of 30 CG iterations), scaled to this line's CG iterations
+    # for a launch of 30 CG iterations, taken with 16 x 64 float tiles; the
+    # 32 x 64 tiles read the same arrays with less halo), scaled to this
+    # line's CG iterations
     traffic = PCG_MG_CAPTURE_BYTES * pcg_iters / PCG_MG_CAPTURE_ITERS
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": traffic, "algorithmic_bytes": pcg_bytes, "kernel": "k_pcg_mg<float>",
