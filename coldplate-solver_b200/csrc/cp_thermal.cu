@@ -65,7 +65,10 @@ cp_status tfail(cp_status s, const char* fmt, ...) {
 constexpr int kThThreads = 256;
 constexpr int kThZ = 16;                  // most layers (a column's sweep is kept in shared memory)
 constexpr int kThMaxNz = kThZ;
-constexpr int kThStage = 6;               // layers per asynchronous staging chunk
+#ifndef CP_TH_STAGE
+#define CP_TH_STAGE 6
+#endif
+constexpr int kThStage = CP_TH_STAGE;     // layers per asynchronous staging chunk
 constexpr int kThStageArr = 5;            // arrays staged per layer at most
 constexpr size_t kThSmemBytes = (size_t)(kThZ + kThStageArr * kThStage) * kThThreads * sizeof(double);
 constexpr int kThMaxLevels = 16;          // 2 x 2 aggregation from up to 2^15 columns per side
