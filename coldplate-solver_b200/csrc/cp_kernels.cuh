@@ -617,7 +617,7 @@ __device__ void finish_metrics(double area, double fs, double st, double dy, dou
 __device__ void sample_metric(const KParams& k, const double* u, const double* v, const double* p,
                               const double* gamma, int kind, double x, double* m, double* sm) {
     const Dims d = k.d;
-    const int M = d.M, N = d.N, MC = M - 1, NC = N - 1;
+    const int M = d.M, N = d.N, NC = N - 1;
     const double hx = k.hx, hy = k.hy, rho = k.rho;
     double acc[5] = {0, 0, 0, 0, 0};  // area, flux, static, dyn, totalWeighted
     int cl = 0, cr = 0;

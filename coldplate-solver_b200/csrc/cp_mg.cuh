@@ -454,6 +454,9 @@ __global__ void __launch_bounds__(512, 1) k_pcg_mg(KParams k, Status* st, const 
     // ---- level-0 tile phases (TMA staged)
     constexpr int kTileR = TileGeom<TV>::R, kTileC = TileGeom<TV>::C, kBoxR = TileGeom<TV>::BoxR,
                   kBoxW = TileGeom<TV>::BoxW, kCBoxR = TileGeom<TV>::CBoxR, kCBoxW = TileGeom<TV>::CBoxW;
+    // the restriction pairs lanes with a shuffle: every thread of the 512 takes the same passes
+    static_assert((kTileR * kTileC / 2) % 512 == 0, "tile pairs must fill whole passes of 512 threads");
+    static_assert(kTileR % 2 == 0 && kTileC % 16 == 0, "tile rows even, tile columns 16-byte aligned");
     const int nI0 = M - 1, nJ0 = w;
     const int tilesI = (nI0 + kTileR - 1) / kTileR, tilesJ = (nJ0 + kTileC - 1) / kTileC;
     const int ntiles = tilesI * tilesJ;

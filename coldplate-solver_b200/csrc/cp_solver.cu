@@ -369,6 +369,7 @@ constexpr size_t kMgTileSmem = (size_t)TileSmem<double>::kBytes > (size_t)TileSm
                                    ? (size_t)TileSmem<double>::kBytes
                                    : (size_t)TileSmem<float>::kBytes;
 constexpr size_t kMgDynSmem = kMgDenseSmem > kMgTileSmem ? kMgDenseSmem : kMgTileSmem;
+static_assert(kMgDynSmem + 4096 <= 227 * 1024, "k_pcg_mg's dynamic shared memory exceeds a block's limit");
 
 // Level sizes: halve (rounding up) until at most kMgDense unknowns; levels
 // above kMgCtaCells unknowns (and always level 0) run grid-wide.
