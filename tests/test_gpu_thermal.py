@@ -307,3 +307,23 @@ def test_full_size_gradient_directional_derivative():
         fd = (Jof(gam + h * d) - Jof(gam - h * d)) / (2 * h)
     ad = float(np.sum(g * d))
     assert abs(fd - ad) <= 1e-4 * abs(ad), (fd, ad)
+
+
+def test_thermal_main_writes_the_reference_files(tmp_path):
+    """python -m coldplate_b200.thermal_main <dir> [qk] [mode] --pnorm 8 on a
+    case written in the reference's files: the result files appear and
+    T_bottom.txt matches the oracle's solution at its printed precision."""
+    from thermal_oracle import solve, write_case
+
+    from coldplate_b200 import cases
+    from coldplate_b200.thermal import load_case
+    from coldplate_b200.thermal_main import main
+    Ny, Nx = 16, 36
+    gam, u, v, _ = inputs(Ny, Nx, 12)
+    write_case(str(tmp_path), 1.0 - gam, u, v, 1e-5, 1e-5, 4e5, 2e-4, cases.power_map(Ny, Nx, 12))
+    assert main([str(tmp_path), "3", "1", "--pnorm", "8", "--rtol", "1e-12"]) == 0
+    for f in ("thermal_metrics.txt", "k_thermal.txt", "T_bottom.txt", "dJ_dgamma.txt"):
+        assert (tmp_path / f).exists(), f
+    prm, inp = load_case(str(tmp_path), qk=3.0)
+    To = solve(oracle_params(**prm), inp["gamma"], inp["u_xy"], inp["v_xy"], inp["q0"])
+    assert np.allclose(np.loadtxt(tmp_path / "T_bottom.txt"), To[0], rtol=0, atol=6e-5)

@@ -79,3 +79,11 @@ def test_power_map_statistics():
     assert q.min() >= 20.0 and q.max() <= 20.0 + 12 * 300.0
     assert q.max() > 70.0
     assert np.array_equal(q, cases.power_map(512, 1024, 7))
+
+
+def test_thermal_main_reports_missing_inputs_like_the_reference(tmp_path, capsys):
+    """The command-line replacement exits 1 on a directory without
+    thermal_params.txt, before touching the GPU (thermal_solver.cpp:700-704)."""
+    from coldplate_b200.thermal_main import main
+    assert main([str(tmp_path)]) == 1
+    assert "Cannot open" in capsys.readouterr().err
