@@ -87,3 +87,40 @@ def test_thermal_main_reports_missing_inputs_like_the_reference(tmp_path, capsys
     from coldplate_b200.thermal_main import main
     assert main([str(tmp_path)]) == 1
     assert "Cannot open" in capsys.readouterr().err
+
+
+def test_inputs_from_flow_crop_matches_the_flow_writer(tmp_path):
+    """inputs_from_flow takes the same columns and the same cell-centred
+    averages as the u_thermal / v_thermal files of output.save_all (up to
+    the files' float rounding), with inlet and outlet buffers."""
+    from coldplate_b200 import output
+    from coldplate_b200.thermal import inputs_from_flow
+    rng = np.random.default_rng(3)
+    Ny, Nx, nin, nout = 6, 14, 2, 3
+    M, N = Ny + 1, Nx + 1
+    fields = {"u": rng.random((M + 1, N)), "v": rng.random((M, N + 1)), "p": rng.random((M + 1, N + 1))}
+
+    class Flow:
+        def get(self, name):
+            return fields[name]
+
+    ct = (rng.random((Ny, Nx)) > 0.5).astype(float)
+    fl = inputs_from_flow(Flow(), ct, nin, nout)
+    assert fl["gamma"].shape == (Ny, Nx - nin - nout)
+    assert np.array_equal(fl["gamma"], 1.0 - ct[:, nin:Nx - nout])
+    output.save_all(str(tmp_path), fields["u"], fields["v"], fields["p"], 1e-5, 1e-5, nin, nout)
+    # the files print six significant digits
+    assert np.allclose(np.loadtxt(tmp_path / "u_thermal.txt"), fl["u_xy"], rtol=1e-5, atol=1e-6)
+    assert np.allclose(np.loadtxt(tmp_path / "v_thermal.txt"), fl["v_xy"], rtol=1e-5, atol=1e-6)
+
+
+def test_thermal_metrics_without_fluid():
+    """No fluid cell: the fluid averages, deviation and range are zero, as
+    the reference's guards give (thermal_output.cpp:239-246)."""
+    from coldplate_b200 import output
+    T = 30.0 + np.arange(2 * 3 * 4, dtype=float).reshape(2, 3, 4)
+    m = output.thermal_metrics(T, np.zeros((3, 4)), 1e-5, 1e-5, [1e-4, 1e-4], 1)
+    assert m["T_avg_fluid"] == 0.0 and m["T_std_fluid"] == 0.0 and m["T_range_fluid"] == 0.0
+    assert m["T_avg_solid"] > 0.0 and m["T_range_global"] == T.max() - T.min()
+    assert m["grad_max"] > 0.0
+    assert 0 <= m["grad_max_k"] < 2 and 0 <= m["grad_max_j"] < 3 and 0 <= m["grad_max_i"] < 4
