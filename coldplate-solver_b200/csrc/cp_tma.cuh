@@ -89,15 +89,19 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, i
 // The coarse (level-1) box of the prolongation covers rows (R / 2) tI ..
 // (R / 2) tI + R / 2 + 1 and columns (C / 2) tJ .. (C / 2) tJ + C / 2 + 3.
 // Rows by element size: 32 for float (a CTA walks half as many tiles as with
-// 16, -6 % per CG iteration at 2048 x 1024, measured), 16 for double (32
-// rows fill 217 KB of shared memory for two stages and measured slower).
+// 16, -6 % per CG iteration at 2048 x 1024, measured; 16 x 128 timed the
+// same, 64 rows slower), 16 for double (32 rows fill 217 KB of shared memory
+// for two stages and measured slower).
 #ifndef CP_TILE_R_FLOAT
 #define CP_TILE_R_FLOAT 32
+#endif
+#ifndef CP_TILE_C_FLOAT
+#define CP_TILE_C_FLOAT 64
 #endif
 template <typename TV>
 struct TileGeom {
     static constexpr int R = sizeof(TV) == 4 ? CP_TILE_R_FLOAT : 16;
-    static constexpr int C = 64;
+    static constexpr int C = sizeof(TV) == 4 ? CP_TILE_C_FLOAT : 64;
     static constexpr int BoxR = R + 2;
     static constexpr int BoxW = C + 4;        // >= C + 2 and a multiple of 16 bytes for 4- and 8-byte types
     static constexpr int CBoxR = R / 2 + 2;
