@@ -16,8 +16,10 @@
 //   k_th_bicgstab   persistent cooperative BiCGStab right-preconditioned by
 //                   one V-cycle: damped z-line Jacobi smoothing (one sweep
 //                   down, one up; exact on the one-column level), residual
-//                   restriction fused with the 2 x 2 sums, prolongation fused
-//                   with the post-smoothing sweep; levels of at most
+//                   restriction fused with the 2 x 2 sums, the prolongation
+//                   formed on the fly in the two post-smoothing passes (the
+//                   residual over cells, then the z-solve over columns,
+//                   staged through shared memory); levels of at most
 //                   kThCtaCols columns run in block 0 alone.  Bounded grid
 //                   barriers, deterministic block sums, AMGCL's stop test
 //                   ||r|| <= rtol ||b||.  The same kernel solves A^T x = rhs
