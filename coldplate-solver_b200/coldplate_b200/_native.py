@@ -14,7 +14,7 @@ LIB_PATH = os.path.join(os.path.dirname(PKG_DIR), "libcoldplate.so")
 
 CP_OK = 0
 STATUS_NAMES = {0: "CP_OK", 1: "CP_ERR_BAD_PARAM", 2: "CP_ERR_UNSUPPORTED", 3: "CP_ERR_NONFINITE",
-                4: "CP_ERR_DIVERGED", 5: "CP_ERR_TIMEOUT", 6: "CP_ERR_CUDA", 7: "CP_ERR_STATE"}
+                5: "CP_ERR_TIMEOUT", 6: "CP_ERR_CUDA", 7: "CP_ERR_STATE"}
 PREC_FP64, PREC_MIXED = 0, 1
 STOP_NAMES = {0: "running", 1: "residual", 2: "max_iter", 3: "dp_window", 4: "error"}
 FIELDS = {"u": 0, "v": 1, "p": 2, "uStar": 3, "vStar": 4, "pStar": 5, "dE": 6, "dN": 7, "gamma": 8,
@@ -42,7 +42,7 @@ PARAM_FIELDS = [
     ("rho", _D), ("eta", _D), ("enableInletRamp", _I), ("rampSteps", _I), ("uvAlpha", _D), ("pAlpha", _D),
     ("enableResidualViscosity", _I), ("enableNormalizedResiduals", _I), ("residNormFloorVel", _D),
     ("residNormFloorMass", _D),
-    ("precision", _I), ("refineRounds", _I), ("historyCapacity", _I), ("chunk", _I),
+    ("precision", _I), ("historyCapacity", _I), ("chunk", _I),
 ]
 
 
@@ -142,6 +142,7 @@ SIGNATURES = {
     "cp_thermal_pnorm_gradient": (_I, [_vp, _D, _dp, _dp, ctypes.POINTER(CpThermalReport)]),
     "cp_history_columns": (_I, []),
     "cp_get_history": (_I, [_vp, _dp, _I, _ip]),
+    "cp_selftest_bounded_wait": (_I, [_I, _D, _ip]),
     "cp_status_string": (ctypes.c_char_p, [_I]),
     "cp_last_error_string": (ctypes.c_char_p, []),
 }

@@ -151,8 +151,10 @@ __device__ __forceinline__ unsigned long long globaltimer_ns() {
     return t;
 }
 
-// Returns false if the wait gave up or another block already failed.
-__device__ __forceinline__ bool grid_barrier(unsigned* counter, unsigned target, int* err) {
+// Returns false if the wait gave up (after limitNs of spinning) or another
+// block already failed.
+__device__ __forceinline__ bool grid_barrier(unsigned* counter, unsigned target, int* err,
+                                             unsigned long long limitNs = kBarrierNs) {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -165,7 +167,7 @@ __device__ __forceinline__ bool grid_barrier(unsigned* counter, unsigned target,
             if (((++spins) & 255u) == 0) {
                 unsigned long long t = globaltimer_ns();
                 if (t0 == 0) t0 = t;
-                else if (t - t0 > kBarrierNs || spins > (1u << 30)) {
+                else if (t - t0 > limitNs || spins > (1u << 30)) {
                     atomicCAS(err, 0, (int)CP_ERR_TIMEOUT);
                     ok = 0;
                     break;

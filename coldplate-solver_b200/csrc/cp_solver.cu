@@ -659,7 +659,6 @@ const char* cp_status_string(cp_status s) {
         case CP_ERR_BAD_PARAM: return "CP_ERR_BAD_PARAM";
         case CP_ERR_UNSUPPORTED: return "CP_ERR_UNSUPPORTED";
         case CP_ERR_NONFINITE: return "CP_ERR_NONFINITE";
-        case CP_ERR_DIVERGED: return "CP_ERR_DIVERGED";
         case CP_ERR_TIMEOUT: return "CP_ERR_TIMEOUT";
         case CP_ERR_CUDA: return "CP_ERR_CUDA";
         case CP_ERR_STATE: return "CP_ERR_STATE";
@@ -722,7 +721,6 @@ void cp_params_default(cp_params* p) {
     p->residNormFloorVel = 1e-6;
     p->residNormFloorMass = 1e-12;
     p->precision = CP_PREC_FP64;
-    p->refineRounds = 0;
     p->historyCapacity = 0;   // 0: maxIterations rows
     p->chunk = 32;
 }
@@ -1325,7 +1323,7 @@ extern "C" cp_status cp_adjoint_dp_dgamma(cp_ctx* c, double* grad, long rows, lo
 // caller provides only the inputs and the output.
 namespace {
 
-// Largest pressure grid the array serves: (Ny + 2) * pitch elements per
+// Largest pressure grid the array serves: (Ny + 3) * pitch elements per
 // working array, where pitch is the row pitch (in doubles) the caller uses.
 constexpr size_t kNoAllocCells = 131072;
 constexpr size_t kNoAllocArrays = 9;                  // fE fN d x r pa pb Ap rhs
@@ -1338,18 +1336,46 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 constexpr int kNoAllocMaxDevices = 64;
 std::mutex g_noalloc_mutex;
 unsigned char* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+void* g_noalloc_ctx[kNoAllocMaxDevices] = {};   // the context the cached address belongs to
 
-// device address of the array for the current device (looked up once per
-// device, with that device current)
+// cuCtxGetCurrent through the runtime's driver entry point (no libcuda link)
+typedef CUresult (*CtxGetCurrentFn)(CUcontext*);
+
+cp_status current_context(void** ctx) {
+    static CtxGetCurrentFn fn = nullptr;
+    if (!fn) {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !f)
+            return fail(CP_ERR_CUDA, "cuCtxGetCurrent is not available");
+        fn = reinterpret_cast<CtxGetCurrentFn>(f);
+    }
+    CUcontext c = nullptr;
+    if (fn(&c) != CUDA_SUCCESS) return fail(CP_ERR_CUDA, "cuCtxGetCurrent failed");
+    *ctx = c;
+    return CP_OK;
+}
+
+// Device address of the array for the current device.  It is looked up
+// (with that device current) on the first call and again whenever the
+// device's context has changed since, e.g. after cudaDeviceReset, which
+// unloads the module and may place the array elsewhere.
 cp_status noalloc_scratch(unsigned char** out) {
     int dev = 0;
     CK(cudaGetDevice(&dev));
     if (dev < 0 || dev >= kNoAllocMaxDevices) return fail(CP_ERR_CUDA, "device ordinal %d out of range", dev);
+    void* ctx = nullptr;
+    cp_status st = current_context(&ctx);
+    if (st != CP_OK) return st;
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (!g_noalloc_ptr[dev]) {
+    if (!ctx || !g_noalloc_ptr[dev] || g_noalloc_ctx[dev] != ctx) {
+        // the lookup also creates the device's primary context if none is current
         void* p = nullptr;
         CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+        if ((st = current_context(&ctx)) != CP_OK) return st;
         g_noalloc_ptr[dev] = static_cast<unsigned char*>(p);
+        g_noalloc_ctx[dev] = ctx;
     }
     *out = g_noalloc_ptr[dev];
     return CP_OK;
@@ -1432,6 +1458,51 @@ extern "C" cp_status cp_pressure_noalloc(const cp_params* p, const double* dE, c
     if (hs.err != 0) return fail((cp_status)hs.err, "device reported %s", cp_status_string((cp_status)hs.err));
     if (iters) *iters = hs.itersP;
     if (residMass) *residMass = hs.lastError;
+    return CP_OK;
+}
+
+// ======================================================================== bounded-wait self-test
+// The persistent kernels wait on grid barriers and the TMA pipelines on
+// mbarriers; every such wait gives up after a time limit and records
+// CP_ERR_TIMEOUT in the status word, so a wait that cannot end returns an
+// error instead of holding the GPU.  This self-test runs each kind of wait
+// on something that never happens (a second block that does not exist, an
+// mbarrier phase nobody arrives on) with a short limit, so that the give-up
+// path is exercised without any fault.
+namespace {
+
+__global__ void k_selftest_wait(int kind, unsigned long long limitNs, unsigned* counter, int* err) {
+    if (kind == 0) {
+        // one block waits for two arrivals
+        grid_barrier(counter, 2u, err, limitNs);
+    } else {
+        __shared__ __align__(8) uint64_t bar;
+        if (threadIdx.x == 0) {
+            mbar_init(&bar, 1);
+            mbar_fence_init();
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) mbar_wait(&bar, 0u, err, limitNs);   // phase 0 never completes
+        __syncthreads();
+    }
+}
+
+}  // namespace
+
+extern "C" cp_status cp_selftest_bounded_wait(int kind, double limit_seconds, int* device_status) {
+    if (kind != 0 && kind != 1) return fail(CP_ERR_BAD_PARAM, "kind must be 0 (grid barrier) or 1 (mbarrier)");
+    if (!(limit_seconds > 0.0) || limit_seconds > 10.0) return fail(CP_ERR_BAD_PARAM, "limit must be in (0, 10] s");
+    if (!device_status) return fail(CP_ERR_BAD_PARAM, "NULL argument");
+    void* buf = nullptr;
+    CK(cudaMalloc(&buf, 256));
+    struct Free { void* p; ~Free() { cudaFree(p); } } guard{buf};
+    CK(cudaMemset(buf, 0, 256));
+    unsigned* counter = static_cast<unsigned*>(buf);
+    int* err = reinterpret_cast<int*>(static_cast<char*>(buf) + 128);
+    k_selftest_wait<<<1, 32>>>(kind, (unsigned long long)(limit_seconds * 1e9), counter, err);
+    CK(cudaGetLastError());
+    CK(cudaDeviceSynchronize());
+    CK(cudaMemcpy(device_status, err, sizeof(int), cudaMemcpyDeviceToHost));
     return CP_OK;
 }
 

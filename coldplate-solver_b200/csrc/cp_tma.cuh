@@ -48,15 +48,17 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
     return ok != 0;
 }
 
-// Bounded wait for the phase with the given parity; false after ~2 s.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, int* err) {
+// Bounded wait for the phase with the given parity; false after limitNs
+// (2 s by default).
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, int* err,
+                                          unsigned long long limitNs = kBarrierNs) {
     unsigned spins = 0;
     unsigned long long t0 = 0;
     while (!mbar_try_wait(bar, parity)) {
         if (((++spins) & 1023u) == 0) {
             const unsigned long long t = globaltimer_ns();
             if (t0 == 0) t0 = t;
-            else if (t - t0 > kBarrierNs) {
+            else if (t - t0 > limitNs) {
                 atomicCAS(err, 0, (int)CP_ERR_TIMEOUT);
                 return false;
             }

@@ -28,7 +28,8 @@ typedef enum cp_status {
     CP_ERR_BAD_PARAM = 1,    /* invalid argument or parameter value          */
     CP_ERR_UNSUPPORTED = 2,  /* a reference option this build does not run  */
     CP_ERR_NONFINITE = 3,    /* NaN/Inf in inputs or produced by the solve   */
-    CP_ERR_DIVERGED = 4,     /* residual growth beyond the divergence limit  */
+    /* 4 is not used: the reference iteration has no divergence rule, and a
+     * solve that blows up stops with CP_ERR_NONFINITE */
     CP_ERR_TIMEOUT = 5,      /* a bounded device-side wait gave up           */
     CP_ERR_CUDA = 6,         /* a CUDA runtime call failed                   */
     CP_ERR_STATE = 7         /* call not valid in the context's state        */
@@ -136,8 +137,6 @@ typedef struct cp_params {
 
     /* ---- additions of this implementation ---- */
     int precision;                  /* cp_precision                           */
-    int refineRounds;               /* mixed: extra FP32 PCG correction rounds
-                                       driven by the FP64 refinement residual */
     int historyCapacity;            /* rows of per-iteration history kept     */
     int chunk;                      /* outer iterations between host polls    */
 } cp_params;
@@ -235,6 +234,9 @@ cp_status cp_pressure(cp_ctx* ctx, int* iters, double* residMass);
  * pitch 512); larger grids return CP_ERR_BAD_PARAM.  The first call on a
  * device looks up the array's device address (cudaGetSymbolAddress) with
  * that device current; make that first call before capturing any stream.
+ * The address is kept with the context it was found in and looked up again
+ * when the current context differs (after cudaDeviceReset, say), so such a
+ * later call is again a first call.
  * All calls share the array, so calls that overlap on the GPU (other streams
  * or other threads) race and must be serialised by the caller. */
 cp_status cp_pressure_noalloc(const cp_params* p, const double* dE, const double* dN, const double* uStar,
@@ -313,6 +315,17 @@ cp_status cp_batch_run(cp_batch* batch, int max_outer, cp_batch_report* rep);
 /* Times trial_outer iterations from the initial state for each candidate tile
  * shape, keeps the fastest, and resets every field (cp_reset) afterwards. */
 cp_status cp_batch_autotune(cp_batch* batch, int trial_outer, cp_batch_report* best);
+
+/* Self-test of the bounded device waits.  The persistent kernels wait on
+ * grid barriers (kind 0) and the TMA pipelines on mbarriers (kind 1); each
+ * wait gives up after a time limit and records CP_ERR_TIMEOUT instead of
+ * holding the GPU.  This call runs one wait of the given kind on an event
+ * that never comes (a second block that does not exist, an mbarrier phase
+ * nobody arrives on) with a limit of limit_seconds (at most 10), and writes
+ * the status word the kernel left into *device_status: CP_ERR_TIMEOUT when
+ * the give-up path works.  Returns CP_OK when the launch itself succeeded.
+ * No counterpart in the reference. */
+cp_status cp_selftest_bounded_wait(int kind, double limit_seconds, int* device_status);
 
 const char* cp_status_string(cp_status s);
 const char* cp_last_error_string(void);

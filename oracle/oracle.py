@@ -223,6 +223,40 @@ class Oracle:
         return it, float(r.value)
 
 
+def dp_window_stop(core_dp, rampSteps: int, window: int, percent: float) -> int | None:
+    """The pressure-drop window stop rule of SIMPLE::runIterations
+    (SIMPLE.cpp:449-491), applied to a per-iteration core total-pressure-drop
+    history: from iteration rampSteps on, the drops fill a circular buffer of
+    `window` entries; once it is full, the loop stops after the first
+    iteration whose buffer has a population standard deviation and a latest
+    deviation from the mean both below `percent` % of max(|mean|, 1).
+    Returns the number of completed iterations when the rule fires (the
+    reference's loop exits after that iteration), or None."""
+    buf = np.zeros(window)
+    idx, filled = 0, False
+    for it, d in enumerate(np.asarray(core_dp, dtype=np.float64)):
+        if it < rampSteps:
+            continue
+        buf[idx] = d
+        idx = (idx + 1) % window
+        if idx == 0:
+            filled = True
+        if filled:
+            s = 0.0
+            for q in range(window):
+                s += buf[q]
+            mean = s / window
+            var = 0.0
+            for q in range(window):
+                var += (buf[q] - mean) * (buf[q] - mean)
+            denom = max(abs(mean), 1.0)
+            std_pct = np.sqrt(var / window) / denom * 100.0
+            latest_pct = abs(buf[(idx - 1 + window) % window] - mean) / denom * 100.0
+            if std_pct < percent and latest_pct < percent:
+                return it + 1
+    return None
+
+
 # --------------------------------------------------------------------------
 # reference build (oracle/_ref)
 
@@ -249,7 +283,8 @@ _REF_KEYS = ("rho", "eta", "brinkmanKMin", "brinkmanQ", "convectionScheme", "ena
              "twoPointFiveDConvectionFactor", "twoPointFiveDSinkMultiplier", "epsilon",
              "maxIterations", "maxPressureIter", "pTol", "momentumTol", "maxMomentumIter",
              "uvAlpha", "pAlpha", "xPlaneCoreInlet", "xPlaneCoreOutlet", "enableInletRamp",
-             "rampSteps", "pressureSolverType", "momentumSolverType", "enableNormalizedResiduals")
+             "rampSteps", "pressureSolverType", "momentumSolverType", "enableNormalizedResiduals",
+             "usePressureDropConvergence", "dpConvergenceWindow", "dpConvergencePercent")
 
 
 def ref_overrides(params: dict, threads: int = 1) -> list[str]:

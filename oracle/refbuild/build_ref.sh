@@ -14,7 +14,10 @@
 # is written into the repository.
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
-REF_DIR="${REF_DIR:-/root/reference}"
+if [ -z "${REF_DIR:-}" ]; then
+    echo "build_ref.sh: set REF_DIR to the reference checkout (the directory holding SIMPLE.cpp)" >&2
+    exit 2
+fi
 OUT="${OUT:-$HERE/../_ref}"
 CXX="${CXX:-g++}"
 # the image's g++ driver does not search the system gcc directory for
