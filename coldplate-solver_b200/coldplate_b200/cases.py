@@ -17,6 +17,8 @@ Workloads
                     q = 0.1, SOU, 2.5-D;
                     fluid inlet/outlet buffers keep the boundary patches pure
                     fluid so the pressure drop is defined
+  constricted_channel  a channel narrowed to a gap that carries the flow
+                    above the reference's velocity clamp (adjoint tests)
   batch             density fields of random sizes (Nx 256-1024, Ny 128-512)
                     and inlet velocities (0.2-1.0 m/s)
   THERMAL_3D,       the 3-D conjugate-heat-transfer settings on the flow's
@@ -207,6 +209,32 @@ def density_field(Ny: int = 1024, Nx: int = 2048, seed: int = 0, U: float = 0.5,
                  epsilon=1e-7, maxIterations=100000)
     knobs.update(over)
     return Case("density_field", _f32(1.0 - gam), U, 2e-4, knobs=knobs)
+
+
+def constricted_channel(Ny: int = 32, Nx: int = 96, gap: int = 6, U: float = 0.5, **over) -> Case:
+    """A straight channel (one solid wall row top and bottom) blocked over
+    16 columns in the middle except for a gap of `gap` rows, with a row and a
+    column of gamma = 0.5 along the block's faces; the density workload's
+    physics (SOU, 2.5-D, Brinkman alpha_max 1e9, q 0.1).  The gap carries the
+    flow at more than 3 U_in, so the reference's +-3 max(U_in, 0.1) velocity
+    clamp is active at the converged state."""
+    gam = np.ones((Ny, Nx))
+    gam[:1] = 0.0
+    gam[Ny - 1:] = 0.0
+    c0, c1 = Nx // 2 - 8, Nx // 2 + 8
+    lo = (Ny - gap) // 2
+    gam[1:lo, c0:c1] = 0.0
+    gam[lo + gap:Ny - 1, c0:c1] = 0.0
+    gam[lo - 1, c0:c1] = 0.5
+    gam[lo + gap, c0:c1] = 0.5
+    gam[1:lo, c0 - 1] = 0.5
+    gam[lo + gap:Ny - 1, c0 - 1] = 0.5
+    knobs = _base_knobs(Nx)
+    knobs.update(convectionScheme=1, enableTwoPointFiveD=1, twoPointFiveDConvectionFactor=1.2,
+                 brinkmanKMin=MU / 1e9, brinkmanQ=0.1, pTol=1e-8, maxPressureIter=30,
+                 epsilon=1e-7, maxIterations=100000)
+    knobs.update(over)
+    return Case("constricted_channel", _f32(1.0 - gam), U, 2e-4, knobs=knobs)
 
 
 def batch(n: int = 64, seed: int = 0, **over) -> list[Case]:

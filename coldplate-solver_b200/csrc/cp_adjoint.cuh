@@ -2,43 +2,62 @@
 //
 // The reference has no flow adjoint (its only adjoint is the 2-D conduction
 // toy in AdjointMethod/thermal_adjoint.py); this is new.  It differentiates
-// the converged state of the SIMPLE discretisation exactly:
+// the fixed point that the reference's SIMPLE iteration actually reaches,
+// velocity clamps included.
 //
-//   R(X; gamma) = 0,   X = (u on U unknowns, v on V unknowns, p on the
-//                          pressure unknowns [1,M-1] x [1,N-2])
+// One outer iteration (iterations.cpp:82-659) assembles the momentum system
+// at the current state X = (u, v, p), runs s Jacobi sweeps from x_0 = u
+// (jacobi_solver.cpp:20-75, s set by its stop rule), clamps the result to
+// +-maxVel (momentum_solver.cpp:335-351), and corrects with p' from the mass
+// imbalance (iterations.cpp:556-597).  At a fixed point p' = 0, and with
+//   y_0 = 0,  y_{j+1} = D^-1 (r0 + N y_j)   (x_j = u + y_j; D = aP0 / uvAlpha,
+//   N the off-diagonal coefficients, r0 = b - A u = -R(X) the unrelaxed
+//   momentum residual of the flux form below)
+// the state satisfies
+//   F_u = y_s = 0                 on every U / V unknown whose sweep result
+//                                  lies inside the clamp,
+//   u = +-maxVel                  on the unknowns the scatter clamps,
+//   R_c = 0                       the mass imbalance of the pressure unknowns.
+// Where a velocity sits on the clamp the momentum residual does not vanish
+// near it, and y_s depends on the sweep count s and on uvAlpha; with s and
+// the clamped set frozen (both are locally constant in gamma) this system
+// is smooth, and its derivative is what central differences of converged
+// solves measure.  Without clamps it reduces to R = 0.
 //
-// R_u: the U-momentum balance of momentum_solver.cpp:197-314 at u* = u with
-//      the relaxation cancelled, written in flux form
+// R_u, the U-momentum balance of momentum_solver.cpp:197-314 with the
+// relaxation cancelled, in flux form:
 //        De(2uP-uE-uW) + Dn(1+hN)(uP-uN) + Dn(1+hS)(uP-uS)
 //        + Fe phi_e - Fw phi_w + Fn phi_n - Fs phi_s + (sink + alpha vol) uP
 //        - hy (pP - pE)
-//      where F are the clamped face-average mass fluxes and phi the SOU face
-//      values of convection.cpp:53-186 (FOU where the SOU stencil is missing
-//      or convectionScheme = 0); the same for R_v;
-// R_c: the mass imbalance massW - massE + massS - massN of the pressure
-//      unknowns (pressure_solver.cpp:733-742).
-// Boundary values enter through the BCs of boundaries.cpp:50-146: the
-// outlet copies u(i,N-1) = u(i,N-2) and v(i,N) = v(i,N-1) map to unknowns,
-// walls, inlet and p(:,N-1) = 0 are constants.
+// where F are the clamped face-average mass fluxes and phi the SOU face
+// values of convection.cpp:53-186 (FOU where the SOU stencil is missing or
+// convectionScheme = 0); the same for R_v.  R_c: the mass imbalance
+// massW - massE + massS - massN (pressure_solver.cpp:733-742).  Boundary
+// values enter through the BCs of boundaries.cpp:50-146: the outlet copies
+// u(i,N-1) = u(i,N-2) and v(i,N) = v(i,N-1) map to unknowns, walls, inlet and
+// p(:,N-1) = 0 are constants.
 //
 // J = full-system total-pressure drop (SIMPLE.cpp:432): inlet patch
 // mass-flux-weighted total pressure minus the outlet patch's
 // (postprocessing.cpp:245-327).
 //
-// Adjoint: J_X^T lambda = dJ/dX, solved by restarted flexible GMRES with
-// the exact transposed Jacobian product (every Newton term of the upwind
-// switches, SOU branches and face-velocity clamps) and a transposed SIMPLE
-// preconditioner P: Jacobi sweeps on the transposed Picard momentum matrix,
-// then a pressure-like correction whose operator G^T diag(aP0)^-1 D^T equals
-// the forward pressure-correction matrix, so the same (multigrid) PCG kernel
-// solves it.  The PCG runs a fixed number of iterations, which makes P
-// slightly different from one application to the next; the flexible variant
-// keeps the preconditioned directions and stays exact under that.
-// Gradient: dJ/dgamma = -lambda^T dR/dgamma, which is local: gamma enters R
-// only through alpha_face = (alpha(cL) + alpha(cR)) / 2 with
-// alpha(g) = alpha_max (1 - g) / (1 + q g + 1e-10) (SIMPLE.cpp:770);
-// thresholds on gamma (inlet, half-cell and sampling masks) are piecewise
-// constant and contribute nothing.
+// Adjoint: J_X^T lambda = dJ/dX, solved by restarted flexible GMRES.  The
+// product J_X^T lambda runs the s sweeps in reverse (stored forward
+// iterates), which gives the adjoints of r0 and of the coefficients, then
+// scatters them through the assembly: every Newton term of the upwind
+// switches, SOU branches and face-velocity clamps.  The preconditioner is a
+// transposed SIMPLE step for this system: -1 on the momentum rows (F_u is
+// already a Jacobi-preconditioned residual), then a pressure-like solve whose
+// operator is uvAlpha times the forward pressure-correction matrix with the
+// clamped faces removed (a clamped face carries a fixed flux, so it does not
+// couple the pressure on either side), solved by the forward (multigrid)
+// PCG kernel with a fixed iteration count; the flexible variant stays exact
+// under that.
+// Gradient: dJ/dgamma = -lambda^T dF/dgamma, local through
+// alpha_face = (alpha(cL) + alpha(cR)) / 2 with
+// alpha(g) = alpha_max (1 - g) / (1 + q g + 1e-10) (SIMPLE.cpp:770), which
+// enters r0 and D; thresholds on gamma (inlet, half-cell and sampling masks)
+// are piecewise constant and contribute nothing.
 #pragma once
 
 #include "cp_kernels.cuh"
@@ -282,28 +301,203 @@ __device__ double adj_row_c(const AdjCtx& a, int i, int j, double lam, AdjVecs V
     return R;
 }
 
-// y = J^T lambda (y zeroed by the caller); with resid != nullptr also the
-// residuals R(X) per row (U, V, C in the field layout).
-__global__ void k_adj_jt(AdjCtx a, AdjVecs V, double* rU, double* rV, double* rC) {
+// ---------------------------------------------------------------- frozen sweeps
+// One momentum component's Jacobi system at the converged state and the
+// adjoints its reverse sweeps accumulate.
+struct AdjSweep {
+    const double *aP, *aE, *aW, *aN, *aS;   // relaxed diagonal D, masked off-diagonals N
+    const double* clamp;                     // 1 where the scatter clamps the sweep result
+    double *r0b, *eb, *wb, *nb, *sb, *db;    // adjoints of r0, aE, aW, aN, aS and D
+};
+
+// One forward Jacobi sweep x+ = x + (b - A x) / aP of one component in the
+// reference's arithmetic (CSR order S, W, P, E, N; jacobi_solver.cpp:44-60)
+// from x = field (x == nullptr) or x; part[block] = the block's sum of r^2
+// of the pre-update residual (the stop rule's sum).
+template <bool IsU>
+__global__ void k_adj_sweep(KParams k, MomSys<double> S, const double* field, const double* x, double* xn,
+                            double* part) {
+    __shared__ double sm[32];
+    const Dims d = k.d;
+    int i1, j1;
+    mom_range<IsU>(d, i1, j1);
+    const int n = i1 * j1;
+    const double* X = x ? x : field;
+    double acc[1] = {0.0};
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        const int i = 1 + t / j1, j = 1 + t % j1;
+        const size_t c = at(d, i, j);
+        double Ax = 0.0;
+        Ax += (-S.aS[c]) * ((i > 1) ? X[c - d.P] : 0.0);
+        Ax += (-S.aW[c]) * ((j > 1) ? X[c - 1] : 0.0);
+        Ax += S.aP[c] * X[c];
+        Ax += (-S.aE[c]) * ((j < j1) ? X[c + 1] : 0.0);
+        Ax += (-S.aN[c]) * ((i < i1) ? X[c + d.P] : 0.0);
+        const double r = S.b[c] - Ax;
+        xn[c] = X[c] + r / S.aP[c];
+        acc[0] += r * r;
+    }
+    block_sum<1>(acc, sm);
+    if (threadIdx.x == 0) part[blockIdx.x] = acc[0];
+}
+
+// clamp[c] = 1 where the sweep result lies outside +-maxVel (the scatter
+// clamps it, momentum_solver.cpp:342), else 0
+template <bool IsU>
+__global__ void k_adj_clampmask(KParams k, const double* xs, double maxVel, double* clamp) {
+    const Dims d = k.d;
+    int i1, j1;
+    mom_range<IsU>(d, i1, j1);
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < i1 * j1; t += gridDim.x * blockDim.x) {
+        const size_t c = at(d, 1 + t / j1, 1 + t % j1);
+        clamp[c] = (xs[c] < -maxVel || maxVel < xs[c]) ? 1.0 : 0.0;
+    }
+}
+
+// One reverse sweep of the recurrence y_{j+1} = D^-1 (r0 + N y_j) of one
+// component (y_j = x_j - field): with w = ybar / D on the unknowns,
+// r0b += w, the coefficient adjoints eb.. += w y_j(neighbour), db -= w y_{j+1},
+// and ybar' = N^T w.  seed: ybar is the adjoint vector itself, masked to the
+// unclamped unknowns (the rows of y_s that are equations).
+template <bool IsU>
+__device__ __forceinline__ void adj_rev_comp(const Dims& d, const AdjSweep& S, const double* field,
+                                             const double* xj, const double* xj1, const double* yb, bool seed,
+                                             double* ybn, int t) {
+    int i1, j1;
+    mom_range<IsU>(d, i1, j1);
+    const int i = 1 + t / j1, j = 1 + t % j1;
+    const size_t c = at(d, i, j);
+    auto Yb = [&](size_t a) -> double { return seed ? yb[a] * (1.0 - S.clamp[a]) : yb[a]; };
+    auto W = [&](size_t a) -> double { return Yb(a) / S.aP[a]; };
+    const double wc = W(c);
+    if (wc != 0.0) {
+        S.r0b[c] += wc;
+        if (j < j1) S.eb[c] += wc * (xj[c + 1] - field[c + 1]);
+        if (j > 1) S.wb[c] += wc * (xj[c - 1] - field[c - 1]);
+        if (i < i1) S.nb[c] += wc * (xj[c + d.P] - field[c + d.P]);
+        if (i > 1) S.sb[c] += wc * (xj[c - d.P] - field[c - d.P]);
+        S.db[c] -= wc * (xj1[c] - field[c]);
+    }
+    double y = 0.0;
+    if (j < j1) y += S.aW[c + 1] * W(c + 1);
+    if (j > 1) y += S.aE[c - 1] * W(c - 1);
+    if (i < i1) y += S.aS[c + d.P] * W(c + d.P);
+    if (i > 1) y += S.aN[c - d.P] * W(c - d.P);
+    ybn[c] = y;
+}
+
+__global__ void k_adj_rev(KParams k, AdjSweep U, AdjSweep V, const double* u, const double* v, const double* xUj,
+                          const double* xUj1, const double* xVj, const double* xVj1, const double* ybU,
+                          const double* ybV, double* ybUn, double* ybVn, int doU, int doV, int seedU, int seedV) {
+    const Dims d = k.d;
+    const int M = d.M, N = d.N;
+    const int nU = doU ? (M - 1) * (N - 2) : 0, nV = doV ? (M - 2) * (N - 1) : 0;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nU + nV; t += gridDim.x * blockDim.x) {
+        if (t < nU) adj_rev_comp<true>(d, U, u, xUj, xUj1, ybU, seedU != 0, ybUn, t);
+        else adj_rev_comp<false>(d, V, v, xVj, xVj1, ybV, seedV != 0, ybVn, t - nU);
+    }
+}
+
+// Coefficient adjoints of one momentum row scattered to the face velocities
+// the coefficients depend on.  aE = De + max(0, -Fe), aW = De + max(0, Fw),
+// aN = Dn + max(0, -Fn), aS = Dn + max(0, Fs) (in-set neighbours only; the
+// half-cell doubling is constant), aP0 = sum of all four + (Fe - Fw + Fn - Fs)
+// + sink + alpha vol, D = aP0 / uvAlpha (momentum_solver.cpp:204-262).
+// F are cs rho h times the clamped face averages.
+template <bool IsU>
+__device__ void adj_coef_row(const AdjCtx& a, int i, int j, const AdjSweep& S, AdjVecs V) {
+    const KParams& k = a.k;
+    const Dims d = k.d;
+    const int M = d.M, N = d.N;
+    const size_t c = at(d, i, j);
+    const double ap0b = S.db[c] / k.uvAlpha;
+    int i1, j1;
+    mom_range<IsU>(d, i1, j1);
+    const bool eIn = j < j1, wIn = j > 1, nIn = i < i1, sIn = i > 1;
+    const double mv = a.maxVel;
+    const double cs = k.convScale, cE = cs * k.rho * k.hy, cN = cs * k.rho * k.hx;
+    const double* u = a.u;
+    const double* v = a.v;
+    auto uv = [&](int ii, int jj) -> double { return u[at(d, ii, jj)]; };
+    auto vv = [&](int ii, int jj) -> double { return v[at(d, ii, jj)]; };
+    double xe, xw, xn, xs;
+    if (IsU) {
+        xe = 0.5 * (uv(i, j) + uv(i, j + 1)); xw = 0.5 * (uv(i, j - 1) + uv(i, j));
+        xn = 0.5 * (vv(i, j) + vv(i, j + 1)); xs = 0.5 * (vv(i - 1, j) + vv(i - 1, j + 1));
+    } else {
+        xe = 0.5 * (uv(i, j) + uv(i + 1, j)); xw = 0.5 * (uv(i, j - 1) + uv(i + 1, j - 1));
+        xn = 0.5 * (vv(i, j) + vv(i + 1, j)); xs = 0.5 * (vv(i - 1, j) + vv(i, j));
+    }
+    const double Fe = cE * dclamp(xe, -mv, mv), Fw = cE * dclamp(xw, -mv, mv);
+    const double Fn = cN * dclamp(xn, -mv, mv), Fs = cN * dclamp(xs, -mv, mv);
+    const double sE = Fe < 0.0 ? 1.0 : 0.0, sW = Fw > 0.0 ? 1.0 : 0.0;
+    const double sN = Fn < 0.0 ? 1.0 : 0.0, sS = Fs > 0.0 ? 1.0 : 0.0;
+    const double Feb = (eIn ? -S.eb[c] * sE : 0.0) + ap0b * (1.0 - sE);
+    const double Fwb = (wIn ? S.wb[c] * sW : 0.0) + ap0b * (sW - 1.0);
+    const double Fnb = (nIn ? -S.nb[c] * sN : 0.0) + ap0b * (1.0 - sN);
+    const double Fsb = (sIn ? S.sb[c] * sS : 0.0) + ap0b * (sS - 1.0);
+    const double gE = 0.5 * cE * clampd(xe, mv) * Feb, gW = 0.5 * cE * clampd(xw, mv) * Fwb;
+    const double gN = 0.5 * cN * clampd(xn, mv) * Fnb, gS = 0.5 * cN * clampd(xs, mv) * Fsb;
+    auto Uk = [&](int ii, int jj, size_t& cc) -> bool {  // U unknowns; u(i,N-1) is the copy of u(i,N-2)
+        if (ii < 1 || ii > M - 1 || jj < 1) return false;
+        if (jj == N - 1) jj = N - 2;
+        if (jj > N - 2) return false;
+        cc = at(d, ii, jj);
+        return true;
+    };
+    auto Vk = [&](int ii, int jj, size_t& cc) -> bool {  // V unknowns; v(i,N) is the copy of v(i,N-1)
+        if (ii < 1 || ii > M - 2 || jj < 1) return false;
+        if (jj == N) jj = N - 1;
+        if (jj > N - 1) return false;
+        cc = at(d, ii, jj);
+        return true;
+    };
+    size_t q;
+    if (IsU) {
+        if (Uk(i, j, q)) adj_add(V.yu, q, gE + gW, true);
+        if (Uk(i, j + 1, q)) adj_add(V.yu, q, gE, true);
+        if (Uk(i, j - 1, q)) adj_add(V.yu, q, gW, true);
+        if (Vk(i, j, q)) adj_add(V.yv, q, gN, true);
+        if (Vk(i, j + 1, q)) adj_add(V.yv, q, gN, true);
+        if (Vk(i - 1, j, q)) adj_add(V.yv, q, gS, true);
+        if (Vk(i - 1, j + 1, q)) adj_add(V.yv, q, gS, true);
+    } else {
+        if (Uk(i, j, q)) adj_add(V.yu, q, gE, true);
+        if (Uk(i + 1, j, q)) adj_add(V.yu, q, gE, true);
+        if (Uk(i, j - 1, q)) adj_add(V.yu, q, gW, true);
+        if (Uk(i + 1, j - 1, q)) adj_add(V.yu, q, gW, true);
+        if (Vk(i, j, q)) adj_add(V.yv, q, gN + gS, true);
+        if (Vk(i + 1, j, q)) adj_add(V.yv, q, gN, true);
+        if (Vk(i - 1, j, q)) adj_add(V.yv, q, gS, true);
+    }
+}
+
+// y = J^T lambda (y zeroed by the caller) after the reverse sweeps:
+// momentum rows scatter -r0b through the residual's Jacobian (dr0 = -dR),
+// their coefficient adjoints through the assembly, and clamped unknowns add
+// lambda itself (their rows are u = +-maxVel); continuity rows scatter lambda.
+__global__ void k_adj_jt(AdjCtx a, AdjVecs V, AdjSweep Us, AdjSweep Vs) {
     const Dims d = a.k.d;
     const int M = d.M, N = d.N;
     const int nU = (M - 1) * (N - 2), nV = (M - 2) * (N - 1), nC = (M - 1) * (N - 2);
-    const bool scatter = (rU == nullptr);
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nU + nV + nC; t += gridDim.x * blockDim.x) {
         if (t < nU) {
             const int i = 1 + t / (N - 2), j = 1 + t % (N - 2);
-            const double R = adj_row_u(a, i, j, scatter ? V.lu[at(d, i, j)] : 0.0, V, scatter);
-            if (!scatter) rU[at(d, i, j)] = R;
+            const size_t c = at(d, i, j);
+            adj_row_u(a, i, j, -Us.r0b[c], V, true);
+            adj_coef_row<true>(a, i, j, Us, V);
+            if (Us.clamp[c] != 0.0) adj_add(V.yu, c, V.lu[c], true);
         } else if (t < nU + nV) {
             const int q = t - nU;
             const int i = 1 + q / (N - 1), j = 1 + q % (N - 1);
-            const double R = adj_row_v(a, i, j, scatter ? V.lv[at(d, i, j)] : 0.0, V, scatter);
-            if (!scatter) rV[at(d, i, j)] = R;
+            const size_t c = at(d, i, j);
+            adj_row_v(a, i, j, -Vs.r0b[c], V, true);
+            adj_coef_row<false>(a, i, j, Vs, V);
+            if (Vs.clamp[c] != 0.0) adj_add(V.yv, c, V.lv[c], true);
         } else {
             const int q = t - nU - nV;
             const int i = 1 + q / (N - 2), j = 1 + q % (N - 2);
-            const double R = adj_row_c(a, i, j, scatter ? V.lc[at(d, i, j)] : 0.0, V, scatter);
-            if (!scatter) rC[at(d, i, j)] = R;
+            adj_row_c(a, i, j, V.lc[at(d, i, j)], V, true);
         }
     }
 }
@@ -403,13 +597,12 @@ __global__ void k_adj_defect(KParams k, AdjVecs V, double gs, double ys, double*
     if (threadIdx.x == 0) { part[2 * blockIdx.x] = acc[0]; part[2 * blockIdx.x + 1] = acc[1]; }
 }
 
-// One Jacobi sweep of the transposed, relaxed Picard momentum system for U
-// and V: (A_P^T x)(i,j) = aP x(i,j) - aW(i,j+1) x(i,j+1) - aE(i,j-1) x(i,j-1)
-// - aS(i+1,j) x(i+1,j) - aN(i-1,j) x(i-1,j) with the masked coefficients of
-// the converged assembly (aP = aP0 / uvAlpha).  first: x = 0.
-__global__ void k_adj_jacobi_t(KParams k, MomSys<double> Us, MomSys<double> Vs, const double* ru,
-                               const double* rv, const double* xu, const double* xv, double* yu, double* yv,
-                               int first) {
+// Momentum part of the preconditioner: z = -r on the unclamped momentum
+// unknowns (F_u is a Jacobi-preconditioned residual, dF_u/du ~ -I) and
+// z = r on clamped ones (identity rows); zd = r / D on the unclamped
+// unknowns and 0 on clamped ones, the input of the pressure-like rhs.
+__global__ void k_adj_prec_mom(KParams k, const double* ru, const double* rv, AdjSweep Us, AdjSweep Vs, double* zu,
+                               double* zv, double* zdu, double* zdv) {
     const Dims d = k.d;
     const int M = d.M, N = d.N;
     const int nU = (M - 1) * (N - 2), nV = (M - 2) * (N - 1);
@@ -417,18 +610,29 @@ __global__ void k_adj_jacobi_t(KParams k, MomSys<double> Us, MomSys<double> Vs, 
         const bool isU = t < nU;
         const int q = isU ? t : t - nU;
         const int w = isU ? N - 2 : N - 1;
-        const int i = 1 + q / w, j = 1 + q % w;
-        const size_t c = at(d, i, j);
-        const MomSys<double>& S = isU ? Us : Vs;
-        const double* x = isU ? xu : xv;
-        const double* r = isU ? ru : rv;
-        double Ax = 0.0;
-        if (!first) {
-            Ax = S.aP[c] * x[c] - S.aW[c + 1] * x[c + 1] - S.aE[c - 1] * x[c - 1] - S.aS[c + d.P] * x[c + d.P] -
-                 S.aN[c - d.P] * x[c - d.P];
-        }
-        const double xn = (first ? 0.0 : x[c]) + (r[c] - Ax) / S.aP[c];
-        (isU ? yu : yv)[c] = xn;
+        const size_t c = at(d, 1 + q / w, 1 + q % w);
+        const AdjSweep& S = isU ? Us : Vs;
+        const double r = (isU ? ru : rv)[c];
+        const bool cl = S.clamp[c] != 0.0;
+        (isU ? zu : zv)[c] = cl ? r : -r;
+        (isU ? zdu : zdv)[c] = cl ? 0.0 : r / S.aP[c];
+    }
+}
+
+// dE' = uvAlpha dE, dN' = uvAlpha dN with the clamped faces set to 0: the
+// pressure-like operator of the preconditioner in the forward PCG's form
+__global__ void k_adj_prec_faces(KParams k, const double* dE, const double* dN, AdjSweep Us, AdjSweep Vs,
+                                 double* dEp, double* dNp) {
+    const Dims d = k.d;
+    const int M = d.M, N = d.N;
+    const int nU = (M - 1) * (N - 2), nV = (M - 2) * (N - 1);
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nU + nV; t += gridDim.x * blockDim.x) {
+        const bool isU = t < nU;
+        const int q = isU ? t : t - nU;
+        const int w = isU ? N - 2 : N - 1;
+        const size_t c = at(d, 1 + q / w, 1 + q % w);
+        if (isU) dEp[c] = Us.clamp[c] != 0.0 ? 0.0 : k.uvAlpha * dE[c];
+        else dNp[c] = Vs.clamp[c] != 0.0 ? 0.0 : k.uvAlpha * dN[c];
     }
 }
 
@@ -450,12 +654,12 @@ __global__ void k_adj_prhs(KParams k, const double* du, const double* dv, const 
     }
 }
 
-// corrections: dm = dm* - D_A^-1 D^T dc with (D_A^-1 D^T dc)_u(i,j) =
-// rho dE(i,j) (dc(i,j+1) - dc(i,j)) and for v rho dN(i,j) (dc(i+1,j) - dc(i,j))
-// (dc zero outside the pressure unknowns); out = (dm, pAlpha dc) on the
-// U / V / continuity unknowns
-__global__ void k_adj_update(KParams k, const double* du, const double* dv, const double* dc, const double* dE,
-                             const double* dN, double relaxC, double* ou, double* ov, double* oc) {
+// corrections after the pressure-like solve: on unclamped momentum unknowns
+// z += (dR_c/dX)^T dc, i.e. u(i,j) += rho hy (dc(i,j+1) - dc(i,j)) and
+// v(i,j) += rho hx (dc(i+1,j) - dc(i,j)) (dc zero outside the pressure
+// unknowns); clamped unknowns keep z; the continuity part is dc
+__global__ void k_adj_update(KParams k, const double* zu, const double* zv, const double* dc, AdjSweep Us,
+                             AdjSweep Vs, double* ou, double* ov, double* oc) {
     const Dims d = k.d;
     const int M = d.M, N = d.N;
     const int nU = (M - 1) * (N - 2), nV = (M - 2) * (N - 1), nP = (M - 1) * (N - 2);
@@ -467,16 +671,16 @@ __global__ void k_adj_update(KParams k, const double* du, const double* dv, cons
         if (t < nU) {
             const int i = 1 + t / (N - 2), j = 1 + t % (N - 2);
             const size_t c = at(d, i, j);
-            ou[c] = du[c] - k.rho * dE[c] * (C(i, j + 1) - C(i, j));
+            ou[c] = zu[c] + (Us.clamp[c] != 0.0 ? 0.0 : k.rho * k.hy * (C(i, j + 1) - C(i, j)));
         } else if (t < nU + nV) {
             const int q = t - nU;
             const int i = 1 + q / (N - 1), j = 1 + q % (N - 1);
             const size_t c = at(d, i, j);
-            ov[c] = dv[c] - k.rho * dN[c] * (C(i + 1, j) - C(i, j));
+            ov[c] = zv[c] + (Vs.clamp[c] != 0.0 ? 0.0 : k.rho * k.hx * (C(i + 1, j) - C(i, j)));
         } else {
             const int q = t - nU - nV;
             const int i = 1 + q / (N - 2), j = 1 + q % (N - 2);
-            oc[at(d, i, j)] = relaxC * dc[at(d, i, j)];
+            oc[at(d, i, j)] = dc[at(d, i, j)];
         }
     }
 }
@@ -547,12 +751,16 @@ __global__ void k_kry_scale(double* dst, const double* src, size_t L, double s) 
 }
 
 // dJ/dgamma(cell a, b) = -sum over the faces the cell touches of
-// lambda_face * vol * vel_face * 0.5 * alpha'(gamma(a,b)); cells Ny x Nx.
-__global__ void k_adj_grad(AdjCtx a, AdjVecs V, double alphaMax, double q, double* grad) {
+// abar_face * 0.5 * alpha'(gamma(a,b)), where abar_face is the adjoint of the
+// face's alpha_face: it enters r0 as -alpha_face vol x_face (the Brinkman
+// term of R) and D = aP0 / uvAlpha as alpha_face vol / uvAlpha; cells Ny x Nx.
+__global__ void k_adj_grad(AdjCtx a, AdjSweep Us, AdjSweep Vs, double alphaMax, double q, double* grad) {
     const KParams& k = a.k;
     const Dims d = k.d;
     const int M = d.M, N = d.N, Ny = M - 1, Nx = N - 1;
-    const double vol = k.hx * k.hy;
+    const double vol = k.hx * k.hy, ia = 1.0 / k.uvAlpha;
+    auto abU = [&](size_t c) -> double { return vol * (Us.db[c] * ia - a.u[c] * Us.r0b[c]); };
+    auto abV = [&](size_t c) -> double { return vol * (Vs.db[c] * ia - a.v[c] * Vs.r0b[c]); };
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < Ny * Nx; t += gridDim.x * blockDim.x) {
         const int ca = t / Nx, cb = t % Nx;
         const double g = a.gamma[at(d, ca, cb)];
@@ -562,16 +770,16 @@ __global__ void k_adj_grad(AdjCtx a, AdjVecs V, double alphaMax, double q, doubl
         // U faces (i, j) with i-1 = ca and j-1 = cb (left cell) or j = cb (right cell); j in [1, N-2]
         const int iu = ca + 1;
         if (iu >= 1 && iu <= M - 1) {
-            if (cb + 1 <= N - 2) s += V.lu[at(d, iu, cb + 1)] * a.u[at(d, iu, cb + 1)];
-            if (cb >= 1 && cb <= N - 2) s += V.lu[at(d, iu, cb)] * a.u[at(d, iu, cb)];
+            if (cb + 1 <= N - 2) s += abU(at(d, iu, cb + 1));
+            if (cb >= 1 && cb <= N - 2) s += abU(at(d, iu, cb));
         }
         // V faces (i, j) with j-1 = cb and i-1 = ca (top cell) or i = ca (bottom cell); i in [1, M-2]
         const int jv = cb + 1;
         if (jv >= 1 && jv <= N - 1) {
-            if (ca + 1 <= M - 2) s += V.lv[at(d, ca + 1, jv)] * a.v[at(d, ca + 1, jv)];
-            if (ca >= 1 && ca <= M - 2) s += V.lv[at(d, ca, jv)] * a.v[at(d, ca, jv)];
+            if (ca + 1 <= M - 2) s += abV(at(d, ca + 1, jv));
+            if (ca >= 1 && ca <= M - 2) s += abV(at(d, ca, jv));
         }
-        grad[t] = -s * vol * 0.5 * dalpha;
+        grad[t] = -s * 0.5 * dalpha;
     }
 }
 

@@ -184,7 +184,7 @@ __device__ __forceinline__ void assemble_row(const KParams& k, const Fields& f, 
 // Range of unknowns of one component: U i in [1, M-1], j in [1, N-2];
 // V i in [1, M-2], j in [1, N-1] (momentum_solver.cpp:52-72).
 template <bool IsU>
-__device__ __forceinline__ void mom_range(const Dims& d, int& i1, int& j1) {
+__host__ __device__ __forceinline__ void mom_range(const Dims& d, int& i1, int& j1) {
     i1 = IsU ? d.M - 1 : d.M - 2;
     j1 = IsU ? d.N - 2 : d.N - 1;
 }

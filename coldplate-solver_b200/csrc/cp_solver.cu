@@ -107,7 +107,10 @@ struct cp_ctx {
     unsigned long long* mgProf = nullptr;   // per-phase timers when CP_MG_PROFILE is set
     MgMaps mgMaps;                           // TMA tensor maps of the level-0 tile phases
     // adjoint buffers (allocated on first use, double)
-    double* adj[20] = {};
+    double* adj[40] = {};
+    // forward Jacobi iterates x_1..x_s of the adjoint's frozen sweeps (U, V),
+    // allocated as the sweep counts need them
+    std::vector<double*> adjXU, adjXV;
     void* adjMom[12] = {};
     Status* adjSt = nullptr;
     double* adjPart = nullptr;
@@ -118,7 +121,6 @@ struct cp_ctx {
     double* adjKryPart = nullptr;
     double* adjH = nullptr;
     int adjRestart = 30;     // m
-    int adjSweeps = 6;       // transposed momentum Jacobi sweeps per preconditioner application
     int adjPIters = 6;       // multigrid-PCG iterations per preconditioner application
     cudaGraphExec_t graph = nullptr;
     bool graphTried = false;
@@ -1060,7 +1062,6 @@ cp_status adjoint_alloc(cp_ctx* c) {
     if ((s = dalloc(c, &c->adjPart, (size_t)4 * kMaxBlocks)) != CP_OK) return s;
     if ((s = dalloc(c, &c->adjBar, 1)) != CP_OK) return s;
     if (const char* e = getenv("CP_ADJ_RESTART")) c->adjRestart = std::min(std::max(atoi(e), 1), kKryMaxDots - 1);
-    if (const char* e = getenv("CP_ADJ_SWEEPS")) c->adjSweeps = std::max(atoi(e), 1);
     if (const char* e = getenv("CP_ADJ_PITERS")) c->adjPIters = std::max(atoi(e), 1);
     if (!c->useMg) c->adjPIters = std::max(c->adjPIters, 100);
     const size_t L = 3 * c->nElem;
@@ -1071,17 +1072,62 @@ cp_status adjoint_alloc(cp_ctx* c) {
 }
 
 template <typename TV>
-cp_status adjoint_pcg(cp_ctx* c, const KParams& k, double* out) {
+cp_status adjoint_pcg(cp_ctx* c, const KParams& k, const double* dE, const double* dN, double* out) {
     PcgBufs<TV> B = pcg_bufs<TV>(c);
     CK(cudaMemsetAsync(c->adjBar, 0, sizeof(unsigned), c->stream));
     if (c->useMg) {
         MgHier<TV> H = mg_hier<TV>(c);
-        CK(launch_coop_cfg(k_pcg_mg<TV>, c->gMg, kMgThreads, kMgDynSmem, c->stream, k, c->adjSt,
-                           (const double*)c->dE, (const double*)c->dN, B, H, out, c->adjPart, c->adjBar, c->mgMaps));
+        CK(launch_coop_cfg(k_pcg_mg<TV>, c->gMg, kMgThreads, kMgDynSmem, c->stream, k, c->adjSt, dE, dN, B, H, out,
+                           c->adjPart, c->adjBar, c->mgMaps));
     } else {
-        CK(launch_coop(k_pcg<TV>, c->gPcg, c->stream, k, c->adjSt, (const double*)c->dE, (const double*)c->dN, B,
-                       out, c->adjPart, c->adjBar));
+        CK(launch_coop(k_pcg<TV>, c->gPcg, c->stream, k, c->adjSt, dE, dN, B, out, c->adjPart, c->adjBar));
     }
+    return CP_OK;
+}
+
+// x_{j+1} buffer of the frozen sweeps (allocated on first use)
+cp_status adjoint_xbuf(cp_ctx* c, std::vector<double*>& xs, size_t j, double** out) {
+    while (xs.size() <= j) {
+        double* q = nullptr;
+        cp_status s = dalloc(c, &q, c->nElem);
+        if (s != CP_OK) return s;
+        CK(cudaMemsetAsync(q, 0, c->nElem * sizeof(double), c->stream));
+        xs.push_back(q);
+    }
+    *out = xs[j];
+    return CP_OK;
+}
+
+// The forward Jacobi sweeps of one component at the converged state, in
+// FP64 and with the reference's stop rule (sum of r^2 of the pre-update
+// residual below momentumTol^2 n, at most maxMomentumIter sweeps); the
+// iterates are kept for the reverse sweeps.  Returns the sweep count.
+template <bool IsU>
+cp_status adjoint_sweeps(cp_ctx* c, const KParams& k, const MomSys<double>& S, const double* field,
+                         std::vector<double*>& xs, int* count) {
+    int i1, j1;
+    mom_range<IsU>(c->d, i1, j1);
+    const double lim = k.momTol * k.momTol * (double)i1 * (double)j1;
+    const int nb = c->gElem;
+    std::vector<double> part(nb);
+    const double* x = nullptr;
+    int its = 0;
+    for (int q = 0; q < std::max(k.maxMom, 1); ++q) {
+        double* xn = nullptr;
+        cp_status s = adjoint_xbuf(c, xs, (size_t)q, &xn);
+        if (s != CP_OK) return s;
+        k_adj_sweep<IsU><<<nb, kThreads, 0, c->stream>>>(k, S, field, x, xn, c->adjPart);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(part.data(), c->adjPart, nb * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        double tot = 0.0;
+        for (int b = 0; b < nb; ++b) tot += part[b];
+        x = xn;
+        its = q + 1;
+        if (!std::isfinite(tot)) return fail(CP_ERR_NONFINITE, "adjoint: momentum sweep residual is not finite");
+        if (tot < lim) break;
+    }
+    *count = its;
     return CP_OK;
 }
 
@@ -1111,8 +1157,11 @@ extern "C" cp_status cp_adjoint_dp_dgamma(cp_ctx* c, double* grad, long rows, lo
     V.lu = A[0]; V.lv = A[1]; V.lc = A[2]; V.yu = A[3]; V.yv = A[4]; V.yp = A[5];
     V.gu = A[6]; V.gv = A[7]; V.gp = A[8]; V.du = A[9]; V.dv = A[10]; V.eu = A[11]; V.ev = A[12];
     double *dc = A[16], *Jd = A[17];
+    double *clampU = A[13], *clampV = A[14], *dEp = A[15], *dNp = A[19];
+    double* ybU[2] = {A[32], A[33]};
+    double* ybV[2] = {A[34], A[35]};
     const size_t bytes = c->nElem * sizeof(double);
-    for (int q = 0; q < 18; ++q) CK(cudaMemsetAsync(A[q], 0, bytes, c->stream));
+    for (int q = 0; q < 40; ++q) CK(cudaMemsetAsync(A[q], 0, bytes, c->stream));
     CK(cudaMemsetAsync(c->adjSt, 0, sizeof(Status), c->stream));
     // the converged state's iteration count fixes the inlet velocity (ramp)
     CK(cudaMemcpyAsync(c->stHost, c->st, sizeof(Status), cudaMemcpyDeviceToHost, c->stream));
@@ -1135,6 +1184,19 @@ extern "C" cp_status cp_adjoint_dp_dgamma(cp_ctx* c, double* grad, long rows, lo
     ac.k = k;
     ac.u = c->u; ac.v = c->v; ac.p = c->p; ac.alpha = c->alpha; ac.gamma = c->gamma;
     ac.maxVel = max_vel(inlet_velocity(k, iterState));
+    // the frozen sweeps: the reference's Jacobi iterates from x_0 = u (v) at
+    // the converged state, their count and the clamped unknowns
+    int sU = 0, sV = 0;
+    if ((s = adjoint_sweeps<true>(c, k, Us, c->u, c->adjXU, &sU)) != CP_OK) return s;
+    if ((s = adjoint_sweeps<false>(c, k, Vs, c->v, c->adjXV, &sV)) != CP_OK) return s;
+    const int nb = c->gElem;
+    k_adj_clampmask<true><<<nb, kThreads, 0, c->stream>>>(k, c->adjXU[sU - 1], ac.maxVel, clampU);
+    k_adj_clampmask<false><<<nb, kThreads, 0, c->stream>>>(k, c->adjXV[sV - 1], ac.maxVel, clampV);
+    CK(cudaGetLastError());
+    AdjSweep UsA{Us.aP, Us.aE, Us.aW, Us.aN, Us.aS, clampU, A[20], A[21], A[22], A[23], A[24], A[25]};
+    AdjSweep VsA{Vs.aP, Vs.aE, Vs.aW, Vs.aN, Vs.aS, clampV, A[26], A[27], A[28], A[29], A[30], A[31]};
+    k_adj_prec_faces<<<nb, kThreads, 0, c->stream>>>(k, c->dE, c->dN, UsA, VsA, dEp, dNp);
+    CK(cudaGetLastError());
     // right-hand side dJ/dX and J
     k_adj_g<<<1, 1024, 0, c->stream>>>(ac, V, Jd);
     CK(cudaGetLastError());
@@ -1142,7 +1204,6 @@ extern "C" cp_status cp_adjoint_dp_dgamma(cp_ctx* c, double* grad, long rows, lo
     KParams kp = k;
     kp.pTol = 0.0;
     kp.maxP = c->adjPIters;
-    const int nb = c->gElem;
     const int m = c->adjRestart;
     const size_t L = 3 * c->nElem;
     double* kry = c->adjKry;
@@ -1154,13 +1215,36 @@ extern "C" cp_status cp_adjoint_dp_dgamma(cp_ctx* c, double* grad, long rows, lo
     V.lu = LAM; V.lv = LAM + c->nElem; V.lc = LAM + 2 * c->nElem;
     std::vector<double> part((size_t)2 * nb);
 
+    // the reverse sweeps of both components for the adjoint vector x: the
+    // adjoints of r0 and of the coefficients into UsA / VsA
+    auto reverse = [&](const double* x) -> cp_status {
+        for (int q = 20; q < 32; ++q) CK(cudaMemsetAsync(A[q], 0, bytes, c->stream));
+        const double* yu = x;
+        const double* yv = x + c->nElem;
+        int pu = 0, pv = 0;
+        for (int j = std::max(sU, sV) - 1; j >= 0; --j) {
+            const int doU = j < sU, doV = j < sV;
+            const double* xUj = j == 0 ? c->u : c->adjXU[j - 1];
+            const double* xVj = j == 0 ? c->v : c->adjXV[j - 1];
+            const double* xUj1 = c->adjXU[std::min(j, sU - 1)];
+            const double* xVj1 = c->adjXV[std::min(j, sV - 1)];
+            k_adj_rev<<<nb, kThreads, 0, c->stream>>>(k, UsA, VsA, c->u, c->v, xUj, xUj1, xVj, xVj1, yu, yv,
+                                                      ybU[pu], ybV[pv], doU, doV, j == sU - 1, j == sV - 1);
+            CK(cudaGetLastError());
+            if (doU) { yu = ybU[pu]; pu ^= 1; }
+            if (doV) { yv = ybV[pv]; pv ^= 1; }
+        }
+        return CP_OK;
+    };
     // y = J^T x (x a Krylov vector); out = gs g - ys y on the unknowns; returns
     // (|out|^2, |g|^2) through the block partials
     auto product = [&](const double* x, double gs, double ys, double* out, double* rr, double* gg) -> cp_status {
         AdjVecs Vx = V;
         Vx.lu = const_cast<double*>(x); Vx.lv = Vx.lu + c->nElem; Vx.lc = Vx.lu + 2 * c->nElem;
+        cp_status s1 = reverse(x);
+        if (s1 != CP_OK) return s1;
         for (double* y : {V.yu, V.yv, V.yp}) CK(cudaMemsetAsync(y, 0, bytes, c->stream));
-        k_adj_jt<<<nb, kThreads, 0, c->stream>>>(ac, Vx, nullptr, nullptr, nullptr);
+        k_adj_jt<<<nb, kThreads, 0, c->stream>>>(ac, Vx, UsA, VsA);
         CK(cudaGetLastError());
         k_adj_defect<<<nb, kThreads, 0, c->stream>>>(k, V, gs, ys, out, out + c->nElem, out + 2 * c->nElem,
                                                      c->adjPart);
@@ -1176,26 +1260,19 @@ extern "C" cp_status cp_adjoint_dp_dgamma(cp_ctx* c, double* grad, long rows, lo
         }
         return CP_OK;
     };
-    // z = P^-1 r: Jacobi sweeps on the transposed Picard momentum system, then
-    // the pressure-like correction
+    // z = P^-1 r: the momentum part, then the pressure-like correction
     auto precondition = [&](const double* r, double* z) -> cp_status {
         const double *ru = r, *rv = r + c->nElem, *rp = r + 2 * c->nElem;
-        double *xu = V.du, *xv = V.dv;
-        double *yu = V.eu, *yv = V.ev;
-        for (int q = 0; q < c->adjSweeps; ++q) {
-            k_adj_jacobi_t<<<nb, kThreads, 0, c->stream>>>(k, Us, Vs, ru, rv, xu, xv, yu, yv, q == 0);
-            CK(cudaGetLastError());
-            std::swap(xu, yu);
-            std::swap(xv, yv);
-        }
-        cp_status s2 = c->prm.precision == CP_PREC_MIXED ? adjoint_prhs<float>(c, kp, xu, xv, rp)
-                                                         : adjoint_prhs<double>(c, kp, xu, xv, rp);
+        k_adj_prec_mom<<<nb, kThreads, 0, c->stream>>>(k, ru, rv, UsA, VsA, V.du, V.dv, V.eu, V.ev);
+        CK(cudaGetLastError());
+        cp_status s2 = c->prm.precision == CP_PREC_MIXED ? adjoint_prhs<float>(c, kp, V.eu, V.ev, rp)
+                                                         : adjoint_prhs<double>(c, kp, V.eu, V.ev, rp);
         if (s2 != CP_OK) return s2;
         CK(cudaMemsetAsync(c->adjSt, 0, sizeof(Status), c->stream));
-        s2 = c->prm.precision == CP_PREC_MIXED ? adjoint_pcg<float>(c, kp, dc) : adjoint_pcg<double>(c, kp, dc);
+        s2 = c->prm.precision == CP_PREC_MIXED ? adjoint_pcg<float>(c, kp, dEp, dNp, dc)
+                                               : adjoint_pcg<double>(c, kp, dEp, dNp, dc);
         if (s2 != CP_OK) return s2;
-        k_adj_update<<<nb, kThreads, 0, c->stream>>>(k, xu, xv, dc, c->dE, c->dN, c->prm.pAlpha, z, z + c->nElem,
-                                                     z + 2 * c->nElem);
+        k_adj_update<<<nb, kThreads, 0, c->stream>>>(k, V.du, V.dv, dc, UsA, VsA, z, z + c->nElem, z + 2 * c->nElem);
         CK(cudaGetLastError());
         return CP_OK;
     };
@@ -1228,7 +1305,6 @@ extern "C" cp_status cp_adjoint_dp_dgamma(cp_ctx* c, double* grad, long rows, lo
         std::fill(gv.begin(), gv.end(), 0.0);
         gv[0] = beta;
         int jn = 0;
-        double est = res;
         for (int j = 0; j < m && it < max_iter; ++j) {
             if ((s = precondition(Vq(j), Zq(j))) != CP_OK) return s;
             if ((s = product(Zq(j), 0.0, -1.0, W, nullptr, nullptr)) != CP_OK) return s;
@@ -1269,10 +1345,9 @@ extern "C" cp_status cp_adjoint_dp_dgamma(cp_ctx* c, double* grad, long rows, lo
             gv[j] = gc[j] * gv[j];
             ++it;
             jn = j + 1;
-            est = gnorm > 0.0 ? std::fabs(gv[j + 1]) / gnorm : 0.0;
+            const double est = gnorm > 0.0 ? std::fabs(gv[j + 1]) / gnorm : 0.0;
             if (est <= tol || hn == 0.0) break;
         }
-        (void)est;
         // y = R^-1 g; lambda += Z y
         for (int i = jn - 1; i >= 0; --i) {
             double a = gv[i];
@@ -1287,10 +1362,11 @@ extern "C" cp_status cp_adjoint_dp_dgamma(cp_ctx* c, double* grad, long rows, lo
         beta = std::sqrt(rr);
         res = gnorm > 0.0 ? beta / gnorm : 0.0;
     }
-    // gradient on the Ny x Nx cells
+    // gradient on the Ny x Nx cells from the reverse sweeps of lambda
+    if ((s = reverse(LAM)) != CP_OK) return s;
     double* gd = A[18];
     const double amax = c->prm.eta / std::max(c->prm.brinkmanKMin, 1e-20);
-    k_adj_grad<<<nb, kThreads, 0, c->stream>>>(ac, V, amax, c->prm.brinkmanQ, gd);
+    k_adj_grad<<<nb, kThreads, 0, c->stream>>>(ac, UsA, VsA, amax, c->prm.brinkmanQ, gd);
     CK(cudaGetLastError());
     CK(cudaEventRecord(c->ev1, c->stream));
     std::vector<double> g((size_t)(M - 1) * (N - 1));

@@ -9,6 +9,10 @@
 #   ref_f64_pin   the same sources re-typed to double by a textual substitution
 #                 (float->double, MatrixXf->MatrixXd, VectorXf->VectorXd, 'f'
 #                 literal suffixes dropped), -ffp-contract=off: the FP64 oracle
+#   ref_dropin    the shipped sources with Utilities/iterations.cpp replaced by
+#                 the GPU drop-in (coldplate-solver_b200/dropin/), linked
+#                 against libcoldplate.so: the reference's own outer loop
+#                 running on the library
 #
 # The re-typed copy lives only in a temporary directory; nothing from REF_DIR
 # is written into the repository.
@@ -70,6 +74,35 @@ find "$SRC64" \( -name '*.cpp' -o -name '*.h' \) -print0 | xargs -0 sed -i -E \
     -e 's/MatrixXf/MatrixXd/g' -e 's/VectorXf/VectorXd/g' \
     -e 's/\b([0-9][0-9]*\.?[0-9]*([eE][-+]?[0-9]+)?)[fF]\b/\1/g'
 build ref_f64_pin "$SRC64" double -O2 -ffp-contract=off
+
+# the reference's own outer loop (SIMPLE::runIterations) over the GPU library:
+# its sources as shipped except Utilities/iterations.cpp, which is replaced by
+# the drop-in coldplate-solver_b200/dropin/iterations_gpu.cpp, linked against
+# coldplate-solver_b200/libcoldplate.so (found through a relative rpath)
+ROOT="$(cd "$HERE/../.." && pwd)"
+LIB="$ROOT/coldplate-solver_b200/libcoldplate.so"
+if [ -f "$LIB" ]; then
+    obj="$TMP/obj_dropin"
+    mkdir -p "$obj"
+    objs=()
+    for s in $SRCS_REL; do
+        [ "$s" = "Utilities/iterations.cpp" ] && continue
+        o="$obj/$(echo "$s" | tr '/' '_').o"
+        extra=()
+        [ "$s" = "SIMPLE.cpp" ] && extra=(-Dmain=ref_main_unused)
+        "$CXX" "${GOMP_B[@]}" -std=c++17 -O2 -fopenmp -w "${extra[@]}" -I"$HERE/shim" -I"$REF_DIR" \
+            -I"$REF_DIR/Utilities" -c "$REF_DIR/$s" -o "$o" &
+        objs+=("$o")
+    done
+    "$CXX" "${GOMP_B[@]}" -std=c++17 -O2 -fopenmp -Wall -I"$HERE/shim" -I"$REF_DIR" -I"$REF_DIR/Utilities" \
+        -I"$ROOT/include" -c "$ROOT/coldplate-solver_b200/dropin/iterations_gpu.cpp" -o "$obj/iterations_gpu.o" &
+    "$CXX" "${GOMP_B[@]}" -std=c++17 -O2 -fopenmp -w -DREF_REAL=float -I"$HERE/shim" -I"$REF_DIR" \
+        -I"$REF_DIR/Utilities" -c "$HERE/harness.cpp" -o "$obj/harness.o" &
+    wait
+    "$CXX" "${GOMP_B[@]}" -fopenmp "${objs[@]}" "$obj/iterations_gpu.o" "$obj/harness.o" "$LIB" \
+        -Wl,-rpath,'$ORIGIN/../../coldplate-solver_b200' -o "$OUT/ref_dropin"
+    echo "built $OUT/ref_dropin"
+fi
 
 # the thermal solver (ThermalSolver/thermal_solver.cpp, one translation unit)
 # against the AMGCL API stand-in in shim/amgcl: the reference's own assembly,

@@ -1,0 +1,60 @@
+"""The adjoint gradient where the reference's velocity clamp is active.
+
+At the converged state of the constricted channel (cases.constricted_channel)
+and of the 256 x 128 density field, velocities sit on the +-3 max(U_in, 0.1)
+clamp.  The adjoint differentiates the fixed point the reference iteration
+reaches there (frozen Jacobi sweep count and clamped set); it must agree with
+central differences (h = 1e-4) of converged FP64 forward solves, restarted
+from the base state and stepped until the difference is stationary, within
+1e-4 relative on every checked cell.  The one-sided quotients are reported:
+on a clamped state they differ from each other by a term in |h| (the slow
+near-null pressure mode the clamp creates), not from the central value.
+"""
+import numpy as np
+import pytest
+
+from coldplate_b200 import Simple, cases
+from coldplate_b200.fdcheck import FiniteDifferences, clamped_unknowns, pick_cells, run_stationary
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-4
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _lib(built_lib):
+    return built_lib
+
+
+def _check(case, cells, base_iters, fd_iters, min_clamped):
+    gamma = 1.0 - case.cellType
+    cap = max(base_iters, fd_iters) + 200
+    prm = case.params(precision="fp64", maxIterations=cap + 10, epsilon=1e-30, historyCapacity=cap + 10)
+    with Simple(gamma=gamma, **prm) as base:
+        J0, n0, rel0 = run_stationary(base, 1e-14, base_iters)
+        grad, rep = base.adjoint_dp_dgamma(max_iter=20000, tol=1e-11)
+        state = {f: base.get(f) for f in ("u", "v", "p")}
+        nclamp = clamped_unknowns(base, 3.0 * max(abs(case.U), 0.1))
+    assert nclamp >= min_clamped, nclamp
+    assert rep["converged"], rep
+    out = []
+    with FiniteDifferences(gamma, prm, state) as fdc:
+        for (i, j) in cells:
+            r = fdc.cell(i, j, 1e-4, 1e-9, fd_iters)
+            out.append((i, j, r["fd"], float(grad[i, j]), r["fwd"], r["bwd"]))
+    bad = [o for o in out if abs(o[3] - o[2]) > TOL * abs(o[2])]
+    assert not bad, (bad, out)
+    return out
+
+
+def test_adjoint_on_the_constricted_channel():
+    case = cases.constricted_channel(32, 96, pressureSolverType=4, maxPressureIter=30, pTol=1e-6)
+    # the gamma = 0.5 cells along the block faces, both sides of the gap
+    _check(case, [(12, 45), (19, 50), (5, 39), (25, 39)], 40000, 40000, min_clamped=50)
+
+
+def test_adjoint_on_the_density_field_256x128():
+    case = cases.density_field(128, 256, seed=0, pressureSolverType=4, maxPressureIter=30, pTol=1e-6)
+    gamma = 1.0 - case.cellType
+    cells = pick_cells(gamma, 6, np.random.default_rng(1))
+    _check(case, cells, 30000, 30000, min_clamped=100)
