@@ -73,6 +73,8 @@ def parse():
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--batch-fields", type=int, default=64)
     ap.add_argument("--batch-outer", type=int, default=200)
+    ap.add_argument("--batch-adjoint-fields", type=int, default=64,
+                    help="fields of the batch whose adjoint is timed after the run")
     ap.add_argument("--no-thermal", action="store_true")
     ap.add_argument("--only", choices=["thermal", "batch"], default=None,
                     help="run one leg alone and print its JSON object (profiling runs)")
@@ -381,21 +383,37 @@ def max_over_ranks(x: float, dist, device: str) -> float:
 BATCH_SINGLE_OUTER = 20
 
 
-def batch_leg(Simple, torch, args) -> dict:
-    """--batch-fields density fields (64 by default: Nx in 256-1024, Ny in
-    128-512, U_in in 0.2-1.0 m/s, mixed precision, epsilon 1e-6) advanced by
-    the batched kernel for --batch-outer outer iterations (200) with the
-    autotuned tile, against the same
-    fields solved one after the other (BATCH_SINGLE_OUTER iterations each).
-    Most of these fields never reach epsilon 1e-6 with the reference's SIMPLE
-    iteration (their residual RMS levels off near 1e-5), so the leg times a
-    fixed number of iterations and reports cell-iterations per second."""
-    from coldplate_b200 import Batch, cases
-    nf, nout = args.batch_fields, args.batch_outer
-    cs = cases.batch(nf, seed=args.seed, **BENCH_KNOBS)
+def batch_fields(args, rank: int = 0, world: int = 1):
+    """The batch workload (--batch-fields density fields: Nx in 256-1024,
+    Ny in 128-512, U_in in 0.2-1.0 m/s) and this rank's share of it: the
+    fields are independent, so under torchrun they are split across the
+    ranks by cells x outer iterations (partition_fields), each rank
+    advancing its own fields with no exchange."""
+    from coldplate_b200 import cases, partition_fields
+    cs = cases.batch(args.batch_fields, seed=args.seed, **BENCH_KNOBS)
     cells = [c.cellType.shape[0] * c.cellType.shape[1] for c in cs]
+    mine = partition_fields([n * args.batch_outer for n in cells], world)[rank]
+    return cs, cells, mine
+
+
+def batch_leg(Simple, torch, args, rank: int = 0, world: int = 1, dist=None) -> dict:
+    """This rank's share of the batch workload, mixed precision, epsilon
+    1e-6, advanced by the batched kernel for --batch-outer outer iterations
+    (200) with the autotuned tile; then the adjoint dP/dgamma of every field
+    at its state; against the same fields solved one after the other
+    (BATCH_SINGLE_OUTER iterations each).  Most of these fields never reach
+    epsilon 1e-6 with the reference's SIMPLE iteration (their residual RMS
+    levels off near 1e-5), so the leg times a fixed number of iterations and
+    reports cell-iterations per second.  Under torchrun the work and the
+    device time are combined over the ranks (sum and max)."""
+    from coldplate_b200 import Batch
+    nout = args.batch_outer
+    cs_all, cells_all, mine = batch_fields(args, rank, world)
+    cs = [cs_all[q] for q in mine]
+    cells = [cells_all[q] for q in mine]
     prm = dict(precision="mixed", epsilon=1e-6, maxIterations=nout, historyCapacity=nout)
     fields = [Simple(cellType=c.cellType, **c.params(**prm)) for c in cs]
+    adj_ms, adj_its, adj_conv = 0.0, [], 0
     try:
         with Batch(fields) as b:
             tune = b.autotune(3)
@@ -403,11 +421,26 @@ def batch_leg(Simple, torch, args) -> dict:
             torch.cuda.synchronize()
             rep = b.run(nout)
             its = [len(f.history()["iter"]) for f in fields]
+        for f in fields[:args.batch_adjoint_fields]:
+            _, ar = f.adjoint_dp_dgamma(max_iter=ADJ_MAX_ITER, tol=ADJ_TOL)
+            adj_ms += ar["device_ms"]
+            adj_its.append(ar["iterations"])
+            adj_conv += int(ar["converged"])
     finally:
         for f in fields:
             f.close()
     work = float(sum(n * k for n, k in zip(cells, its)))
     t = rep["device_ms"] / 1e3
+    n_adj = len(adj_its)
+    adj_cells = float(sum(cells[:n_adj]))
+    t_adj = adj_ms / 1e3
+    if dist is not None:
+        tot = torch.tensor([work, adj_cells], dtype=torch.float64, device="cuda")
+        mx = torch.tensor([t, t_adj], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tot, op=dist.ReduceOp.SUM)
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        work, adj_cells = float(tot[0]), float(tot[1])
+        t, t_adj = float(mx[0]), float(mx[1])
     # the same fields solved alone (one context, cp_step) for a few iterations each
     t1, work1 = 0.0, 0.0
     for c, n in zip(cs, cells):
@@ -415,14 +448,18 @@ def batch_leg(Simple, torch, args) -> dict:
             r = s.step(BATCH_SINGLE_OUTER)
             t1 += r["device_ms"] / 1e3
             work1 += n * BATCH_SINGLE_OUTER
-    return {"workload": f"{nf} density fields, Nx 256-1024, Ny 128-512, U_in 0.2-1.0 m/s, seed {args.seed}, "
-                        f"mixed, {nout} outer iterations",
-            "cells": int(sum(cells)), "t_s": t, "launches": rep["launches"],
+    return {"workload": f"{args.batch_fields} density fields, Nx 256-1024, Ny 128-512, U_in 0.2-1.0 m/s, seed "
+                        f"{args.seed}, mixed, {nout} outer iterations; adjoint of each field after the batch"
+                        + (f"; fields split over {world} ranks by cells" if world > 1 else ""),
+            "cells": int(sum(cells_all)), "fields_this_rank": len(cs), "t_s": t, "launches": rep["launches"],
             "tile": [rep["tileRows"], rep["tileCols"]], "autotune_trial_ms": tune["device_ms"],
             "cell_iterations_per_s": work / t,
             "sequential_single_cell_iterations_per_s": work1 / t1,
             "speedup_vs_sequential": (work / t) / (work1 / t1),
-            "fields_done": rep["fieldsDone"]}
+            "fields_done": rep["fieldsDone"],
+            "adjoint": {"fields": n_adj, "t_s": t_adj, "converged": adj_conv,
+                        "iterations_max": max(adj_its) if adj_its else None,
+                        "cells_per_s": adj_cells / t_adj if t_adj > 0 else None}}
 
 
 # ------------------------------------------------------------------ 3-D thermal solve + p-norm adjoint
@@ -620,7 +657,7 @@ def main():
     # ---- batched solves: 64 density fields of random size in one persistent kernel
     batch_line = None
     if not args.no_batch:
-        batch_line = batch_leg(Simple, torch, args)
+        batch_line = batch_leg(Simple, torch, args, rank, world, dist)
 
     # ---- 3-D thermal solve and its p-norm adjoint on a 1024 x 512 density flow
     thermal_line = None

@@ -209,6 +209,23 @@ class Simple:
         return it.value, r.value
 
 
+def partition_fields(work, n_parts: int) -> list[list[int]]:
+    """Split fields of the given work (e.g. cells x expected outer
+    iterations) into n_parts groups of nearly equal total work, one per GPU:
+    largest first, each to the currently lightest group.  Fields are
+    independent, so the groups need no exchange; every field lands in
+    exactly one group.  Returns the field indices of each group, ascending."""
+    if n_parts < 1:
+        raise ValueError("n_parts must be >= 1")
+    load = [0.0] * n_parts
+    parts: list[list[int]] = [[] for _ in range(n_parts)]
+    for q in sorted(range(len(work)), key=lambda i: (-float(work[i]), i)):
+        k = min(range(n_parts), key=lambda r: (load[r], r))
+        parts[k].append(q)
+        load[k] += float(work[q])
+    return [sorted(pq) for pq in parts]
+
+
 class Batch:
     """Several ``Simple`` fields (grid sizes, geometries and inlet velocities
     may all differ) advanced together by one persistent kernel per launch
