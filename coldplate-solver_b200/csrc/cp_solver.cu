@@ -22,6 +22,7 @@
 
 #include "cp_kernels.cuh"
 #include "cp_mg.cuh"
+#include "cp_sa.cuh"
 #include "cp_adjoint.cuh"
 #include "cp_batch.cuh"
 
@@ -105,6 +106,15 @@ struct cp_ctx {
     // about a quarter, with the same converged pressure drop.
     double mgScale = 1.8;
     unsigned long long* mgProf = nullptr;   // per-phase timers when CP_MG_PROFILE is set
+    // smoothed-aggregation hierarchy (pressureSolverType 4); the 2 x 2 one
+    // above stays for type 2 and for batches
+    bool useSa = false;
+    int saL = 0, saLg = 0;
+    int saNI[kSaMaxLevels] = {}, saNJ[kSaMaxLevels] = {}, saP[kSaMaxLevels] = {};
+    void* saArr[kSaMaxLevels][13] = {};     // c[0..8] x y b t (level 0: x y t only)
+    void* saY[9] = {};
+    void* saDense = nullptr;
+    double saOmega = 0.9, saW0 = 2.0 / 3.0, saWc = 0.8;
     MgMaps mgMaps;                           // TMA tensor maps of the level-0 tile phases
     // adjoint buffers (allocated on first use, double)
     double* adj[40] = {};
@@ -454,6 +464,78 @@ cp_status mg_build(cp_ctx* c) {
     return CP_OK;
 }
 
+template <typename TV>
+SaHier<TV> sa_hier(cp_ctx* c) {
+    SaHier<TV> H;
+    memset(&H, 0, sizeof(H));
+    H.L = c->saL;
+    H.Lg = c->saLg;
+    H.omega = c->saOmega;
+    H.w0 = c->saW0;
+    H.wc = c->saWc;
+    H.dense = (TV*)c->saDense;
+    for (int q = 0; q < 9; ++q) H.Y[q] = (TV*)c->saY[q];
+    for (int l = 0; l < c->saL; ++l) {
+        SaLevel<TV>& v = H.lv[l];
+        v.nI = c->saNI[l]; v.nJ = c->saNJ[l]; v.P = c->saP[l];
+        TV** a = reinterpret_cast<TV**>(c->saArr[l]);
+        for (int q = 0; q < 9; ++q) v.c[q] = a[q];
+        v.x = a[9]; v.y = a[10]; v.b = a[11]; v.t = a[12];
+    }
+    return H;
+}
+
+// dynamic shared memory of k_pcg_sa: the dense set-up workspace
+constexpr size_t kSaDynSmem = sizeof(double) * (size_t)(kSaDense * 2 * kSaDense + kSaDense);
+static_assert(kSaDynSmem + 4096 <= 227 * 1024, "k_pcg_sa's dynamic shared memory exceeds a block's limit");
+
+// Level sizes of the smoothed aggregation: 3 x 3 aggregates (rounding up)
+// until at most kSaDense unknowns; levels above kSaCtaCells unknowns (and
+// always level 0) run grid-wide.
+cp_status sa_build(cp_ctx* c) {
+    int nI = c->d.M - 1, nJ = c->d.N - 2;
+    int L = 0;
+    for (;;) {
+        if (L >= kSaMaxLevels) return fail(CP_ERR_BAD_PARAM, "smoothed-aggregation hierarchy too deep");
+        c->saNI[L] = nI; c->saNJ[L] = nJ;
+        ++L;
+        if ((long long)nI * nJ <= kSaDense && L >= 2) break;
+        nI = sa_coarse(nI); nJ = sa_coarse(nJ);
+    }
+    c->saL = L;
+    int Lg = 1;
+    while (Lg < L && (long long)c->saNI[Lg] * c->saNJ[Lg] > kSaCtaCells) ++Lg;
+    c->saLg = Lg;
+    c->saP[0] = c->d.P;
+    cp_status s;
+    for (int q = 9; q <= 12; ++q) {
+        if (q == 11) continue;                 // level 0's rhs is the CG residual
+        if ((s = dalloc_bytes(c, &c->saArr[0][q], c->nElem * c->es)) != CP_OK) return s;
+    }
+    for (int l = 1; l < L; ++l) {
+        c->saP[l] = ((c->saNJ[l] + 2 + 31) / 32) * 32;
+        const size_t ne = (size_t)(c->saNI[l] + 2) * c->saP[l];
+        for (int q = 0; q < 13; ++q)
+            if ((s = dalloc_bytes(c, &c->saArr[l][q], ne * c->es)) != CP_OK) return s;
+    }
+    for (int q = 0; q < 9; ++q)
+        if ((s = dalloc_bytes(c, &c->saY[q], c->nElem * c->es)) != CP_OK) return s;
+    if ((s = dalloc_bytes(c, &c->saDense, (size_t)kSaDense * kSaDense * c->es)) != CP_OK) return s;
+    if (const char* e = getenv("CP_SA_OMEGA")) c->saOmega = atof(e);
+    if (const char* e = getenv("CP_SA_W0")) c->saW0 = atof(e);
+    if (const char* e = getenv("CP_SA_WC")) c->saWc = atof(e);
+    int nb = 0;
+    if (c->prm.precision == CP_PREC_MIXED) {
+        cudaFuncSetAttribute(k_pcg_sa<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSaDynSmem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_pcg_sa<float>, kMgThreads, kSaDynSmem);
+    } else {
+        cudaFuncSetAttribute(k_pcg_sa<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSaDynSmem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_pcg_sa<double>, kMgThreads, kSaDynSmem);
+    }
+    if (nb < 1) return fail(CP_ERR_CUDA, "smoothed-aggregation PCG kernel does not fit on an SM");
+    return CP_OK;
+}
+
 template <typename Kern, typename... Args>
 cudaError_t launch_coop_cfg(Kern kern, int grid, int threads, size_t smem, cudaStream_t s, Args... args) {
     cudaLaunchConfig_t cfg = {};
@@ -496,7 +578,11 @@ cp_status enqueue_pressure(cp_ctx* c, EvRec* rec = nullptr) {
     CK(cudaGetLastError());
     CK(cudaMemsetAsync(c->barP, 0, sizeof(unsigned), c->stream));
     REC_BEGIN(rec, CP_K_PCG);
-    if (c->useMg) {
+    if (c->useSa) {
+        SaHier<TV> H = sa_hier<TV>(c);
+        CK(launch_coop_cfg(k_pcg_sa<TV>, c->gMg, kMgThreads, kSaDynSmem, c->stream, c->k, c->st,
+                           (const double*)c->dE, (const double*)c->dN, B, H, c->pStar, c->partP, c->barP));
+    } else if (c->useMg) {
         MgHier<TV> H = mg_hier<TV>(c);
         CK(launch_coop_cfg(k_pcg_mg<TV>, c->gMg, kMgThreads, kMgDynSmem, c->stream, c->k, c->st,
                            (const double*)c->dE, (const double*)c->dN, B, H, c->pStar, c->partP, c->barP, c->mgMaps));
@@ -797,6 +883,11 @@ cp_status cp_create(const cp_params* prm, cp_ctx** out) {
         return bail(fail(CP_ERR_CUDA, "too many SMs for the partial-sum buffers"));
     c->useMg = (prm->pressureSolverType == 2 || prm->pressureSolverType == 4);
     if (c->useMg && (s = mg_build(c)) != CP_OK) return bail(s);
+    // type 4 (AMGCL's AMG-CG in the reference) runs the smoothed-aggregation
+    // cycle; CP_PRESSURE_CYCLE=pairs selects the 2 x 2 aggregation of type 2
+    const char* cyc = getenv("CP_PRESSURE_CYCLE");
+    c->useSa = prm->pressureSolverType == 4 && !(cyc && strcmp(cyc, "pairs") == 0);
+    if (c->useSa && (s = sa_build(c)) != CP_OK) return bail(s);
     if ((s = dalloc(c, &c->partJ, (size_t)4 * c->gJac)) != CP_OK) return bail(s);
     if ((s = dalloc(c, &c->partM, (size_t)4 * c->nbMass)) != CP_OK) return bail(s);
     if ((s = dalloc(c, &c->partP, (size_t)3 * std::max(c->gPcg, c->gMg))) != CP_OK) return bail(s);
@@ -1075,7 +1166,11 @@ template <typename TV>
 cp_status adjoint_pcg(cp_ctx* c, const KParams& k, const double* dE, const double* dN, double* out) {
     PcgBufs<TV> B = pcg_bufs<TV>(c);
     CK(cudaMemsetAsync(c->adjBar, 0, sizeof(unsigned), c->stream));
-    if (c->useMg) {
+    if (c->useSa) {
+        SaHier<TV> H = sa_hier<TV>(c);
+        CK(launch_coop_cfg(k_pcg_sa<TV>, c->gMg, kMgThreads, kSaDynSmem, c->stream, k, c->adjSt, dE, dN, B, H, out,
+                           c->adjPart, c->adjBar));
+    } else if (c->useMg) {
         MgHier<TV> H = mg_hier<TV>(c);
         CK(launch_coop_cfg(k_pcg_mg<TV>, c->gMg, kMgThreads, kMgDynSmem, c->stream, k, c->adjSt, dE, dN, B, H, out,
                            c->adjPart, c->adjBar, c->mgMaps));

@@ -104,3 +104,36 @@ def test_multigrid_pcg_stops_on_the_relative_residual(ptol):
     if it > 1:
         it2, rel2 = solve(it - 1)
         assert it2 == it - 1 and rel2 > ptol * 0.999, (it2, rel2)
+
+
+def test_smoothed_aggregation_cycle_matches_its_oracle():
+    """pressureSolverType 4 runs smoothed aggregation (3 x 3 aggregates,
+    9-point Galerkin levels, weights 2/3 and 0.8, V(1,1) with Jacobi 0.9):
+    the GPU's FP64 CG iteration count equals that of the same cycle in the
+    oracle (oracle/pressure_sa.py) on a 512 x 256 density state, whose
+    hierarchy has two grid-wide levels and CTA levels below."""
+    from coldplate_b200 import cases
+    from pressure_sa import Level, galerkin, pcg, pressure_stencil, vcycle
+    case = cases.density_field(256, 512, seed=0)
+    o = oracle_for(case, pressureSolverType=1, maxPressureIter=200)
+    o.run(30)
+    o.momentum(True)
+    o.momentum(False)
+    dE, dN, uS, vS = o.get("dE"), o.get("dN"), o.get("uStar"), o.get("vStar")
+    A, b, nI, nJ = pressure_system(dE, dN, uS, vS, 1000.0, case.hx, case.hy)
+    St = pressure_stencil(dE, dN, 1000.0, case.hx, case.hy)
+    levels, Al = [], St
+    while Al[(0, 0)].size > 64:
+        lv = Level(Al, 2.0 / 3.0 if not levels else 0.8)
+        levels.append(lv)
+        Al = galerkin(lv)
+    levels.append(Level(Al, None))
+    _, it_o = pcg(St, b.reshape(nI, nJ), lambda r: vcycle(levels, r, 0.9), tol=1e-6, maxit=200)
+    with gpu_for(case, pressureSolverType=4, maxPressureIter=200, pTol=1e-6, precision="fp64") as g:
+        for f, a in (("dE", dE), ("dN", dN), ("uStar", uS), ("vStar", vS)):
+            g.set(f, a)
+        it, _ = g.solvePressureSystem()
+        x = g.get("pStar")[1:-1, 1:-2].reshape(-1)
+    assert len(levels) >= 4 and it_o <= 20
+    assert abs(it - it_o) <= 1, (it, it_o)
+    assert np.linalg.norm(b - A @ x) <= 1e-6 * 1.001 * np.linalg.norm(b)
