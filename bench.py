@@ -51,6 +51,8 @@ ADJ_MAX_ITER = 2000
 # ncu captures of the dominant kernels (profiles/): DRAM bytes read + written
 PCG_MG_CAPTURE_BYTES = (850.3 + 1406.4) * 1e6     # k_pcg_mg<float>, one launch
 PCG_MG_CAPTURE_ITERS = 30
+PCG_SA_CAPTURE_BYTES = None                        # k_pcg_sa<float>, one launch (not captured yet)
+PCG_SA_CAPTURE_ITERS = 1
 THERMAL_CAPTURE_BYTES_PER_CELL_ITER = 702.0        # k_th_bicgstab, 512 x 256 x 12 capture
 
 
@@ -631,11 +633,23 @@ def main():
     w_mix = 4
     pcg_ms = kt["ms"]["pcg"] / max(kt["launches"]["pcg"], 1)
     pcg_iters = kt["pcgIterations"] / max(kt["launches"]["pcg"], 1)
-    # 23 w per unknown per multigrid-PCG iteration: 8 w for the CG vectors
-    # (read x, r, p, dE, dN; write x, r, p) and 15 w for the V(1,1) cycle
-    # (fine-level restriction and prolongation-smoothing, 11.25 w, times 4/3
-    # for the coarse levels)
-    pcg_bytes = pcg_iters * 23 * w_mix * nP
+    sa = os.environ.get("CP_PRESSURE_CYCLE") != "pairs"
+    if sa:
+        # smoothed aggregation: 37 w per unknown per CG iteration: 8 w for the
+        # CG vectors (read x, r, p, dE, dN; write x, r, p), 23 w for level 0 of
+        # the V(1,1) cycle (residual 7, restriction 5, prolongation 5,
+        # post-smoothing 6) and 6 w for the 9-point coarse levels (four passes
+        # over 13 arrays at a ninth of the unknowns, 47 w there, times 9/8 for
+        # the levels below)
+        words, kname = 37, "k_pcg_sa<float>"
+        cap_bytes, cap_iters = PCG_SA_CAPTURE_BYTES, PCG_SA_CAPTURE_ITERS
+    else:
+        # 2 x 2 aggregation: 23 w per unknown per CG iteration: 8 w for the CG
+        # vectors and 15 w for the V(1,1) cycle (fine-level restriction and
+        # prolongation-smoothing, 11.25 w, times 4/3 for the coarse levels)
+        words, kname = 23, "k_pcg_mg<float>"
+        cap_bytes, cap_iters = PCG_MG_CAPTURE_BYTES, PCG_MG_CAPTURE_ITERS
+    pcg_bytes = pcg_iters * words * w_mix * nP
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -644,14 +658,13 @@ def main():
     peak = float(peaks.get("hbm_gbs", 6650.0))
     achieved = pcg_bytes / (pcg_ms * 1e-3) / 1e9
     # DRAM traffic of one launch from the ncu capture of this kernel on this
-    # workload (profiles/k_pcg_mg_float_density_2048x1024.md: 850.3 + 1406.4 MB
-    # for a launch of 30 CG iterations, taken with 16 x 64 float tiles; the
-    # 32 x 64 tiles read the same arrays with less halo), scaled to this
-    # line's CG iterations
-    traffic = PCG_MG_CAPTURE_BYTES * pcg_iters / PCG_MG_CAPTURE_ITERS
+    # workload (profiles/), scaled to this line's CG iterations
+    traffic = cap_bytes * pcg_iters / cap_iters if cap_bytes else None
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": traffic, "algorithmic_bytes": pcg_bytes, "kernel": "k_pcg_mg<float>",
-                "traffic_source": "ncu capture (2048x1024, 30 CG iterations) scaled by CG iterations",
+                "traffic": traffic, "algorithmic_bytes": pcg_bytes, "kernel": kname,
+                "bytes_per_unknown_per_cg_iteration": words * w_mix,
+                "traffic_source": (f"ncu capture (2048x1024, {cap_iters} CG iterations) scaled by CG iterations"
+                                   if cap_bytes else "no capture of this kernel yet"),
                 "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"}
 
     # ---- batched solves: 64 density fields of random size in one persistent kernel
