@@ -42,7 +42,7 @@ PARAM_FIELDS = [
     ("rho", _D), ("eta", _D), ("enableInletRamp", _I), ("rampSteps", _I), ("uvAlpha", _D), ("pAlpha", _D),
     ("enableResidualViscosity", _I), ("enableNormalizedResiduals", _I), ("residNormFloorVel", _D),
     ("residNormFloorMass", _D),
-    ("precision", _I), ("historyCapacity", _I), ("chunk", _I),
+    ("precision", _I), ("historyCapacity", _I), ("chunk", _I), ("adjointModel", _I),
 ]
 
 
@@ -79,7 +79,8 @@ class CpKernelTiming(ctypes.Structure):
 
 class CpAdjointReport(ctypes.Structure):
     _fields_ = [("iterations", ctypes.c_int), ("converged", ctypes.c_int), ("residual", ctypes.c_double),
-                ("J", ctypes.c_double), ("device_ms", ctypes.c_double)]
+                ("J", ctypes.c_double), ("device_ms", ctypes.c_double), ("model", ctypes.c_int),
+                ("clampedUnknowns", ctypes.c_int)]
 
 
 class CpBatchReport(ctypes.Structure):

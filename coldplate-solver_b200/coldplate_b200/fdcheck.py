@@ -132,12 +132,14 @@ def main(argv=None) -> dict:
     ap.add_argument("--fd-iters", type=int, default=6000)
     ap.add_argument("--dtol", type=float, default=1e-7)
     ap.add_argument("--adjoint-tol", type=float, default=1e-10)
+    ap.add_argument("--adjoint-model", type=int, default=0, help="cp_adjoint_model: 0 auto, 1 equations, 2 fixed point")
     a = ap.parse_args(argv)
 
     case = make_case(a.case, a.ny, a.nx, a.seed)
     gamma = 1.0 - case.cellType
     cap = max(a.base_iters, a.fd_iters) + 200
-    prm = case.params(precision="fp64", maxIterations=cap + 10, epsilon=1e-30, historyCapacity=cap + 10)
+    prm = case.params(precision="fp64", maxIterations=cap + 10, epsilon=1e-30, historyCapacity=cap + 10,
+                      adjointModel=a.adjoint_model)
     t0 = time.time()
     with Simple(gamma=gamma, **prm) as base:
         J0, n0, rel0 = run_stationary(base, a.stationary, a.base_iters)
@@ -145,7 +147,7 @@ def main(argv=None) -> dict:
         state = {f: base.get(f) for f in ("u", "v", "p")}
         nclamp = clamped_unknowns(base, 3.0 * max(abs(case.U), 0.1))
     print(f"base: dP {J0:.12g} Pa after {n0} iterations (stationary {rel0:.1e}), {nclamp} velocities on the "
-          f"clamp; adjoint {rep['iterations']} iterations, residual {rep['residual']:.1e}, "
+          f"clamp; adjoint (model {rep['model']}) {rep['iterations']} iterations, residual {rep['residual']:.1e}, "
           f"{rep['device_ms']:.0f} ms", flush=True)
     rng = np.random.default_rng(a.seed + 1)
     cells = pick_cells(gamma, a.cells, rng, buffer=32 if a.case == "density" else 8)
@@ -166,7 +168,7 @@ def main(argv=None) -> dict:
     sig = np.array([abs(r["fd"]) >= 1e-2 * scale for r in rows])
     out = {"workload": f"{a.case} {a.nx}x{a.ny} seed {a.seed}", "cells": len(rows), "h": a.h,
            "dp_pa": J0, "base_iterations": n0, "clamped_velocities": nclamp,
-           "adjoint_iterations": rep["iterations"], "adjoint_residual": rep["residual"],
+           "adjoint_iterations": rep["iterations"], "adjoint_residual": rep["residual"], "adjoint_model": rep["model"],
            "max_rel_err": float(rel.max()), "median_rel_err": float(np.median(rel)),
            "max_rel_err_significant": float(rel[sig].max()) if sig.any() else None,
            "significant_cells": int(sig.sum()), "max_err_over_scale": float(max(r["err_over_scale"] for r in rows)),

@@ -354,6 +354,38 @@ __global__ void k_adj_clampmask(KParams k, const double* xs, double maxVel, doub
     }
 }
 
+// part[2 b] = clamped unknowns of block b, part[2 b + 1] = the largest
+// |x_s - x_0| over its unclamped unknowns (U and V): how far the state is
+// from a fixed point of the frozen iteration
+__global__ void k_adj_fixedpoint(KParams k, const double* xsU, const double* u, const double* clampU,
+                                 const double* xsV, const double* v, const double* clampV, double* part) {
+    __shared__ double sm[64];
+    const Dims d = k.d;
+    const int M = d.M, N = d.N;
+    const int nU = (M - 1) * (N - 2), nV = (M - 2) * (N - 1);
+    double cnt = 0.0, mx = 0.0;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nU + nV; t += gridDim.x * blockDim.x) {
+        const bool isU = t < nU;
+        const int q = isU ? t : t - nU;
+        const int w = isU ? N - 2 : N - 1;
+        const size_t c = at(d, 1 + q / w, 1 + q % w);
+        const double cl = (isU ? clampU : clampV)[c];
+        if (cl != 0.0) cnt += 1.0;
+        else mx = dmax(mx, fabs((isU ? xsU : xsV)[c] - (isU ? u : v)[c]));
+    }
+    double a[1] = {cnt};
+    block_sum<1>(a, sm);
+    mx = warp_max(mx);
+    if ((threadIdx.x & 31) == 0) sm[32 + (threadIdx.x >> 5)] = mx;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double m = 0.0;
+        for (int q = 0; q < (int)((blockDim.x + 31) >> 5); ++q) m = dmax(m, sm[32 + q]);
+        part[2 * blockIdx.x] = a[0];
+        part[2 * blockIdx.x + 1] = m;
+    }
+}
+
 // One reverse sweep of the recurrence y_{j+1} = D^-1 (r0 + N y_j) of one
 // component (y_j = x_j - field): with w = ybar / D on the unknowns,
 // r0b += w, the coefficient adjoints eb.. += w y_j(neighbour), db -= w y_{j+1},
@@ -780,6 +812,129 @@ __global__ void k_adj_grad(AdjCtx a, AdjSweep Us, AdjSweep Vs, double alphaMax, 
             if (ca >= 1 && ca <= M - 2) s += abV(at(d, ca, jv));
         }
         grad[t] = -s * 0.5 * dalpha;
+    }
+}
+
+// ---------------------------------------------------------------- equations model
+// The adjoint of the discretisation R(X) = 0 itself: exact at a state with no
+// velocity on the clamp (there the fixed point of the iteration satisfies
+// R = 0, whatever the sweep count), the model for states that are not fixed
+// points of the iteration, and the one whose preconditioner (Jacobi sweeps on
+// the transposed Picard momentum matrix, then the pressure-like correction
+// with the forward pressure matrix) converges robustly.
+
+// Equations model: y = J_R^T lambda (y zeroed by the caller); with resid != nullptr also the
+// residuals R(X) per row (U, V, C in the field layout).
+__global__ void k_adj_jt_eq(AdjCtx a, AdjVecs V, double* rU, double* rV, double* rC) {
+    const Dims d = a.k.d;
+    const int M = d.M, N = d.N;
+    const int nU = (M - 1) * (N - 2), nV = (M - 2) * (N - 1), nC = (M - 1) * (N - 2);
+    const bool scatter = (rU == nullptr);
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nU + nV + nC; t += gridDim.x * blockDim.x) {
+        if (t < nU) {
+            const int i = 1 + t / (N - 2), j = 1 + t % (N - 2);
+            const double R = adj_row_u(a, i, j, scatter ? V.lu[at(d, i, j)] : 0.0, V, scatter);
+            if (!scatter) rU[at(d, i, j)] = R;
+        } else if (t < nU + nV) {
+            const int q = t - nU;
+            const int i = 1 + q / (N - 1), j = 1 + q % (N - 1);
+            const double R = adj_row_v(a, i, j, scatter ? V.lv[at(d, i, j)] : 0.0, V, scatter);
+            if (!scatter) rV[at(d, i, j)] = R;
+        } else {
+            const int q = t - nU - nV;
+            const int i = 1 + q / (N - 2), j = 1 + q % (N - 2);
+            const double R = adj_row_c(a, i, j, scatter ? V.lc[at(d, i, j)] : 0.0, V, scatter);
+            if (!scatter) rC[at(d, i, j)] = R;
+        }
+    }
+}
+
+// Equations model: one Jacobi sweep of the transposed, relaxed Picard momentum system for U
+// and V: (A_P^T x)(i,j) = aP x(i,j) - aW(i,j+1) x(i,j+1) - aE(i,j-1) x(i,j-1)
+// - aS(i+1,j) x(i+1,j) - aN(i-1,j) x(i-1,j) with the masked coefficients of
+// the converged assembly (aP = aP0 / uvAlpha).  first: x = 0.
+__global__ void k_adj_jacobi_t(KParams k, MomSys<double> Us, MomSys<double> Vs, const double* ru,
+                               const double* rv, const double* xu, const double* xv, double* yu, double* yv,
+                               int first) {
+    const Dims d = k.d;
+    const int M = d.M, N = d.N;
+    const int nU = (M - 1) * (N - 2), nV = (M - 2) * (N - 1);
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nU + nV; t += gridDim.x * blockDim.x) {
+        const bool isU = t < nU;
+        const int q = isU ? t : t - nU;
+        const int w = isU ? N - 2 : N - 1;
+        const int i = 1 + q / w, j = 1 + q % w;
+        const size_t c = at(d, i, j);
+        const MomSys<double>& S = isU ? Us : Vs;
+        const double* x = isU ? xu : xv;
+        const double* r = isU ? ru : rv;
+        double Ax = 0.0;
+        if (!first) {
+            Ax = S.aP[c] * x[c] - S.aW[c + 1] * x[c + 1] - S.aE[c - 1] * x[c - 1] - S.aS[c + d.P] * x[c + d.P] -
+                 S.aN[c - d.P] * x[c - d.P];
+        }
+        const double xn = (first ? 0.0 : x[c]) + (r[c] - Ax) / S.aP[c];
+        (isU ? yu : yv)[c] = xn;
+    }
+}
+
+// Equations model, corrections: dm = dm* - D_A^-1 D^T dc with (D_A^-1 D^T dc)_u(i,j) =
+// rho dE(i,j) (dc(i,j+1) - dc(i,j)) and for v rho dN(i,j) (dc(i+1,j) - dc(i,j))
+// (dc zero outside the pressure unknowns); out = (dm, pAlpha dc) on the
+// U / V / continuity unknowns
+__global__ void k_adj_update_eq(KParams k, const double* du, const double* dv, const double* dc, const double* dE,
+                             const double* dN, double relaxC, double* ou, double* ov, double* oc) {
+    const Dims d = k.d;
+    const int M = d.M, N = d.N;
+    const int nU = (M - 1) * (N - 2), nV = (M - 2) * (N - 1), nP = (M - 1) * (N - 2);
+    auto C = [&](int i, int j) -> double {
+        if (i < 1 || i > M - 1 || j < 1 || j > N - 2) return 0.0;
+        return dc[at(d, i, j)];
+    };
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nU + nV + nP; t += gridDim.x * blockDim.x) {
+        if (t < nU) {
+            const int i = 1 + t / (N - 2), j = 1 + t % (N - 2);
+            const size_t c = at(d, i, j);
+            ou[c] = du[c] - k.rho * dE[c] * (C(i, j + 1) - C(i, j));
+        } else if (t < nU + nV) {
+            const int q = t - nU;
+            const int i = 1 + q / (N - 1), j = 1 + q % (N - 1);
+            const size_t c = at(d, i, j);
+            ov[c] = dv[c] - k.rho * dN[c] * (C(i + 1, j) - C(i, j));
+        } else {
+            const int q = t - nU - nV;
+            const int i = 1 + q / (N - 2), j = 1 + q % (N - 2);
+            oc[at(d, i, j)] = relaxC * dc[at(d, i, j)];
+        }
+    }
+}
+
+// Equations model: dJ/dgamma(cell a, b) = -sum over the faces the cell touches of
+// lambda_face * vol * vel_face * 0.5 * alpha'(gamma(a,b)); cells Ny x Nx.
+__global__ void k_adj_grad_eq(AdjCtx a, AdjVecs V, double alphaMax, double q, double* grad) {
+    const KParams& k = a.k;
+    const Dims d = k.d;
+    const int M = d.M, N = d.N, Ny = M - 1, Nx = N - 1;
+    const double vol = k.hx * k.hy;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < Ny * Nx; t += gridDim.x * blockDim.x) {
+        const int ca = t / Nx, cb = t % Nx;
+        const double g = a.gamma[at(d, ca, cb)];
+        const double den = 1.0 + q * g + 1e-10;
+        const double dalpha = -alphaMax * (den + (1.0 - g) * q) / (den * den);
+        double s = 0.0;
+        // U faces (i, j) with i-1 = ca and j-1 = cb (left cell) or j = cb (right cell); j in [1, N-2]
+        const int iu = ca + 1;
+        if (iu >= 1 && iu <= M - 1) {
+            if (cb + 1 <= N - 2) s += V.lu[at(d, iu, cb + 1)] * a.u[at(d, iu, cb + 1)];
+            if (cb >= 1 && cb <= N - 2) s += V.lu[at(d, iu, cb)] * a.u[at(d, iu, cb)];
+        }
+        // V faces (i, j) with j-1 = cb and i-1 = ca (top cell) or i = ca (bottom cell); i in [1, M-2]
+        const int jv = cb + 1;
+        if (jv >= 1 && jv <= N - 1) {
+            if (ca + 1 <= M - 2) s += V.lv[at(d, ca + 1, jv)] * a.v[at(d, ca + 1, jv)];
+            if (ca >= 1 && ca <= M - 2) s += V.lv[at(d, ca, jv)] * a.v[at(d, ca, jv)];
+        }
+        grad[t] = -s * vol * 0.5 * dalpha;
     }
 }
 

@@ -56,7 +56,14 @@ struct SaHier {
     TV* Y[9];               // coloured probes A P e_c (level-0 sized)
     TV* dense;              // inverse of the coarsest operator
     double omega, w0, wc;   // Jacobi damping, prolongator smoothing weights
+    unsigned long long* prof;  // optional per-phase device time (ns, block 0's view), or null
 };
+
+// profile slots: set-up, Galerkin, CG matvec, CG update, CTA levels, then
+// restriction out of level l at SA_P_DOWN + l and prolongation into level l
+// at SA_P_UP + l
+enum SaPhase { SA_P_SETUP = 0, SA_P_GALERKIN, SA_P_MATVEC, SA_P_UPDATE, SA_P_CTA, SA_P_DOWN, SA_P_UP = SA_P_DOWN + kSaMaxLevels,
+               SA_P_COUNT = SA_P_UP + kSaMaxLevels };
 
 __host__ __device__ __forceinline__ int sa_coarse(int n) { return (n + 2) / 3; }
 
@@ -333,6 +340,14 @@ __global__ void __launch_bounds__(512, 1) k_pcg_sa(KParams k, Status* st, const 
 
     SaLevel<TV> L0 = H.lv[0];
     L0.b = B.r;
+    unsigned long long tp = (H.prof && blockIdx.x == 0 && threadIdx.x == 0) ? globaltimer_ns() : 0ull;
+    auto tick = [&](int ph) {
+        if (H.prof && blockIdx.x == 0 && threadIdx.x == 0) {
+            const unsigned long long t = globaltimer_ns();
+            atomicAdd(H.prof + ph, t - tp);
+            tp = t;
+        }
+    };
     const Stencil5<TV> A0{B.fE, B.fN, B.d, M - 1, w, d.P};
     auto stencil = [&](int l) { return Stencil9<TV>{H.lv[l].c, H.lv[l].nI, H.lv[l].nJ, H.lv[l].P}; };
     auto lvl = [&](int l) -> const SaLevel<TV>& { return l == 0 ? L0 : H.lv[l]; };
@@ -364,6 +379,7 @@ __global__ void __launch_bounds__(512, 1) k_pcg_sa(KParams k, Status* st, const 
     double bnorm2[1];
     sum_partials<1>(partA, G, 1, bnorm2, sm);
     const double rTol = k.pTol * sqrt(bnorm2[0]);
+    tick(SA_P_SETUP);
 
     // ---- set-up: coarse operators by coloured probes
     for (int l = 0; l < H.L - 1; ++l) {
@@ -383,6 +399,7 @@ __global__ void __launch_bounds__(512, 1) k_pcg_sa(KParams k, Status* st, const 
     }
     if (blockIdx.x == 0) sa_dense_setup(H.lv[H.L - 1], H.dense, dsm);
     SA_SYNC();
+    tick(SA_P_GALERKIN);
 
     // one restriction l -> l+1 (two passes) and one prolongation l+1 -> l
     // with post-smoothing (two passes), on the grid or on CTA 0
@@ -421,8 +438,10 @@ __global__ void __launch_bounds__(512, 1) k_pcg_sa(KParams k, Status* st, const 
     };
     // ---- z = M r (V-cycle); z in level 0's y, rz = r.z
     auto vcycle = [&](double& rz) -> bool {
-        for (int l = 0; l < H.Lg; ++l)
+        for (int l = 0; l < H.Lg; ++l) {
             if (!restrict_level(l, true)) return false;
+            tick(SA_P_DOWN + l);
+        }
         if (blockIdx.x == 0) {
             for (int l = H.Lg; l < H.L - 1; ++l) restrict_level(l, false);
             sa_dense_solve(H.lv[H.L - 1], H.dense);
@@ -430,8 +449,11 @@ __global__ void __launch_bounds__(512, 1) k_pcg_sa(KParams k, Status* st, const 
         }
         target += G;
         if (!grid_barrier(bar, target, &st->err)) return false;
-        for (int l = H.Lg - 1; l >= 0; --l)
+        tick(SA_P_CTA);
+        for (int l = H.Lg - 1; l >= 0; --l) {
             if (!prolong_level(l, true, l == 0 ? &rz : nullptr)) return false;
+            tick(SA_P_UP + l);
+        }
         double t2[2];
         sum_partials<2>(partB, G, 2, t2, sm);
         rz = t2[1];
@@ -469,6 +491,7 @@ __global__ void __launch_bounds__(512, 1) k_pcg_sa(KParams k, Status* st, const 
         SA_SYNC();
         double pAp[1];
         sum_partials<1>(partA, G, 1, pAp, sm);
+        tick(SA_P_MATVEC);
         if (fabs(pAp[0]) < 1e-20) break;
         const double alpha = rz / pAp[0];
         const TV al = (TV)alpha, omT = (TV)om;
@@ -486,6 +509,7 @@ __global__ void __launch_bounds__(512, 1) k_pcg_sa(KParams k, Status* st, const 
         SA_SYNC();
         double tB[2];
         sum_partials<2>(partB, G, 2, tB, sm);
+        tick(SA_P_UPDATE);
         if (sqrt(tB[0]) <= rTol) { ++it; break; }
         double rzn = 0.0;
         if (!vcycle(rzn)) return;

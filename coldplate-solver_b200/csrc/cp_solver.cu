@@ -115,6 +115,7 @@ struct cp_ctx {
     void* saY[9] = {};
     void* saDense = nullptr;
     double saOmega = 0.9, saW0 = 2.0 / 3.0, saWc = 0.8;
+    unsigned long long* saProf = nullptr;    // per-phase timers when CP_SA_PROFILE is set
     MgMaps mgMaps;                           // TMA tensor maps of the level-0 tile phases
     // adjoint buffers (allocated on first use, double)
     double* adj[40] = {};
@@ -131,6 +132,7 @@ struct cp_ctx {
     double* adjKryPart = nullptr;
     double* adjH = nullptr;
     int adjRestart = 30;     // m
+    int adjSweeps = 6;       // equations model: transposed momentum Jacobi sweeps per preconditioner application
     int adjPIters = 6;       // multigrid-PCG iterations per preconditioner application
     cudaGraphExec_t graph = nullptr;
     bool graphTried = false;
@@ -474,6 +476,7 @@ SaHier<TV> sa_hier(cp_ctx* c) {
     H.w0 = c->saW0;
     H.wc = c->saWc;
     H.dense = (TV*)c->saDense;
+    H.prof = c->saProf;
     for (int q = 0; q < 9; ++q) H.Y[q] = (TV*)c->saY[q];
     for (int l = 0; l < c->saL; ++l) {
         SaLevel<TV>& v = H.lv[l];
@@ -524,6 +527,7 @@ cp_status sa_build(cp_ctx* c) {
     if (const char* e = getenv("CP_SA_OMEGA")) c->saOmega = atof(e);
     if (const char* e = getenv("CP_SA_W0")) c->saW0 = atof(e);
     if (const char* e = getenv("CP_SA_WC")) c->saWc = atof(e);
+    if (getenv("CP_SA_PROFILE") && (s = dalloc(c, &c->saProf, (size_t)SA_P_COUNT)) != CP_OK) return s;
     int nb = 0;
     if (c->prm.precision == CP_PREC_MIXED) {
         cudaFuncSetAttribute(k_pcg_sa<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSaDynSmem);
@@ -811,6 +815,7 @@ void cp_params_default(cp_params* p) {
     p->precision = CP_PREC_FP64;
     p->historyCapacity = 0;   // 0: maxIterations rows
     p->chunk = 32;
+    p->adjointModel = CP_ADJ_AUTO;
 }
 
 cp_status cp_read_fluid_params(const char* path, cp_params* p) {
@@ -912,6 +917,18 @@ cp_status cp_create(const cp_params* prm, cp_ctx** out) {
 cp_status cp_destroy(cp_ctx* c) {
     if (!c) return CP_OK;
     if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->saProf) {
+        // CP_SA_PROFILE: device time per phase of the smoothed-aggregation PCG,
+        // summed over the context's life (block 0's clock after each barrier)
+        unsigned long long t[SA_P_COUNT];
+        if (cudaMemcpy(t, c->saProf, sizeof t, cudaMemcpyDeviceToHost) == cudaSuccess) {
+            fprintf(stderr, "CP_SA_PROFILE ms: setup %.3f galerkin %.3f matvec %.3f update %.3f cta %.3f", t[SA_P_SETUP] * 1e-6,
+                    t[SA_P_GALERKIN] * 1e-6, t[SA_P_MATVEC] * 1e-6, t[SA_P_UPDATE] * 1e-6, t[SA_P_CTA] * 1e-6);
+            for (int l = 0; l < c->saLg; ++l) fprintf(stderr, " down%d %.3f", l, t[SA_P_DOWN + l] * 1e-6);
+            for (int l = 0; l < c->saLg; ++l) fprintf(stderr, " up%d %.3f", l, t[SA_P_UP + l] * 1e-6);
+            fprintf(stderr, " levels %d grid %d\n", c->saL, c->saLg);
+        }
+    }
     if (c->graph) cudaGraphExecDestroy(c->graph);
     for (void* q : c->allocs) cudaFree(q);
     if (c->stHost) cudaFreeHost(c->stHost);
@@ -1154,6 +1171,7 @@ cp_status adjoint_alloc(cp_ctx* c) {
     if ((s = dalloc(c, &c->adjBar, 1)) != CP_OK) return s;
     if (const char* e = getenv("CP_ADJ_RESTART")) c->adjRestart = std::min(std::max(atoi(e), 1), kKryMaxDots - 1);
     if (const char* e = getenv("CP_ADJ_PITERS")) c->adjPIters = std::max(atoi(e), 1);
+    if (const char* e = getenv("CP_ADJ_SWEEPS")) c->adjSweeps = std::max(atoi(e), 1);
     if (!c->useMg) c->adjPIters = std::max(c->adjPIters, 100);
     const size_t L = 3 * c->nElem;
     if ((s = dalloc(c, &c->adjKry, (size_t)(2 * c->adjRestart + 3) * L)) != CP_OK) return s;
@@ -1290,8 +1308,32 @@ extern "C" cp_status cp_adjoint_dp_dgamma(cp_ctx* c, double* grad, long rows, lo
     CK(cudaGetLastError());
     AdjSweep UsA{Us.aP, Us.aE, Us.aW, Us.aN, Us.aS, clampU, A[20], A[21], A[22], A[23], A[24], A[25]};
     AdjSweep VsA{Vs.aP, Vs.aE, Vs.aW, Vs.aN, Vs.aS, clampV, A[26], A[27], A[28], A[29], A[30], A[31]};
-    k_adj_prec_faces<<<nb, kThreads, 0, c->stream>>>(k, c->dE, c->dN, UsA, VsA, dEp, dNp);
-    CK(cudaGetLastError());
+    // which model: the fixed point of the frozen iteration where the state is
+    // one (every unclamped sweep result equals the state to 1e-7 maxVel) and
+    // velocities sit on the clamp; the equations R = 0 otherwise (exact
+    // without clamped velocities, and the only meaningful linearisation away
+    // from a fixed point)
+    int nClamped = 0;
+    double fpRes = 0.0;
+    {
+        k_adj_fixedpoint<<<nb, kThreads, 0, c->stream>>>(k, c->adjXU[sU - 1], c->u, clampU, c->adjXV[sV - 1], c->v,
+                                                          clampV, c->adjPart);
+        CK(cudaGetLastError());
+        std::vector<double> pf((size_t)2 * nb);
+        CK(cudaMemcpyAsync(pf.data(), c->adjPart, pf.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        double cnt = 0.0;
+        for (int b = 0; b < nb; ++b) { cnt += pf[2 * b]; fpRes = std::max(fpRes, pf[2 * b + 1]); }
+        nClamped = (int)cnt;
+    }
+    int model = c->prm.adjointModel;
+    if (model != CP_ADJ_EQUATIONS && model != CP_ADJ_FIXED_POINT)
+        model = (nClamped > 0 && fpRes <= 1e-7 * ac.maxVel) ? CP_ADJ_FIXED_POINT : CP_ADJ_EQUATIONS;
+    const bool fixedPoint = model == CP_ADJ_FIXED_POINT;
+    if (fixedPoint) {
+        k_adj_prec_faces<<<nb, kThreads, 0, c->stream>>>(k, c->dE, c->dN, UsA, VsA, dEp, dNp);
+        CK(cudaGetLastError());
+    }
     // right-hand side dJ/dX and J
     k_adj_g<<<1, 1024, 0, c->stream>>>(ac, V, Jd);
     CK(cudaGetLastError());
@@ -1336,10 +1378,13 @@ extern "C" cp_status cp_adjoint_dp_dgamma(cp_ctx* c, double* grad, long rows, lo
     auto product = [&](const double* x, double gs, double ys, double* out, double* rr, double* gg) -> cp_status {
         AdjVecs Vx = V;
         Vx.lu = const_cast<double*>(x); Vx.lv = Vx.lu + c->nElem; Vx.lc = Vx.lu + 2 * c->nElem;
-        cp_status s1 = reverse(x);
-        if (s1 != CP_OK) return s1;
+        if (fixedPoint) {
+            cp_status s1 = reverse(x);
+            if (s1 != CP_OK) return s1;
+        }
         for (double* y : {V.yu, V.yv, V.yp}) CK(cudaMemsetAsync(y, 0, bytes, c->stream));
-        k_adj_jt<<<nb, kThreads, 0, c->stream>>>(ac, Vx, UsA, VsA);
+        if (fixedPoint) k_adj_jt<<<nb, kThreads, 0, c->stream>>>(ac, Vx, UsA, VsA);
+        else k_adj_jt_eq<<<nb, kThreads, 0, c->stream>>>(ac, Vx, nullptr, nullptr, nullptr);
         CK(cudaGetLastError());
         k_adj_defect<<<nb, kThreads, 0, c->stream>>>(k, V, gs, ys, out, out + c->nElem, out + 2 * c->nElem,
                                                      c->adjPart);
@@ -1356,7 +1401,32 @@ extern "C" cp_status cp_adjoint_dp_dgamma(cp_ctx* c, double* grad, long rows, lo
         return CP_OK;
     };
     // z = P^-1 r: the momentum part, then the pressure-like correction
+    // the equations model: Jacobi sweeps on the transposed Picard momentum
+    // system, then the pressure-like correction with the forward matrix
+    auto precondition_eq = [&](const double* r, double* z) -> cp_status {
+        const double *ru = r, *rv = r + c->nElem, *rp = r + 2 * c->nElem;
+        double *xu = V.du, *xv = V.dv;
+        double *yu = V.eu, *yv = V.ev;
+        for (int q = 0; q < c->adjSweeps; ++q) {
+            k_adj_jacobi_t<<<nb, kThreads, 0, c->stream>>>(k, Us, Vs, ru, rv, xu, xv, yu, yv, q == 0);
+            CK(cudaGetLastError());
+            std::swap(xu, yu);
+            std::swap(xv, yv);
+        }
+        cp_status s2 = c->prm.precision == CP_PREC_MIXED ? adjoint_prhs<float>(c, kp, xu, xv, rp)
+                                                         : adjoint_prhs<double>(c, kp, xu, xv, rp);
+        if (s2 != CP_OK) return s2;
+        CK(cudaMemsetAsync(c->adjSt, 0, sizeof(Status), c->stream));
+        s2 = c->prm.precision == CP_PREC_MIXED ? adjoint_pcg<float>(c, kp, c->dE, c->dN, dc)
+                                               : adjoint_pcg<double>(c, kp, c->dE, c->dN, dc);
+        if (s2 != CP_OK) return s2;
+        k_adj_update_eq<<<nb, kThreads, 0, c->stream>>>(k, xu, xv, dc, c->dE, c->dN, c->prm.pAlpha, z,
+                                                        z + c->nElem, z + 2 * c->nElem);
+        CK(cudaGetLastError());
+        return CP_OK;
+    };
     auto precondition = [&](const double* r, double* z) -> cp_status {
+        if (!fixedPoint) return precondition_eq(r, z);
         const double *ru = r, *rv = r + c->nElem, *rp = r + 2 * c->nElem;
         k_adj_prec_mom<<<nb, kThreads, 0, c->stream>>>(k, ru, rv, UsA, VsA, V.du, V.dv, V.eu, V.ev);
         CK(cudaGetLastError());
@@ -1457,11 +1527,16 @@ extern "C" cp_status cp_adjoint_dp_dgamma(cp_ctx* c, double* grad, long rows, lo
         beta = std::sqrt(rr);
         res = gnorm > 0.0 ? beta / gnorm : 0.0;
     }
-    // gradient on the Ny x Nx cells from the reverse sweeps of lambda
-    if ((s = reverse(LAM)) != CP_OK) return s;
+    // gradient on the Ny x Nx cells (fixed point: from the reverse sweeps of
+    // lambda)
     double* gd = A[18];
     const double amax = c->prm.eta / std::max(c->prm.brinkmanKMin, 1e-20);
-    k_adj_grad<<<nb, kThreads, 0, c->stream>>>(ac, UsA, VsA, amax, c->prm.brinkmanQ, gd);
+    if (fixedPoint) {
+        if ((s = reverse(LAM)) != CP_OK) return s;
+        k_adj_grad<<<nb, kThreads, 0, c->stream>>>(ac, UsA, VsA, amax, c->prm.brinkmanQ, gd);
+    } else {
+        k_adj_grad_eq<<<nb, kThreads, 0, c->stream>>>(ac, V, amax, c->prm.brinkmanQ, gd);
+    }
     CK(cudaGetLastError());
     CK(cudaEventRecord(c->ev1, c->stream));
     std::vector<double> g((size_t)(M - 1) * (N - 1));
@@ -1482,6 +1557,8 @@ extern "C" cp_status cp_adjoint_dp_dgamma(cp_ctx* c, double* grad, long rows, lo
         rep->residual = res;
         rep->J = Jh;
         rep->device_ms = ms;
+        rep->model = model;
+        rep->clampedUnknowns = nClamped;
     }
     return CP_OK;
 }

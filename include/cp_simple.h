@@ -91,7 +91,8 @@ typedef struct cp_params {
     /* pressure solver (SIMPLE.h:145-156): type 1 runs the reference's
      * Jacobi-preconditioned CG (pressure_solver.cpp:121-184); types 2 and 4
      * (AMGCL AMG-CG in the reference; 4 is its default) run CG preconditioned
-     * by an aggregation-multigrid V-cycle; 0 (SOR) and 3 (LDLT) are
+     * by a multigrid V-cycle: smoothed aggregation for 4, 2 x 2 aggregation
+     * for 2 (and for every field of a batch); 0 (SOR) and 3 (LDLT) are
      * CP_ERR_UNSUPPORTED */
     int pressureSolverType;
     int parallelizeDirectSolver;
@@ -139,6 +140,7 @@ typedef struct cp_params {
     int precision;                  /* cp_precision                           */
     int historyCapacity;            /* rows of per-iteration history kept     */
     int chunk;                      /* outer iterations between host polls    */
+    int adjointModel;               /* cp_adjoint_model of cp_adjoint_dp_dgamma */
 } cp_params;
 
 /* Per-iteration record (one row of the history, see cp_get_history). */
@@ -248,17 +250,29 @@ cp_status cp_pressure_noalloc(const cp_params* p, const double* dE, const double
  * current state (run the forward solve to convergence first).  New: the
  * reference has no flow adjoint.  grad receives dJ/dgamma for the Ny x Nx
  * cells (strides in elements).  The adjoint equations J_X^T lambda = dJ/dX
- * of the converged discretisation are solved by defect correction with a
- * transposed-SIMPLE preconditioner (transposed momentum Jacobi sweeps and a
- * PCG solve of the pressure-like block, whose matrix is the forward pressure
- * matrix); iteration stops when
- * ||dJ/dX - J_X^T lambda|| <= tol ||dJ/dX|| or after max_iter. */
+ * are solved by restarted flexible GMRES(30) with a transposed-SIMPLE
+ * preconditioner; iteration stops when ||dJ/dX - J_X^T lambda|| <= tol
+ * ||dJ/dX|| or after max_iter.  cp_params.adjointModel selects what is
+ * differentiated (cp_adjoint_model); the report says which model ran. */
+typedef enum cp_adjoint_model {
+    CP_ADJ_AUTO = 0,         /* FIXED_POINT where the state is a fixed point of the
+                                iteration with velocities on the clamp, else
+                                EQUATIONS                                          */
+    CP_ADJ_EQUATIONS = 1,    /* the discretisation R(X) = 0: exact with no velocity
+                                on the clamp (R = 0 holds there at a fixed point)  */
+    CP_ADJ_FIXED_POINT = 2   /* the iteration's fixed point with the Jacobi sweep
+                                count and the clamped unknowns frozen: the momentum
+                                rows are s Jacobi sweeps from u (their result must
+                                equal u), clamped unknowns stay at +-maxVel        */
+} cp_adjoint_model;
 typedef struct cp_adjoint_report {
-    int iterations;        /* defect-correction iterations run          */
+    int iterations;        /* FGMRES iterations run                     */
     int converged;         /* 1 if the relative residual reached tol    */
     double residual;       /* final relative residual                   */
     double J;              /* pressure drop evaluated at the state [Pa] */
     double device_ms;      /* device time of the adjoint (CUDA events)  */
+    int model;             /* cp_adjoint_model used (EQUATIONS or FIXED_POINT) */
+    int clampedUnknowns;   /* velocity unknowns the scatter clamps at the state */
 } cp_adjoint_report;
 cp_status cp_adjoint_dp_dgamma(cp_ctx* ctx, double* grad, long rows, long cols, long row_stride,
                                long col_stride, int max_iter, double tol, cp_adjoint_report* rep);

@@ -53,12 +53,19 @@ def _logs_of(g) -> tuple[np.ndarray, np.ndarray]:
                 np.loadtxt(os.path.join(d, "pressure_drop_history.txt"), comments=("#", "I", "i"), ndmin=2))
 
 
+def _as_float32(prm: dict) -> dict:
+    """The parameters as the reference's float build holds them (its members
+    are float): the drop-in passes those values on, so the Python path runs
+    with the same ones."""
+    return {k: float(np.float32(v)) if isinstance(v, float) else v for k, v in prm.items()}
+
+
 def test_reference_loop_over_the_library_matches_the_python_path():
     from coldplate_b200 import Simple
     case = window_cases()["density"]
     prm = case.params(maxIterations=60, epsilon=1e-30, usePressureDropConvergence=0)
     res_d, dp_d = _run_dropin(case, prm)
-    with Simple(cellType=case.cellType, **prm) as g:
+    with Simple(cellType=case.cellType, **_as_float32(prm)) as g:
         g.step(60)
         res_p, dp_p = _logs_of(g)
     assert res_d.shape == res_p.shape == (60, res_p.shape[1]), (res_d.shape, res_p.shape)
