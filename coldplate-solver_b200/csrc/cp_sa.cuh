@@ -56,6 +56,10 @@ struct SaHier {
     TV* Y[9];               // coloured probes A P e_c (level-0 sized)
     TV* dense;              // inverse of the coarsest operator
     double omega, w0, wc;   // Jacobi damping, prolongator smoothing weights
+    TV* r2;                 // second CG residual buffer (the residual ping-pongs)
+    int reuse;              // rebuild the coarse operators every `reuse` outer iterations
+    int force;              // 1: rebuild now and leave the hierarchy marked stale
+    int* dirty;             // device flag: the stored hierarchy is not the forward's
     unsigned long long* prof;  // optional per-phase device time (ns, block 0's view), or null
 };
 
@@ -314,6 +318,111 @@ __device__ void sa_dense_solve(const SaLevel<TV>& l, const TV* inv) {
     __syncthreads();
 }
 
+// ---------------------------------------------------------------- level-0 passes
+// Level 0 has the 5-point operator of the face coefficients fE (east), fN
+// (north) and the diagonal d.  Its arrays are zero on the frame (only the
+// unknowns are ever written), and fE / fN are zero on the frame rows and
+// columns, so these passes read neighbours without range checks wherever a
+// zero frame value gives the right term.  Arithmetic in TV.
+template <typename TV>
+struct Sa0 {
+    const TV *fE, *fN, *d;
+    int nI, nJ, P;
+};
+
+// CG matvec on p = z + beta p_old: writes p and Ap, returns p.Ap's share
+template <typename TV>
+__device__ __forceinline__ double sa0_matvec(const Sa0<TV>& A, const TV* z, const TV* pold, TV bt, bool first,
+                                             TV* pnew, TV* Ap, int i, int j) {
+    const int c = i * A.P + j;
+    auto dir = [&](int q) -> TV { return first ? z[q] : (TV)(z[q] + bt * pold[q]); };
+    const TV pc = dir(c);
+    const TV ap = A.d[c] * pc - A.fE[c] * dir(c + 1) - A.fE[c - 1] * dir(c - 1) - A.fN[c] * dir(c + A.P) -
+                  A.fN[c - A.P] * dir(c - A.P);
+    pnew[c] = pc;
+    Ap[c] = ap;
+    return (double)pc * (double)ap;
+}
+
+// CG update fused with the first half of the next restriction:
+// x += alpha p, r' = r - alpha Ap (into rn), x0' = omega r' / d (the
+// pre-smoothed level-0 iterate), and the residual of the pre-smoothing
+// t = r' - A x0' = (1 - omega) r' + sum of the faces' f x0'(neighbour), with
+// x0' of the neighbours recomputed from r and Ap; y = t / d.  Returns |r'|^2.
+template <typename TV>
+__device__ __forceinline__ double sa0_update(const Sa0<TV>& A, TV al, TV om, const TV* p, const TV* Ap, TV* x,
+                                             const TV* r, TV* rn, TV* x0, TV* t, TV* y, int i, int j) {
+    const int c = i * A.P + j;
+    auto x0n = [&](int q) -> TV { return om * (r[q] - al * Ap[q]) / A.d[q]; };
+    const TV rc = r[c] - al * Ap[c];
+    x[c] = x[c] + al * p[c];
+    rn[c] = rc;
+    x0[c] = om * rc / A.d[c];
+    TV r1 = ((TV)1 - om) * rc;
+    if (j < A.nJ) r1 += A.fE[c] * x0n(c + 1);
+    if (j > 1) r1 += A.fE[c - 1] * x0n(c - 1);
+    if (i < A.nI) r1 += A.fN[c] * x0n(c + A.P);
+    if (i > 1) r1 += A.fN[c - A.P] * x0n(c - A.P);
+    t[c] = r1;
+    y[c] = r1 / A.d[c];
+    return (double)rc * (double)rc;
+}
+
+// the same residual half for the first cycle (x0 stored already)
+template <typename TV>
+__device__ __forceinline__ void sa0_resid(const Sa0<TV>& A, TV om, const TV* b, const TV* x0, TV* t, TV* y, int i,
+                                          int j) {
+    const int c = i * A.P + j;
+    const TV r1 = ((TV)1 - om) * b[c] + A.fE[c] * x0[c + 1] + A.fE[c - 1] * x0[c - 1] + A.fN[c] * x0[c + A.P] +
+                  A.fN[c - A.P] * x0[c - A.P];
+    t[c] = r1;
+    y[c] = r1 / A.d[c];
+}
+
+// second half of the restriction into level 1, one aggregate:
+// b_c = sum over the aggregate of t - w A y, x_c = omega b_c / d_c
+template <typename TV>
+__device__ __forceinline__ void sa0_restrict(const Sa0<TV>& A, const TV* t, const TV* y, const SaLevel<TV>& C,
+                                             TV w, double omega, int I, int J) {
+    double s = 0.0;
+    const int i1 = min(3 * I, A.nI), j1 = min(3 * J, A.nJ);
+    for (int i = 3 * I - 2; i <= i1; ++i)
+        for (int j = 3 * J - 2; j <= j1; ++j) {
+            const int c = i * A.P + j;
+            const TV ay = A.d[c] * y[c] - A.fE[c] * y[c + 1] - A.fE[c - 1] * y[c - 1] - A.fN[c] * y[c + A.P] -
+                          A.fN[c - A.P] * y[c - A.P];
+            s += (double)(t[c] - w * ay);
+        }
+    const int qc = I * C.P + J;
+    C.b[qc] = (TV)s;
+    C.x[qc] = (TV)(omega * s / (double)C.c[4][qc]);
+}
+
+// prolongation from level 1 fused with the post-smoothing of level 0:
+// t = x0 + P e at the cell and its four neighbours ((P e)(m) = e(agg m) -
+// w / d_m (A e0)(m)), then y = t + omega (b - A t) / d.  Returns y.
+template <typename TV>
+__device__ __forceinline__ TV sa0_prolong(const Sa0<TV>& A, const TV* x0, const TV* b, const TV* e, int Pc, TV w,
+                                          TV om, int i, int j) {
+    auto E0 = [&](int ii, int jj) -> TV {
+        if (ii < 1 || ii > A.nI || jj < 1 || jj > A.nJ) return (TV)0;
+        return e[((ii - 1) / 3 + 1) * Pc + (jj - 1) / 3 + 1];
+    };
+    auto T = [&](int ii, int jj) -> TV {
+        if (ii < 1 || ii > A.nI || jj < 1 || jj > A.nJ) return (TV)0;
+        const int q = ii * A.P + jj;
+        const TV ec = E0(ii, jj);
+        const TV ae = A.d[q] * ec - A.fE[q] * E0(ii, jj + 1) - A.fE[q - 1] * E0(ii, jj - 1) -
+                      A.fN[q] * E0(ii + 1, jj) - A.fN[q - A.P] * E0(ii - 1, jj);
+        return x0[q] + ec - w * ae / A.d[q];
+    };
+    const int c = i * A.P + j;
+    const TV tc = T(i, j);
+    const TV at = A.d[c] * tc - A.fE[c] * T(i, j + 1) - A.fE[c - 1] * T(i, j - 1) - A.fN[c] * T(i + 1, j) -
+                  A.fN[c - A.P] * T(i - 1, j);
+    return tc + om * (b[c] - at) / A.d[c];
+}
+
 // ---------------------------------------------------------------- the solver
 template <typename TV>
 __global__ void __launch_bounds__(512, 1) k_pcg_sa(KParams k, Status* st, const double* dE, const double* dN,
@@ -329,6 +438,7 @@ __global__ void __launch_bounds__(512, 1) k_pcg_sa(KParams k, Status* st, const 
     const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = G * blockDim.x;
     const SaSplit all{tid, nth}, cta{(int)threadIdx.x, (int)blockDim.x};
     const double rho = k.rho, hx = k.hx, hy = k.hy, om = H.omega;
+    const TV omT = (TV)om, w0T = (TV)H.w0;
     unsigned target = 0;
     double* partA = part;
     double* partB = part + G;
@@ -337,9 +447,17 @@ __global__ void __launch_bounds__(512, 1) k_pcg_sa(KParams k, Status* st, const 
         target += G;                                                \
         if (!grid_barrier(bar, target, &st->err)) return;           \
     } while (0)
+    // the coarse operators are rebuilt every H.reuse outer iterations (they
+    // only precondition: the CG matvec always uses the current level 0), and
+    // whenever the stored ones are not the forward's
+    const bool rebuild = H.force || *(volatile int*)H.dirty || H.reuse <= 1 || (st->iter % H.reuse) == 0;
 
     SaLevel<TV> L0 = H.lv[0];
     L0.b = B.r;
+    const Sa0<TV> A0f{B.fE, B.fN, B.d, M - 1, w, d.P};
+    const Stencil5<TV> A0{B.fE, B.fN, B.d, M - 1, w, d.P};
+    auto stencil = [&](int l) { return Stencil9<TV>{H.lv[l].c, H.lv[l].nI, H.lv[l].nJ, H.lv[l].P}; };
+    auto wgt = [&](int l) { return l == 0 ? H.w0 : H.wc; };
     unsigned long long tp = (H.prof && blockIdx.x == 0 && threadIdx.x == 0) ? globaltimer_ns() : 0ull;
     auto tick = [&](int ph) {
         if (H.prof && blockIdx.x == 0 && threadIdx.x == 0) {
@@ -348,16 +466,13 @@ __global__ void __launch_bounds__(512, 1) k_pcg_sa(KParams k, Status* st, const 
             tp = t;
         }
     };
-    const Stencil5<TV> A0{B.fE, B.fN, B.d, M - 1, w, d.P};
-    auto stencil = [&](int l) { return Stencil9<TV>{H.lv[l].c, H.lv[l].nI, H.lv[l].nJ, H.lv[l].P}; };
-    auto lvl = [&](int l) -> const SaLevel<TV>& { return l == 0 ? L0 : H.lv[l]; };
-    auto wgt = [&](int l) { return l == 0 ? H.w0 : H.wc; };
 
-    // ---- set-up: level-0 operator (the reference's formulas), x = 0, r = b
+    // ---- set-up: level-0 operator (the reference's formulas), x = 0, r = b,
+    // x0 = omega r / d
     double bb[1] = {0.0};
     for (int t = tid; t < n; t += nth) {
         const int i = 1 + t / w, j = 1 + t % w;
-        const size_t c = at(d, i, j);
+        const int c = i * d.P + j;
         const double aE = rho * dE[c] * hy;
         const double aW = (j > 1) ? rho * dE[c - 1] * hy : 0.0;
         const double aN = (i < M - 1) ? rho * dN[c] * hx : 0.0;
@@ -381,111 +496,113 @@ __global__ void __launch_bounds__(512, 1) k_pcg_sa(KParams k, Status* st, const 
     const double rTol = k.pTol * sqrt(bnorm2[0]);
     tick(SA_P_SETUP);
 
-    // ---- set-up: coarse operators by coloured probes
-    for (int l = 0; l < H.L - 1; ++l) {
-        const bool grid = l < H.Lg;
-        if (!grid && blockIdx.x != 0) continue;
-        const SaSplit sp = grid ? all : cta;
-        const SaLevel<TV>& f = lvl(l);
-        if (l == 0) sa_cells(sp, f.nI, f.nJ, [&](int i, int j) { sa_probe_cell(A0, f.P, H.Y, wgt(l), i, j); });
-        else sa_cells(sp, f.nI, f.nJ, [&](int i, int j) { sa_probe_cell(stencil(l), f.P, H.Y, wgt(l), i, j); });
-        if (grid) SA_SYNC(); else __syncthreads();
-        const SaLevel<TV>& C = H.lv[l + 1];
-        if (l == 0)
-            sa_cells(sp, C.nI, C.nJ, [&](int I, int J) { sa_galerkin_cell(A0, f.P, H.Y, C, wgt(l), I, J); });
-        else
-            sa_cells(sp, C.nI, C.nJ, [&](int I, int J) { sa_galerkin_cell(stencil(l), f.P, H.Y, C, wgt(l), I, J); });
-        if (grid) SA_SYNC(); else __syncthreads();
+    // ---- set-up: coarse operators by coloured probes (when rebuilt)
+    if (rebuild) {
+        for (int l = 0; l < H.L - 1; ++l) {
+            const bool grid = l < H.Lg;
+            if (!grid && blockIdx.x != 0) continue;
+            const SaSplit sp = grid ? all : cta;
+            const SaLevel<TV>& f = H.lv[l];
+            if (l == 0) sa_cells(sp, f.nI, f.nJ, [&](int i, int j) { sa_probe_cell(A0, f.P, H.Y, wgt(l), i, j); });
+            else sa_cells(sp, f.nI, f.nJ, [&](int i, int j) { sa_probe_cell(stencil(l), f.P, H.Y, wgt(l), i, j); });
+            if (grid) SA_SYNC(); else __syncthreads();
+            const SaLevel<TV>& C = H.lv[l + 1];
+            if (l == 0)
+                sa_cells(sp, C.nI, C.nJ, [&](int I, int J) { sa_galerkin_cell(A0, f.P, H.Y, C, wgt(l), I, J); });
+            else
+                sa_cells(sp, C.nI, C.nJ,
+                         [&](int I, int J) { sa_galerkin_cell(stencil(l), f.P, H.Y, C, wgt(l), I, J); });
+            if (grid) SA_SYNC(); else __syncthreads();
+        }
+        if (blockIdx.x == 0) sa_dense_setup(H.lv[H.L - 1], H.dense, dsm);
+        SA_SYNC();
     }
-    if (blockIdx.x == 0) sa_dense_setup(H.lv[H.L - 1], H.dense, dsm);
-    SA_SYNC();
     tick(SA_P_GALERKIN);
 
-    // one restriction l -> l+1 (two passes) and one prolongation l+1 -> l
-    // with post-smoothing (two passes), on the grid or on CTA 0
+    // levels >= 1: restriction l -> l+1 and prolongation l+1 -> l with
+    // post-smoothing, two passes each, on the grid or on CTA 0
     auto restrict_level = [&](int l, bool grid) -> bool {
         const SaSplit sp = grid ? all : cta;
-        const SaLevel<TV>& f = lvl(l);
+        const SaLevel<TV>& f = H.lv[l];
         const SaLevel<TV>& C = H.lv[l + 1];
-        if (l == 0) sa_cells(sp, f.nI, f.nJ, [&](int i, int j) { sa_resid_cell(A0, f, i, j); });
-        else sa_cells(sp, f.nI, f.nJ, [&](int i, int j) { sa_resid_cell(stencil(l), f, i, j); });
+        sa_cells(sp, f.nI, f.nJ, [&](int i, int j) { sa_resid_cell(stencil(l), f, i, j); });
         if (grid) { target += G; if (!grid_barrier(bar, target, &st->err)) return false; } else __syncthreads();
-        if (l == 0) sa_cells(sp, C.nI, C.nJ, [&](int I, int J) { sa_restrict_cell(A0, f, C, wgt(l), om, I, J); });
-        else sa_cells(sp, C.nI, C.nJ, [&](int I, int J) { sa_restrict_cell(stencil(l), f, C, wgt(l), om, I, J); });
+        sa_cells(sp, C.nI, C.nJ, [&](int I, int J) { sa_restrict_cell(stencil(l), f, C, wgt(l), om, I, J); });
         if (grid) { target += G; if (!grid_barrier(bar, target, &st->err)) return false; } else __syncthreads();
         return true;
     };
-    auto prolong_level = [&](int l, bool grid, double* rz) -> bool {
+    auto prolong_level = [&](int l, bool grid) -> bool {
         const SaSplit sp = grid ? all : cta;
-        const SaLevel<TV>& f = lvl(l);
+        const SaLevel<TV>& f = H.lv[l];
         const SaLevel<TV>& C = H.lv[l + 1];
-        if (l == 0) sa_cells(sp, f.nI, f.nJ, [&](int i, int j) { sa_prolong_cell(A0, f, C.y, C.P, wgt(l), i, j); });
-        else sa_cells(sp, f.nI, f.nJ, [&](int i, int j) { sa_prolong_cell(stencil(l), f, C.y, C.P, wgt(l), i, j); });
+        sa_cells(sp, f.nI, f.nJ, [&](int i, int j) { sa_prolong_cell(stencil(l), f, C.y, C.P, wgt(l), i, j); });
         if (grid) { target += G; if (!grid_barrier(bar, target, &st->err)) return false; } else __syncthreads();
-        double acc[1] = {0.0};
-        if (l == 0)
-            sa_cells(sp, f.nI, f.nJ, [&](int i, int j) {
-                const double y = sa_smooth_cell(A0, f, om, i, j);
-                acc[0] += (double)f.b[(size_t)i * f.P + j] * y;
-            });
-        else sa_cells(sp, f.nI, f.nJ, [&](int i, int j) { sa_smooth_cell(stencil(l), f, om, i, j); });
-        if (rz) {
-            block_sum<1>(acc, sm);
-            if (threadIdx.x == 0) partB[2 * blockIdx.x + 1] = acc[0];
-        }
+        sa_cells(sp, f.nI, f.nJ, [&](int i, int j) { sa_smooth_cell(stencil(l), f, om, i, j); });
         if (grid) { target += G; if (!grid_barrier(bar, target, &st->err)) return false; } else __syncthreads();
         return true;
     };
-    // ---- z = M r (V-cycle); z in level 0's y, rz = r.z
-    auto vcycle = [&](double& rz) -> bool {
-        for (int l = 0; l < H.Lg; ++l) {
+    // ---- z = M r (V-cycle) with r = L0.b; level 0's residual half (t, y)
+    // is done already (by the CG update, or by `first`); z in L0.y is
+    // overwritten by the prolongation; rz = r.z
+    const SaLevel<TV>& C1 = H.lv[1];
+    auto vcycle = [&](double& rz, bool first) -> bool {
+        if (first) {
+            sa_cells(all, L0.nI, L0.nJ, [&](int i, int j) { sa0_resid(A0f, omT, L0.b, L0.x, L0.t, L0.y, i, j); });
+            target += G;
+            if (!grid_barrier(bar, target, &st->err)) return false;
+        }
+        sa_cells(all, C1.nI, C1.nJ, [&](int I, int J) { sa0_restrict(A0f, L0.t, L0.y, C1, w0T, om, I, J); });
+        target += G;
+        if (!grid_barrier(bar, target, &st->err)) return false;
+        tick(SA_P_DOWN);
+        for (int l = 1; l < H.Lg; ++l) {
             if (!restrict_level(l, true)) return false;
             tick(SA_P_DOWN + l);
         }
         if (blockIdx.x == 0) {
             for (int l = H.Lg; l < H.L - 1; ++l) restrict_level(l, false);
             sa_dense_solve(H.lv[H.L - 1], H.dense);
-            for (int l = H.L - 2; l >= H.Lg; --l) prolong_level(l, false, nullptr);
+            for (int l = H.L - 2; l >= H.Lg; --l) prolong_level(l, false);
         }
         target += G;
         if (!grid_barrier(bar, target, &st->err)) return false;
         tick(SA_P_CTA);
-        for (int l = H.Lg - 1; l >= 0; --l) {
-            if (!prolong_level(l, true, l == 0 ? &rz : nullptr)) return false;
+        for (int l = H.Lg - 1; l >= 1; --l) {
+            if (!prolong_level(l, true)) return false;
             tick(SA_P_UP + l);
         }
+        double acc[1] = {0.0};
+        sa_cells(all, L0.nI, L0.nJ, [&](int i, int j) {
+            const TV y = sa0_prolong(A0f, L0.x, L0.b, C1.y, C1.P, w0T, omT, i, j);
+            const int c = i * L0.P + j;
+            L0.y[c] = y;
+            acc[0] += (double)L0.b[c] * (double)y;
+        });
+        block_sum<1>(acc, sm);
+        if (threadIdx.x == 0) partB[2 * blockIdx.x + 1] = acc[0];
+        target += G;
+        if (!grid_barrier(bar, target, &st->err)) return false;
         double t2[2];
         sum_partials<2>(partB, G, 2, t2, sm);
         rz = t2[1];
+        tick(SA_P_UP);
         return true;
     };
 
     double rz = 0.0;
-    if (!vcycle(rz)) return;
+    if (!vcycle(rz, true)) return;
     double beta = 0.0;
     int it = 0;
     TV* pbuf[2] = {B.pa, B.pb};
-    const TV* z = L0.y;
+    TV* rbuf[2] = {B.r, H.r2};
     for (; it < k.maxP; ++it) {
         TV* __restrict__ pnew = pbuf[it & 1];
         const TV* pold = pbuf[(it + 1) & 1];
         const TV bt = (TV)beta;
         const bool first = it == 0;
-        auto dir = [&](size_t c) -> TV { return first ? z[c] : (TV)(z[c] + bt * pold[c]); };
         double accA[1] = {0.0};
-        for (int t = tid; t < n; t += nth) {
-            const int i = 1 + t / w, j = 1 + t % w;
-            const size_t c = at(d, i, j);
-            const TV pc = dir(c);
-            TV ap = B.d[c] * pc;
-            if (j < w) ap -= B.fE[c] * dir(c + 1);
-            if (j > 1) ap -= B.fE[c - 1] * dir(c - 1);
-            if (i < M - 1) ap -= B.fN[c] * dir(c + d.P);
-            if (i > 1) ap -= B.fN[c - d.P] * dir(c - d.P);
-            pnew[c] = pc;
-            B.Ap[c] = ap;
-            accA[0] += (double)pc * (double)ap;
-        }
+        sa_cells(all, L0.nI, L0.nJ,
+                 [&](int i, int j) { accA[0] += sa0_matvec(A0f, L0.y, pold, bt, first, pnew, B.Ap, i, j); });
         block_sum<1>(accA, sm);
         if (threadIdx.x == 0) partA[blockIdx.x] = accA[0];
         SA_SYNC();
@@ -493,17 +610,14 @@ __global__ void __launch_bounds__(512, 1) k_pcg_sa(KParams k, Status* st, const 
         sum_partials<1>(partA, G, 1, pAp, sm);
         tick(SA_P_MATVEC);
         if (fabs(pAp[0]) < 1e-20) break;
-        const double alpha = rz / pAp[0];
-        const TV al = (TV)alpha, omT = (TV)om;
+        const TV al = (TV)(rz / pAp[0]);
+        const TV* rold = rbuf[it & 1];
+        TV* rnew = rbuf[(it + 1) & 1];
         double accB[1] = {0.0};
-        for (int t = tid; t < n; t += nth) {
-            const size_t c = at(d, 1 + t / w, 1 + t % w);
-            B.x[c] = B.x[c] + al * pnew[c];
-            const TV r = B.r[c] - al * B.Ap[c];
-            B.r[c] = r;
-            L0.x[c] = omT * r / B.d[c];
-            accB[0] += (double)r * (double)r;
-        }
+        sa_cells(all, L0.nI, L0.nJ, [&](int i, int j) {
+            accB[0] += sa0_update(A0f, al, omT, pnew, B.Ap, B.x, rold, rnew, L0.x, L0.t, L0.y, i, j);
+        });
+        L0.b = rnew;
         block_sum<1>(accB, sm);
         if (threadIdx.x == 0) partB[2 * blockIdx.x] = accB[0];
         SA_SYNC();
@@ -512,17 +626,21 @@ __global__ void __launch_bounds__(512, 1) k_pcg_sa(KParams k, Status* st, const 
         tick(SA_P_UPDATE);
         if (sqrt(tB[0]) <= rTol) { ++it; break; }
         double rzn = 0.0;
-        if (!vcycle(rzn)) return;
+        if (!vcycle(rzn, false)) return;
         beta = rzn / rz;
         rz = rzn;
     }
     for (int t = tid; t < n; t += nth) {
         const int i = 1 + t / w, j = 1 + t % w;
-        const size_t c = at(d, i, j);
+        const int c = i * d.P + j;
         pStar[c] = (double)B.x[c];
         if (j == w) pStar[c + 1] = 0.0;
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) st->itersP = it;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        st->itersP = it;
+        if (H.force) *H.dirty = 1;
+        else if (rebuild) *H.dirty = 0;
+    }
 #undef SA_SYNC
 }
 

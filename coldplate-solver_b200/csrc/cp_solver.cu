@@ -116,6 +116,8 @@ struct cp_ctx {
     void* saDense = nullptr;
     double saOmega = 0.9, saW0 = 2.0 / 3.0, saWc = 0.8;
     unsigned long long* saProf = nullptr;    // per-phase timers when CP_SA_PROFILE is set
+    int saReuse = 8;                         // outer iterations between coarse-operator rebuilds
+    int* saDirty = nullptr;                  // device flag: rebuild the coarse operators on the next solve
     MgMaps mgMaps;                           // TMA tensor maps of the level-0 tile phases
     // adjoint buffers (allocated on first use, double)
     double* adj[40] = {};
@@ -248,12 +250,23 @@ void build_density(const cp_ctx* c, const std::vector<double>& cellTypePadded, s
     }
 }
 
+// the smoothed-aggregation coarse operators are rebuilt by the next solve
+// (after a change of geometry or state from the host, or a dispatch call)
+cp_status mark_sa_stale(cp_ctx* c) {
+    if (!c->saDirty) return CP_OK;
+    static const int one = 1;
+    CK(cudaMemcpyAsync(c->saDirty, &one, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    return CP_OK;
+}
+
 cp_status upload_cells(cp_ctx* c, const std::vector<double>& g, const std::vector<double>& a) {
     const int M = c->d.M, N = c->d.N;
     CK(cudaMemcpy2DAsync(c->gamma, (size_t)c->d.P * 8, g.data(), (size_t)N * 8, (size_t)N * 8, M,
                          cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpy2DAsync(c->alpha, (size_t)c->d.P * 8, a.data(), (size_t)N * 8, (size_t)N * 8, M,
                          cudaMemcpyHostToDevice, c->stream));
+    cp_status s = mark_sa_stale(c);
+    if (s != CP_OK) return s;
     CK(cudaStreamSynchronize(c->stream));
     return CP_OK;
 }
@@ -477,6 +490,10 @@ SaHier<TV> sa_hier(cp_ctx* c) {
     H.wc = c->saWc;
     H.dense = (TV*)c->saDense;
     H.prof = c->saProf;
+    H.r2 = (TV*)c->saArr[0][11];
+    H.reuse = c->saReuse;
+    H.force = 0;
+    H.dirty = c->saDirty;
     for (int q = 0; q < 9; ++q) H.Y[q] = (TV*)c->saY[q];
     for (int l = 0; l < c->saL; ++l) {
         SaLevel<TV>& v = H.lv[l];
@@ -511,10 +528,14 @@ cp_status sa_build(cp_ctx* c) {
     c->saLg = Lg;
     c->saP[0] = c->d.P;
     cp_status s;
-    for (int q = 9; q <= 12; ++q) {
-        if (q == 11) continue;                 // level 0's rhs is the CG residual
+    // level 0: pre-smoothed iterate, corrected iterate, the second CG
+    // residual buffer (its rhs is the CG residual), scratch
+    for (int q = 9; q <= 12; ++q)
         if ((s = dalloc_bytes(c, &c->saArr[0][q], c->nElem * c->es)) != CP_OK) return s;
-    }
+    if ((s = dalloc(c, &c->saDirty, 1)) != CP_OK) return s;
+    const int one = 1;
+    CK(cudaMemcpyAsync(c->saDirty, &one, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
     for (int l = 1; l < L; ++l) {
         c->saP[l] = ((c->saNJ[l] + 2 + 31) / 32) * 32;
         const size_t ne = (size_t)(c->saNI[l] + 2) * c->saP[l];
@@ -527,6 +548,7 @@ cp_status sa_build(cp_ctx* c) {
     if (const char* e = getenv("CP_SA_OMEGA")) c->saOmega = atof(e);
     if (const char* e = getenv("CP_SA_W0")) c->saW0 = atof(e);
     if (const char* e = getenv("CP_SA_WC")) c->saWc = atof(e);
+    if (const char* e = getenv("CP_SA_REUSE")) c->saReuse = std::max(atoi(e), 1);
     if (getenv("CP_SA_PROFILE") && (s = dalloc(c, &c->saProf, (size_t)SA_P_COUNT)) != CP_OK) return s;
     int nb = 0;
     if (c->prm.precision == CP_PREC_MIXED) {
@@ -1011,6 +1033,7 @@ cp_status cp_set_field(cp_ctx* c, cp_field which, const double* host, long rows,
     if (s != CP_OK) return s;
     CK(cudaMemcpy2DAsync(dp, (size_t)c->d.P * 8, dense.data(), (size_t)C * 8, (size_t)C * 8, R,
                          cudaMemcpyHostToDevice, c->stream));
+    if (mark_sa_stale(c) != CP_OK) return CP_ERR_CUDA;
     CK(cudaStreamSynchronize(c->stream));
     return CP_OK;
 }
@@ -1125,6 +1148,7 @@ cp_status cp_pressure(cp_ctx* c, int* iters, double* residMass) {
     if (s != CP_OK) return s;
     if (c->stHost->done) return fail(CP_ERR_STATE, "loop already stopped; call cp_reset_loop first");
     CK(cudaMemsetAsync(c->pStar, 0, c->nElem * sizeof(double), c->stream));
+    if ((s = mark_sa_stale(c)) != CP_OK) return s;
     s = c->prm.precision == CP_PREC_MIXED ? enqueue_pressure<float>(c) : enqueue_pressure<double>(c);
     if (s != CP_OK) return s;
     std::vector<double> part((size_t)4 * c->nbMass);
@@ -1186,6 +1210,7 @@ cp_status adjoint_pcg(cp_ctx* c, const KParams& k, const double* dE, const doubl
     CK(cudaMemsetAsync(c->adjBar, 0, sizeof(unsigned), c->stream));
     if (c->useSa) {
         SaHier<TV> H = sa_hier<TV>(c);
+        H.force = 1;   // the adjoint's operator: rebuild, and leave the forward's marked stale
         CK(launch_coop_cfg(k_pcg_sa<TV>, c->gMg, kMgThreads, kSaDynSmem, c->stream, k, c->adjSt, dE, dN, B, H, out,
                            c->adjPart, c->adjBar));
     } else if (c->useMg) {

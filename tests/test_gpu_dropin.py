@@ -53,11 +53,17 @@ def _logs_of(g) -> tuple[np.ndarray, np.ndarray]:
                 np.loadtxt(os.path.join(d, "pressure_drop_history.txt"), comments=("#", "I", "i"), ndmin=2))
 
 
+# SIMPLE.h float members the case does not set, at their defaults
+_FLOAT_DEFAULTS = dict(uvAlpha=0.7, pAlpha=0.3, momentumTol=1e-6, residNormFloorVel=1e-6, residNormFloorMass=1e-12,
+                       twoPointFiveDSinkMultiplier=1.0)
+
+
 def _as_float32(prm: dict) -> dict:
     """The parameters as the reference's float build holds them (its members
     are float): the drop-in passes those values on, so the Python path runs
     with the same ones."""
-    return {k: float(np.float32(v)) if isinstance(v, float) else v for k, v in prm.items()}
+    out = {**_FLOAT_DEFAULTS, **prm}
+    return {k: float(np.float32(v)) if isinstance(v, float) else v for k, v in out.items()}
 
 
 def test_reference_loop_over_the_library_matches_the_python_path():
