@@ -23,10 +23,21 @@
 //   * V(1,1) cycle with damped Jacobi (omega 0.9) before and after the
 //     coarse correction, a dense inverse on the coarsest level (<= 64
 //     unknowns).  The cycle is symmetric, so CG applies.
-// Levels with more than kSaCtaCells unknowns (and always level 0) run on the
-// whole grid between bounded grid barriers; smaller levels run on CTA 0.
-// The CG recurrences, the |p.Ap| < 1e-20 exit and AMGCL's relative stop rule
-// ||r|| <= pTol ||b|| are those of k_pcg_mg.
+// A row of P has at most four entries: the unknown's own aggregate and the
+// aggregates across its horizontal, vertical and diagonal neighbours (none
+// diagonal on the 5-point level 0).  Level 0 and the grid-wide coarse levels
+// store these weights, so the restriction P^T t is a weighted sum over the
+// 5 x 5 support and the prolongation four multiply-adds per unknown.
+// Level 0 runs its CG passes on row segments: a warp takes 32 groups of 16
+// bytes (4 floats or 2 doubles) of one row, with vector loads of the row and
+// of its two neighbour rows and the horizontal neighbours from the adjacent
+// lanes.  Levels with more than kSaCtaCells unknowns, or too many to stage,
+// run on the whole grid between bounded grid barriers; the rest (and the
+// dense inverse) are copied into CTA 0's shared memory once per launch and
+// cycled there.  The coarse operators are rebuilt every `reuse` outer
+// iterations; the CG matvec and level 0's smoother and prolongation always
+// use the current operator.  The CG recurrences, the |p.Ap| < 1e-20 exit and
+// AMGCL's relative stop rule ||r|| <= pTol ||b|| are those of k_pcg_mg.
 #pragma once
 
 #include "cp_mg.cuh"
@@ -34,30 +45,36 @@
 namespace cp {
 
 constexpr int kSaMaxLevels = 12;
-constexpr int kSaCtaCells = 4096;    // levels at or below this size run on one CTA
+constexpr int kSaCtaCells = 4096;    // levels at or below this size may run on one CTA
 constexpr int kSaDense = 64;         // coarsest level size solved by a dense inverse
+constexpr size_t kSaSmemBudget = 200 * 1024;   // CTA 0's staged levels and dense inverse
 
 // A level: unknowns i in [1, nI], j in [1, nJ] with a zero frame, row pitch P.
 // Level 0 keeps its 5-point operator as face coefficients (fE, fN, d of the
 // PCG buffers); levels >= 1 hold a 9-point stencil c[k], k = (di+1)*3 + (dj+1),
 // c[4] the diagonal, entries towards unknowns outside the level zero.
+// pw[0..3]: the prolongation weights of each unknown towards its own,
+// horizontal, vertical and diagonal aggregate (level 0 and grid-wide levels
+// that have a coarser one; zero on the frame).
 template <typename TV>
 struct SaLevel {
     int nI, nJ, P;
     TV* c[9];
     TV *x, *y, *b, *t;      // pre-smoothed iterate, corrected iterate, rhs, scratch
+    TV* pw[4];
 };
 
 template <typename TV>
 struct SaHier {
-    int L, Lg;              // levels; levels [0, Lg) run grid-wide
+    int L, Lg;              // levels; levels [0, Lg) run grid-wide, [Lg, L) on CTA 0
     SaLevel<TV> lv[kSaMaxLevels];
-    const TV *fE, *fN, *d;  // level-0 operator
+    TV* dinv0;              // level-0 inverse diagonal
     TV* Y[9];               // coloured probes A P e_c (level-0 sized)
     TV* dense;              // inverse of the coarsest operator
     double omega, w0, wc;   // Jacobi damping, prolongator smoothing weights
     TV* r2;                 // second CG residual buffer (the residual ping-pongs)
     int reuse;              // rebuild the coarse operators every `reuse` outer iterations
+    int split0;             // level-0 prolongation and post-smoothing as two passes
     int force;              // 1: rebuild now and leave the hierarchy marked stale
     int* dirty;             // device flag: the stored hierarchy is not the forward's
     unsigned long long* prof;  // optional per-phase device time (ns, block 0's view), or null
@@ -68,6 +85,15 @@ struct SaHier {
 // at SA_P_UP + l
 enum SaPhase { SA_P_SETUP = 0, SA_P_GALERKIN, SA_P_MATVEC, SA_P_UPDATE, SA_P_CTA, SA_P_DOWN, SA_P_UP = SA_P_DOWN + kSaMaxLevels,
                SA_P_COUNT = SA_P_UP + kSaMaxLevels };
+
+// shared-memory elements of levels [Lg, L) staged on CTA 0 (13 arrays of
+// (nI + 2) x (nJ + 2) each) plus the dense inverse of level L - 1
+__host__ __device__ inline size_t sa_cta_elems(const int* nI, const int* nJ, int Lg, int L) {
+    size_t e = 0;
+    for (int l = Lg; l < L; ++l) e += 13 * (size_t)(nI[l] + 2) * (nJ[l] + 2);
+    const size_t n = (size_t)nI[L - 1] * nJ[L - 1];
+    return e + n * n;
+}
 
 __host__ __device__ __forceinline__ int sa_coarse(int n) { return (n + 2) / 3; }
 
@@ -113,10 +139,23 @@ struct SaSplit {
     int t0, nt;
 };
 
+// cells t0, t0 + nt, ... of a level in row-major order, (i, j) stepped
+// without a division per cell
 template <typename F>
 __device__ __forceinline__ void sa_cells(SaSplit s, int nI, int nJ, F&& fn) {
     const int n = nI * nJ;
-    for (int t = s.t0; t < n; t += s.nt) fn(1 + t / nJ, 1 + t % nJ);
+    if (s.t0 >= n) return;
+    int i = 1 + s.t0 / nJ, j = 1 + s.t0 % nJ;
+    const int di = s.nt / nJ, dj = s.nt % nJ;
+    for (int t = s.t0; t < n; t += s.nt) {
+        fn(i, j);
+        i += di;
+        j += dj;
+        if (j > nJ) {
+            j -= nJ;
+            ++i;
+        }
+    }
 }
 
 // ---------------------------------------------------------------- Galerkin set-up
@@ -202,72 +241,197 @@ __device__ __forceinline__ void sa_galerkin_cell(const St& A, int Pf, TV* const*
     }
 }
 
-// ---------------------------------------------------------------- cycle pieces
-// (A v)(i, j) on a level, v zero outside the unknowns (frame) and read only
-// inside them
-template <typename TV, class St>
-__device__ __forceinline__ double sa_av(const St& A, int P, const TV* v, int i, int j) {
-    double s = 0.0;
+// ---------------------------------------------------------------- prolongation weights
+// Offset (-1, 0 or +1) of the aggregate across a fine unknown's horizontal
+// (vertical) neighbours when it sits on the first or last column (row) of its
+// aggregate; 0 in the middle one.
+__device__ __forceinline__ int sa_side(int i) {
+    const int r = (i - 1) % 3;
+    return r == 0 ? -1 : (r == 2 ? 1 : 0);
+}
+
+// Row (i, j) of P = (I - w D^-1 A) P0: pw[0] towards the own aggregate,
+// pw[1] / pw[2] / pw[3] towards the horizontal / vertical / diagonal one
+// (sa_pk's entries, grouped by aggregate).
+template <class St>
+__device__ __forceinline__ void sa_pweights(const St& A, int i, int j, double w, double (&pw)[4]) {
+    const int ri = (i - 1) % 3, rj = (j - 1) % 3;
+    double s[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
     for (int a = 0; a < St::kN; ++a) {
         const int k = St::k_of(a);
-        const int ni = i + sa_di(k), nj = j + sa_dj(k);
+        const int di = sa_di(k), dj = sa_dj(k);
+        const int ni = i + di, nj = j + dj;
         if (ni < 1 || ni > A.nI || nj < 1 || nj > A.nJ) continue;
-        s += A(i, j, k) * (double)v[(size_t)ni * P + nj];
+        const bool oi = ri + di < 0 || ri + di > 2, oj = rj + dj < 0 || rj + dj > 2;
+        s[(oi ? 2 : 0) + (oj ? 1 : 0)] += A(i, j, k);
     }
+    const double sc = w / A(i, j, 4);
+    pw[0] = 1.0 - sc * s[0];
+    pw[1] = -sc * s[1];
+    pw[2] = -sc * s[2];
+    pw[3] = -sc * s[3];
+}
+
+// ---------------------------------------------------------------- cycle pieces
+// (A v) at q = (i, j) of a coarse level whose c[k] and v are zero on the
+// frame (the stencil towards outside the level is zero), without range checks
+template <typename TV>
+__device__ __forceinline__ double sa9_av(const SaLevel<TV>& f, const TV* v, size_t q) {
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k < 9; ++k)
+        s += (double)f.c[k][q] * (double)v[(ptrdiff_t)q + (k / 3 - 1) * (ptrdiff_t)f.P + (k % 3 - 1)];
     return s;
 }
 
-// restriction, part 1 (fine unknown): t = r1 = b - A x (x the pre-smoothed
-// iterate) and y = r1 / d
-template <typename TV, class St>
-__device__ __forceinline__ void sa_resid_cell(const St& A, const SaLevel<TV>& f, int i, int j) {
+// restriction, part 1 (fine unknown of a grid-wide coarse level):
+// t = r1 = b - A x (x the pre-smoothed iterate)
+template <typename TV>
+__device__ __forceinline__ void sa_resid_cell(const SaLevel<TV>& f, int i, int j) {
     const size_t q = (size_t)i * f.P + j;
-    const double r1 = (double)f.b[q] - sa_av(A, f.P, f.x, i, j);
-    f.t[q] = (TV)r1;
-    f.y[q] = (TV)(r1 / A(i, j, 4));
+    f.t[q] = (TV)((double)f.b[q] - sa9_av(f, f.x, q));
 }
 
-// restriction, part 2 (coarse unknown): b_c = sum over the aggregate of
-// r1 - w A D^-1 r1 (= P^T r1), and the pre-smoothed x_c = omega b_c / d_c
-template <typename TV, class St>
-__device__ __forceinline__ void sa_restrict_cell(const St& A, const SaLevel<TV>& f, const SaLevel<TV>& C, double w,
-                                                 double omega, int I, int J) {
+// restriction, part 2 with stored weights (coarse unknown): b_c = (P^T t)_c
+// over the aggregate's 5 x 5 support (the ring rows / columns weigh in with
+// their vertical / horizontal / diagonal weights; no diagonal ones with
+// Corners false), and the pre-smoothed x_c = omega b_c / d_c
+template <typename TV, bool Corners>
+__device__ __forceinline__ void sa_restrict_w(const SaLevel<TV>& f, const SaLevel<TV>& C, double omega, int I,
+                                              int J) {
+    const int i0 = 3 * I - 3, j0 = 3 * J - 3;
     double s = 0.0;
-    for (int i = 3 * I - 2; i <= min(3 * I, f.nI); ++i)
-        for (int j = 3 * J - 2; j <= min(3 * J, f.nJ); ++j)
-            s += (double)f.t[(size_t)i * f.P + j] - w * sa_av(A, f.P, f.y, i, j);
+#pragma unroll
+    for (int a = 0; a < 5; ++a) {
+        const int ii = i0 + a;
+        const int ra = (a == 0 || a == 4) ? 1 : 0;
+#pragma unroll
+        for (int b = 0; b < 5; ++b) {
+            const int rb = (b == 0 || b == 4) ? 1 : 0;
+            if (!Corners && ra && rb) continue;
+            const int jj = j0 + b;
+            if (ii < 1 || ii > f.nI || jj < 1 || jj > f.nJ) continue;
+            const size_t q = (size_t)ii * f.P + jj;
+            s += (double)f.pw[2 * ra + rb][q] * (double)f.t[q];
+        }
+    }
     const size_t qc = (size_t)I * C.P + J;
     C.b[qc] = (TV)s;
     C.x[qc] = (TV)(omega * s / (double)C.c[4][qc]);
 }
 
-// prolongation, part 1 (fine unknown): t = x + P e, e the coarse corrected
-// iterate: (P e)(m) = e(agg m) - w / d_m sum_n A_mn e(agg n)
-template <typename TV, class St>
-__device__ __forceinline__ void sa_prolong_cell(const St& A, const SaLevel<TV>& f, const TV* e, int Pc, double w,
-                                                int i, int j) {
-    auto e0 = [&](int ii, int jj) -> double { return (double)e[(size_t)((ii - 1) / 3 + 1) * Pc + (jj - 1) / 3 + 1]; };
-    double s = 0.0;
-#pragma unroll
-    for (int a = 0; a < St::kN; ++a) {
-        const int k = St::k_of(a);
-        const int ni = i + sa_di(k), nj = j + sa_dj(k);
-        if (ni < 1 || ni > A.nI || nj < 1 || nj > A.nJ) continue;
-        s += A(i, j, k) * e0(ni, nj);
-    }
+// prolongation, part 1 with stored weights (fine unknown): t = x + P e
+template <typename TV>
+__device__ __forceinline__ void sa_prolong_w(const SaLevel<TV>& f, const TV* e, int Pc, int i, int j) {
     const size_t q = (size_t)i * f.P + j;
-    f.t[q] = (TV)((double)f.x[q] + e0(i, j) - w * s / A(i, j, 4));
+    const int sh = sa_side(j), sv = sa_side(i) * Pc;
+    const TV* er = e + (size_t)((i - 1) / 3 + 1) * Pc + (j - 1) / 3 + 1;
+    const double t = (double)f.x[q] + (double)f.pw[0][q] * (double)er[0] + (double)f.pw[1][q] * (double)er[sh] +
+                     (double)f.pw[2][q] * (double)er[sv] + (double)f.pw[3][q] * (double)er[sv + sh];
+    f.t[q] = (TV)t;
 }
 
-// prolongation, part 2 (fine unknown): post-smoothing y = t + omega (b - A t) / d
-template <typename TV, class St>
-__device__ __forceinline__ double sa_smooth_cell(const St& A, const SaLevel<TV>& f, double omega, int i, int j) {
+// prolongation, part 2 (fine unknown of a grid-wide coarse level):
+// post-smoothing y = t + omega (b - A t) / d
+template <typename TV>
+__device__ __forceinline__ void sa_smooth_cell(const SaLevel<TV>& f, double omega, int i, int j) {
     const size_t q = (size_t)i * f.P + j;
     const double tc = (double)f.t[q];
-    const double y = tc + omega * ((double)f.b[q] - sa_av(A, f.P, f.t, i, j)) / A(i, j, 4);
-    f.y[q] = (TV)y;
-    return y;
+    f.y[q] = (TV)(tc + omega * ((double)f.b[q] - sa9_av(f, f.t, q)) / (double)f.c[4][q]);
+}
+
+// ---------------------------------------------------------------- CTA 0's levels
+// A level staged in CTA 0's shared memory: 13 arrays of ne = (nI + 2) x
+// (nJ + 2) elements from s (c[0..8], x, y, b, t), frames included (zero
+// outside the unknowns, like the stencil towards them), pitch nJ + 2.  The
+// passes run without range checks, with arithmetic in TV; P is applied
+// through the operator (t - w A D^-1 t summed over the aggregate, and
+// e(agg) - w D^-1 A e(agg)).
+template <typename TV>
+struct SaSm {
+    TV* s;
+    int nI, nJ, P, ne;
+    __device__ __forceinline__ TV* c(int k) const { return s + k * ne; }
+    __device__ __forceinline__ TV* x() const { return s + 9 * ne; }
+    __device__ __forceinline__ TV* y() const { return s + 10 * ne; }
+    __device__ __forceinline__ TV* b() const { return s + 11 * ne; }
+    __device__ __forceinline__ TV* t() const { return s + 12 * ne; }
+};
+
+// level l of the staged levels [Lg, L) at dsm
+template <typename TV>
+__device__ __forceinline__ SaSm<TV> sa_sm(const SaHier<TV>& H, TV* dsm, int l) {
+    int off = 0;
+    for (int m = H.Lg; m < l; ++m) off += 13 * (H.lv[m].nI + 2) * (H.lv[m].nJ + 2);
+    const int nI = H.lv[l].nI, nJ = H.lv[l].nJ;
+    return SaSm<TV>{dsm + off, nI, nJ, nJ + 2, (nI + 2) * (nJ + 2)};
+}
+
+template <typename TV>
+__device__ __forceinline__ TV sa_sm_av(const SaSm<TV>& f, const TV* v, int q) {
+    TV s = (TV)0;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) s += f.s[k * f.ne + q] * v[q + (k / 3 - 1) * f.P + (k % 3 - 1)];
+    return s;
+}
+
+// restriction out of a staged level: t = b - A x, y = t / d; then
+// t <- t - w A y; then per coarse unknown b_c = sum of t over the aggregate,
+// x_c = omega b_c / d_c
+template <typename TV>
+__device__ __forceinline__ void sa_sm_resid(const SaSm<TV>& f, int i, int j) {
+    const int q = i * f.P + j;
+    const TV r1 = f.b()[q] - sa_sm_av(f, f.x(), q);
+    f.t()[q] = r1;
+    f.y()[q] = r1 / f.s[4 * f.ne + q];
+}
+template <typename TV>
+__device__ __forceinline__ void sa_sm_smoothres(const SaSm<TV>& f, TV w, int i, int j) {
+    const int q = i * f.P + j;
+    f.t()[q] -= w * sa_sm_av(f, f.y(), q);
+}
+template <typename TV>
+__device__ __forceinline__ void sa_sm_aggsum(const SaSm<TV>& f, const SaSm<TV>& C, TV omega, int I, int J) {
+    TV s = (TV)0;
+    const int i1 = min(3 * I, f.nI), j1 = min(3 * J, f.nJ);
+    for (int i = 3 * I - 2; i <= i1; ++i)
+        for (int j = 3 * J - 2; j <= j1; ++j) s += f.t()[i * f.P + j];
+    const int qc = I * C.P + J;
+    C.b()[qc] = s;
+    C.x()[qc] = omega * s / C.s[4 * C.ne + qc];
+}
+// prolongation into a staged level: t = x + P e, then y = t + omega (b - A t) / d
+template <typename TV>
+__device__ __forceinline__ void sa_sm_prolong(const SaSm<TV>& f, const SaSm<TV>& C, TV w, int i, int j) {
+    const int q = i * f.P + j;
+    const TV* e = C.y();
+    auto e0 = [&](int ii, int jj) -> TV { return e[((ii - 1) / 3 + 1) * C.P + (jj - 1) / 3 + 1]; };
+    TV s = (TV)0;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) s += f.s[k * f.ne + q] * e0(i + k / 3 - 1, j + k % 3 - 1);
+    f.t()[q] = f.x()[q] + e0(i, j) - w * s / f.s[4 * f.ne + q];
+}
+template <typename TV>
+__device__ __forceinline__ void sa_sm_smooth(const SaSm<TV>& f, TV omega, int i, int j) {
+    const int q = i * f.P + j;
+    const TV tc = f.t()[q];
+    f.y()[q] = tc + omega * (f.b()[q] - sa_sm_av(f, f.t(), q)) / f.s[4 * f.ne + q];
+}
+// coarsest staged level: y = A^-1 b with the staged dense inverse (b is
+// gathered into t first)
+template <typename TV>
+__device__ __forceinline__ void sa_sm_dense(const SaSm<TV>& l, const TV* inv) {
+    const int n = l.nI * l.nJ;
+    TV* bv = l.t();
+    for (int a = threadIdx.x; a < n; a += blockDim.x) bv[a] = l.b()[(1 + a / l.nJ) * l.P + 1 + a % l.nJ];
+    __syncthreads();
+    for (int a = threadIdx.x; a < n; a += blockDim.x) {
+        TV s = (TV)0;
+        for (int b2 = 0; b2 < n; ++b2) s += inv[a * n + b2] * bv[b2];
+        l.y()[(1 + a / l.nJ) * l.P + 1 + a % l.nJ] = s;
+    }
+    __syncthreads();
 }
 
 // dense inverse of the coarsest (9-point) operator by Gauss-Jordan (SPD, no
@@ -305,122 +469,341 @@ __device__ void sa_dense_setup(const SaLevel<TV>& l, TV* inv, double* work /* sm
     __syncthreads();
 }
 
-// coarsest level: y = A^-1 b
-template <typename TV>
-__device__ void sa_dense_solve(const SaLevel<TV>& l, const TV* inv) {
-    const int n = l.nI * l.nJ;
-    for (int a = threadIdx.x; a < n; a += blockDim.x) {
-        double s = 0.0;
-        for (int b2 = 0; b2 < n; ++b2)
-            s += (double)inv[a * n + b2] * (double)l.b[(size_t)(1 + b2 / l.nJ) * l.P + 1 + b2 % l.nJ];
-        l.y[(size_t)(1 + a / l.nJ) * l.P + 1 + a % l.nJ] = (TV)s;
-    }
-    __syncthreads();
-}
-
-// ---------------------------------------------------------------- level-0 passes
-// Level 0 has the 5-point operator of the face coefficients fE (east), fN
-// (north) and the diagonal d.  Its arrays are zero on the frame (only the
-// unknowns are ever written), and fE / fN are zero on the frame rows and
-// columns, so these passes read neighbours without range checks wherever a
-// zero frame value gives the right term.  Arithmetic in TV.
+// ---------------------------------------------------------------- level 0
+// Level 0's operator: face coefficients fE (east), fN (north), the diagonal
+// d, its inverse and the prolongation weights towards the own, horizontal and
+// vertical aggregate.  Every level-0 array is zero on the frame (only the
+// unknowns are ever written) and fE / fN are zero on the frame rows and
+// columns, so the passes read neighbours without range checks wherever a zero
+// frame value gives the right term.  Arithmetic in TV.
 template <typename TV>
 struct Sa0 {
-    const TV *fE, *fN, *d;
+    const TV *fE, *fN, *d, *dinv, *pO, *pH, *pV;
     int nI, nJ, P;
 };
 
-// CG matvec on p = z + beta p_old: writes p and Ap, returns p.Ap's share
+// 16 bytes of one row: 4 floats or 2 doubles
 template <typename TV>
-__device__ __forceinline__ double sa0_matvec(const Sa0<TV>& A, const TV* z, const TV* pold, TV bt, bool first,
-                                             TV* pnew, TV* Ap, int i, int j) {
-    const int c = i * A.P + j;
+struct SaVec {
+    static constexpr int n = 16 / (int)sizeof(TV);
+    TV v[n];
+};
+__device__ __forceinline__ SaVec<float> sa_ld(const float* p) {
+    const float4 f = *reinterpret_cast<const float4*>(p);
+    return {{f.x, f.y, f.z, f.w}};
+}
+__device__ __forceinline__ SaVec<double> sa_ld(const double* p) {
+    const double2 f = *reinterpret_cast<const double2*>(p);
+    return {{f.x, f.y}};
+}
+__device__ __forceinline__ void sa_st(float* p, const SaVec<float>& a) {
+    *reinterpret_cast<float4*>(p) = make_float4(a.v[0], a.v[1], a.v[2], a.v[3]);
+}
+__device__ __forceinline__ void sa_st(double* p, const SaVec<double>& a) {
+    *reinterpret_cast<double2*>(p) = make_double2(a.v[0], a.v[1]);
+}
+template <typename TV>
+__device__ __forceinline__ SaVec<TV> sa_zero() {
+    SaVec<TV> a;
+#pragma unroll
+    for (int k = 0; k < SaVec<TV>::n; ++k) a.v[k] = (TV)0;
+    return a;
+}
+
+// Row segments of level 0: warp w takes segments w, w + nwarps, ... of 32
+// lane groups of one row, lane group g covering columns [g V, g V + V)
+// (V = 16 / sizeof(TV)); fn(i, j0, act, lane) with act false on the groups
+// past the row's last unknown.  The loop is uniform over each warp, so fn
+// may shuffle.  A vector of groups below g V <= nJ stays inside the row
+// (the pitch is a multiple of 32 and at least nJ + 3), and column g V + V,
+// read by lane 31, at most at the next row's column 0.
+template <typename TV, typename F>
+__device__ __forceinline__ void sa_rows(int nI, int nJ, F&& fn) {
+    constexpr int V = SaVec<TV>::n;
+    const int lane = threadIdx.x & 31;
+    const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), nw = (int)((gridDim.x * blockDim.x) >> 5);
+    const int Ga = nJ / V + 1, S = (Ga + 31) >> 5;
+    for (int s = warp; s < nI * S; s += nw) {
+        const int i = 1 + s / S, g = ((s % S) << 5) + lane;
+        fn(i, g * V, g < Ga, lane);
+    }
+}
+
+template <typename TV>
+__device__ __forceinline__ TV sa_from_west(TV v) { return __shfl_up_sync(0xffffffffu, v, 1); }
+template <typename TV>
+__device__ __forceinline__ TV sa_from_east(TV v) { return __shfl_down_sync(0xffffffffu, v, 1); }
+
+// CG matvec on p = z + beta p_old (p_old unused when first): writes p and Ap
+// on one lane group, returns the group's share of p.Ap
+template <typename TV>
+__device__ __forceinline__ double sa0_matvec(const Sa0<TV>& A, const TV* __restrict__ z, const TV* __restrict__ pold,
+                                             TV bt, bool first, TV* __restrict__ pnew, TV* __restrict__ Ap, int i,
+                                             int j0, bool act, int lane) {
+    constexpr int V = SaVec<TV>::n;
+    const int P = A.P, c = i * P + j0;
     auto dir = [&](int q) -> TV { return first ? z[q] : (TV)(z[q] + bt * pold[q]); };
-    const TV pc = dir(c);
-    const TV ap = A.d[c] * pc - A.fE[c] * dir(c + 1) - A.fE[c - 1] * dir(c - 1) - A.fN[c] * dir(c + A.P) -
-                  A.fN[c - A.P] * dir(c - A.P);
-    pnew[c] = pc;
-    Ap[c] = ap;
-    return (double)pc * (double)ap;
-}
-
-// CG update fused with the first half of the next restriction:
-// x += alpha p, r' = r - alpha Ap (into rn), x0' = omega r' / d (the
-// pre-smoothed level-0 iterate), and the residual of the pre-smoothing
-// t = r' - A x0' = (1 - omega) r' + sum of the faces' f x0'(neighbour), with
-// x0' of the neighbours recomputed from r and Ap; y = t / d.  Returns |r'|^2.
-template <typename TV>
-__device__ __forceinline__ double sa0_update(const Sa0<TV>& A, TV al, TV om, const TV* p, const TV* Ap, TV* x,
-                                             const TV* r, TV* rn, TV* x0, TV* t, TV* y, int i, int j) {
-    const int c = i * A.P + j;
-    auto x0n = [&](int q) -> TV { return om * (r[q] - al * Ap[q]) / A.d[q]; };
-    const TV rc = r[c] - al * Ap[c];
-    x[c] = x[c] + al * p[c];
-    rn[c] = rc;
-    x0[c] = om * rc / A.d[c];
-    TV r1 = ((TV)1 - om) * rc;
-    if (j < A.nJ) r1 += A.fE[c] * x0n(c + 1);
-    if (j > 1) r1 += A.fE[c - 1] * x0n(c - 1);
-    if (i < A.nI) r1 += A.fN[c] * x0n(c + A.P);
-    if (i > 1) r1 += A.fN[c - A.P] * x0n(c - A.P);
-    t[c] = r1;
-    y[c] = r1 / A.d[c];
-    return (double)rc * (double)rc;
-}
-
-// the same residual half for the first cycle (x0 stored already)
-template <typename TV>
-__device__ __forceinline__ void sa0_resid(const Sa0<TV>& A, TV om, const TV* b, const TV* x0, TV* t, TV* y, int i,
-                                          int j) {
-    const int c = i * A.P + j;
-    const TV r1 = ((TV)1 - om) * b[c] + A.fE[c] * x0[c + 1] + A.fE[c - 1] * x0[c - 1] + A.fN[c] * x0[c + A.P] +
-                  A.fN[c - A.P] * x0[c - A.P];
-    t[c] = r1;
-    y[c] = r1 / A.d[c];
-}
-
-// second half of the restriction into level 1, one aggregate:
-// b_c = sum over the aggregate of t - w A y, x_c = omega b_c / d_c
-template <typename TV>
-__device__ __forceinline__ void sa0_restrict(const Sa0<TV>& A, const TV* t, const TV* y, const SaLevel<TV>& C,
-                                             TV w, double omega, int I, int J) {
-    double s = 0.0;
-    const int i1 = min(3 * I, A.nI), j1 = min(3 * J, A.nJ);
-    for (int i = 3 * I - 2; i <= i1; ++i)
-        for (int j = 3 * J - 2; j <= j1; ++j) {
-            const int c = i * A.P + j;
-            const TV ay = A.d[c] * y[c] - A.fE[c] * y[c + 1] - A.fE[c - 1] * y[c - 1] - A.fN[c] * y[c + A.P] -
-                          A.fN[c - A.P] * y[c - A.P];
-            s += (double)(t[c] - w * ay);
+    auto dirv = [&](int q) -> SaVec<TV> {
+        SaVec<TV> a = sa_ld(z + q);
+        if (!first) {
+            const SaVec<TV> o = sa_ld(pold + q);
+#pragma unroll
+            for (int k = 0; k < V; ++k) a.v[k] = (TV)(a.v[k] + bt * o.v[k]);
         }
-    const int qc = I * C.P + J;
-    C.b[qc] = (TV)s;
-    C.x[qc] = (TV)(omega * s / (double)C.c[4][qc]);
+        return a;
+    };
+    SaVec<TV> pc = sa_zero<TV>(), pn = pc, ps = pc, d = pc, fe = pc, fn = pc, fs = pc;
+    if (act) {
+        pc = dirv(c);
+        pn = dirv(c + P);
+        ps = dirv(c - P);
+        d = sa_ld(A.d + c);
+        fe = sa_ld(A.fE + c);
+        fn = sa_ld(A.fN + c);
+        fs = sa_ld(A.fN + c - P);
+    }
+    TV pw = sa_from_west(pc.v[V - 1]), pe = sa_from_east(pc.v[0]), fw = sa_from_west(fe.v[V - 1]);
+    if (lane == 0) {
+        const bool h = act && j0 > 0;
+        pw = h ? dir(c - 1) : (TV)0;
+        fw = h ? A.fE[c - 1] : (TV)0;
+    }
+    if (lane == 31) pe = act ? dir(c + V) : (TV)0;
+    SaVec<TV> ap;
+    double acc = 0.0;
+#pragma unroll
+    for (int k = 0; k < V; ++k) {
+        const TV W = k ? pc.v[k - 1] : pw, E = k < V - 1 ? pc.v[k + 1] : pe, FW = k ? fe.v[k - 1] : fw;
+        TV a = d.v[k] * pc.v[k] - fe.v[k] * E - FW * W - fn.v[k] * pn.v[k] - fs.v[k] * ps.v[k];
+        if (j0 + k < 1 || j0 + k > A.nJ) a = (TV)0;
+        ap.v[k] = a;
+        acc += (double)pc.v[k] * (double)a;
+    }
+    if (act) {
+        sa_st(pnew + c, pc);
+        sa_st(Ap + c, ap);
+    }
+    return acc;
 }
 
-// prolongation from level 1 fused with the post-smoothing of level 0:
-// t = x0 + P e at the cell and its four neighbours ((P e)(m) = e(agg m) -
-// w / d_m (A e0)(m)), then y = t + omega (b - A t) / d.  Returns y.
+// CG update fused with the first half of the next restriction: x += alpha p,
+// r' = r - alpha Ap (into rn), the pre-smoothed level-0 iterate
+// x0' = omega r' / d, and the residual of the pre-smoothing
+// t = r' - A x0' = (1 - omega) r' + sum over the faces of f x0'(neighbour),
+// the neighbours' x0' recomputed from r and Ap.  Returns the group's |r'|^2.
 template <typename TV>
-__device__ __forceinline__ TV sa0_prolong(const Sa0<TV>& A, const TV* x0, const TV* b, const TV* e, int Pc, TV w,
-                                          TV om, int i, int j) {
-    auto E0 = [&](int ii, int jj) -> TV {
-        if (ii < 1 || ii > A.nI || jj < 1 || jj > A.nJ) return (TV)0;
-        return e[((ii - 1) / 3 + 1) * Pc + (jj - 1) / 3 + 1];
+__device__ __forceinline__ double sa0_update(const Sa0<TV>& A, TV al, TV om, const TV* __restrict__ p,
+                                             const TV* __restrict__ Ap, TV* __restrict__ x, const TV* __restrict__ r,
+                                             TV* __restrict__ rn, TV* __restrict__ x0, TV* __restrict__ t, int i,
+                                             int j0, bool act, int lane) {
+    constexpr int V = SaVec<TV>::n;
+    const int P = A.P, c = i * P + j0;
+    auto x0at = [&](int q) -> TV { return om * (r[q] - al * Ap[q]) * A.dinv[q]; };
+    auto x0v = [&](int q) -> SaVec<TV> {
+        const SaVec<TV> rr = sa_ld(r + q), aa = sa_ld(Ap + q), di = sa_ld(A.dinv + q);
+        SaVec<TV> o;
+#pragma unroll
+        for (int k = 0; k < V; ++k) o.v[k] = om * (rr.v[k] - al * aa.v[k]) * di.v[k];
+        return o;
     };
-    auto T = [&](int ii, int jj) -> TV {
+    SaVec<TV> rc = sa_zero<TV>(), xc = rc, xn = rc, xs = rc, xx = rc, pp = rc, fe = rc, fn = rc, fs = rc;
+    if (act) {
+        const SaVec<TV> rr = sa_ld(r + c), aa = sa_ld(Ap + c), di = sa_ld(A.dinv + c);
+#pragma unroll
+        for (int k = 0; k < V; ++k) {
+            rc.v[k] = rr.v[k] - al * aa.v[k];
+            xc.v[k] = om * rc.v[k] * di.v[k];
+        }
+        xn = x0v(c + P);
+        xs = x0v(c - P);
+        xx = sa_ld(x + c);
+        pp = sa_ld(p + c);
+        fe = sa_ld(A.fE + c);
+        fn = sa_ld(A.fN + c);
+        fs = sa_ld(A.fN + c - P);
+    }
+    TV xw = sa_from_west(xc.v[V - 1]), xe = sa_from_east(xc.v[0]), fw = sa_from_west(fe.v[V - 1]);
+    if (lane == 0) {
+        const bool h = act && j0 > 0;
+        xw = h ? x0at(c - 1) : (TV)0;
+        fw = h ? A.fE[c - 1] : (TV)0;
+    }
+    if (lane == 31) xe = act ? x0at(c + V) : (TV)0;
+    SaVec<TV> tt;
+    double acc = 0.0;
+#pragma unroll
+    for (int k = 0; k < V; ++k) {
+        const TV W = k ? xc.v[k - 1] : xw, E = k < V - 1 ? xc.v[k + 1] : xe, FW = k ? fe.v[k - 1] : fw;
+        TV t1 = ((TV)1 - om) * rc.v[k] + fe.v[k] * E + FW * W + fn.v[k] * xn.v[k] + fs.v[k] * xs.v[k];
+        if (j0 + k < 1 || j0 + k > A.nJ) t1 = (TV)0;
+        tt.v[k] = t1;
+        xx.v[k] = xx.v[k] + al * pp.v[k];
+        acc += (double)rc.v[k] * (double)rc.v[k];
+    }
+    if (act) {
+        sa_st(x + c, xx);
+        sa_st(rn + c, rc);
+        sa_st(x0 + c, xc);
+        sa_st(t + c, tt);
+    }
+    return acc;
+}
+
+// the same residual half for the first cycle, x0 = omega b / d stored:
+// t = (1 - omega) b + sum over the faces of f x0(neighbour)
+template <typename TV>
+__device__ __forceinline__ void sa0_resid(const Sa0<TV>& A, TV om, const TV* __restrict__ b,
+                                          const TV* __restrict__ x0, TV* __restrict__ t, int i, int j0, bool act,
+                                          int lane) {
+    constexpr int V = SaVec<TV>::n;
+    const int P = A.P, c = i * P + j0;
+    SaVec<TV> xc = sa_zero<TV>(), xn = xc, xs = xc, bb = xc, fe = xc, fn = xc, fs = xc;
+    if (act) {
+        xc = sa_ld(x0 + c);
+        xn = sa_ld(x0 + c + P);
+        xs = sa_ld(x0 + c - P);
+        bb = sa_ld(b + c);
+        fe = sa_ld(A.fE + c);
+        fn = sa_ld(A.fN + c);
+        fs = sa_ld(A.fN + c - P);
+    }
+    TV xw = sa_from_west(xc.v[V - 1]), xe = sa_from_east(xc.v[0]), fw = sa_from_west(fe.v[V - 1]);
+    if (lane == 0) {
+        const bool h = act && j0 > 0;
+        xw = h ? x0[c - 1] : (TV)0;
+        fw = h ? A.fE[c - 1] : (TV)0;
+    }
+    if (lane == 31) xe = act ? x0[c + V] : (TV)0;
+    SaVec<TV> tt;
+#pragma unroll
+    for (int k = 0; k < V; ++k) {
+        const TV W = k ? xc.v[k - 1] : xw, E = k < V - 1 ? xc.v[k + 1] : xe, FW = k ? fe.v[k - 1] : fw;
+        TV t1 = ((TV)1 - om) * bb.v[k] + fe.v[k] * E + FW * W + fn.v[k] * xn.v[k] + fs.v[k] * xs.v[k];
+        if (j0 + k < 1 || j0 + k > A.nJ) t1 = (TV)0;
+        tt.v[k] = t1;
+    }
+    if (act) sa_st(t + c, tt);
+}
+
+// prolongation from level 1 fused with level 0's post-smoothing:
+// t = x0 + P e on the lane group and its neighbours (P e = pO e(own) +
+// pH e(horizontal) + pV e(vertical)), then
+// y = t + omega (b - A t) / d = (1 - omega) t + omega (b + sum f t(nb)) / d.
+// Writes y, returns the group's share of b.y.
+template <typename TV>
+__device__ __forceinline__ double sa0_prolong(const Sa0<TV>& A, const TV* __restrict__ x0, const TV* __restrict__ b,
+                                              const TV* __restrict__ e, int Pc, TV om, TV* __restrict__ y, int i,
+                                              int j0, bool act, int lane) {
+    constexpr int V = SaVec<TV>::n;
+    const int P = A.P, c = i * P + j0;
+    // t at (ii, jj) from its x0 and weights; 0 outside the unknowns
+    auto tat = [&](int ii, int jj, TV xv, TV po, TV ph, TV pv) -> TV {
         if (ii < 1 || ii > A.nI || jj < 1 || jj > A.nJ) return (TV)0;
-        const int q = ii * A.P + jj;
-        const TV ec = E0(ii, jj);
-        const TV ae = A.d[q] * ec - A.fE[q] * E0(ii, jj + 1) - A.fE[q - 1] * E0(ii, jj - 1) -
-                      A.fN[q] * E0(ii + 1, jj) - A.fN[q - A.P] * E0(ii - 1, jj);
-        return x0[q] + ec - w * ae / A.d[q];
+        const TV* er = e + ((ii - 1) / 3 + 1) * Pc + (jj - 1) / 3 + 1;
+        return xv + po * er[0] + ph * er[sa_side(jj)] + pv * er[sa_side(ii) * Pc];
     };
-    const int c = i * A.P + j;
-    const TV tc = T(i, j);
-    const TV at = A.d[c] * tc - A.fE[c] * T(i, j + 1) - A.fE[c - 1] * T(i, j - 1) - A.fN[c] * T(i + 1, j) -
-                  A.fN[c - A.P] * T(i - 1, j);
-    return tc + om * (b[c] - at) / A.d[c];
+    auto trow = [&](int ii) -> SaVec<TV> {
+        const int q = ii * P + j0;
+        const SaVec<TV> xv = sa_ld(x0 + q), po = sa_ld(A.pO + q), ph = sa_ld(A.pH + q), pv = sa_ld(A.pV + q);
+        SaVec<TV> o;
+#pragma unroll
+        for (int k = 0; k < V; ++k) o.v[k] = tat(ii, j0 + k, xv.v[k], po.v[k], ph.v[k], pv.v[k]);
+        return o;
+    };
+    auto tone = [&](int q, int jj) -> TV { return tat(i, jj, x0[q], A.pO[q], A.pH[q], A.pV[q]); };
+    SaVec<TV> tc = sa_zero<TV>(), tn = tc, ts = tc, bb = tc, di = tc, fe = tc, fn = tc, fs = tc;
+    if (act) {
+        tc = trow(i);
+        tn = trow(i + 1);
+        ts = trow(i - 1);
+        bb = sa_ld(b + c);
+        di = sa_ld(A.dinv + c);
+        fe = sa_ld(A.fE + c);
+        fn = sa_ld(A.fN + c);
+        fs = sa_ld(A.fN + c - P);
+    }
+    TV tw = sa_from_west(tc.v[V - 1]), te = sa_from_east(tc.v[0]), fw = sa_from_west(fe.v[V - 1]);
+    if (lane == 0) {
+        const bool h = act && j0 > 0;
+        tw = h ? tone(c - 1, j0 - 1) : (TV)0;
+        fw = h ? A.fE[c - 1] : (TV)0;
+    }
+    if (lane == 31) te = act ? tone(c + V, j0 + V) : (TV)0;
+    SaVec<TV> yv;
+    double acc = 0.0;
+#pragma unroll
+    for (int k = 0; k < V; ++k) {
+        const TV W = k ? tc.v[k - 1] : tw, E = k < V - 1 ? tc.v[k + 1] : te, FW = k ? fe.v[k - 1] : fw;
+        TV yk = ((TV)1 - om) * tc.v[k] +
+                om * di.v[k] * (bb.v[k] + fe.v[k] * E + FW * W + fn.v[k] * tn.v[k] + fs.v[k] * ts.v[k]);
+        if (j0 + k < 1 || j0 + k > A.nJ) yk = (TV)0;
+        yv.v[k] = yk;
+        acc += (double)bb.v[k] * (double)yk;
+    }
+    if (act) sa_st(y + c, yv);
+    return acc;
+}
+
+// the same prolongation in two passes: t = x0 + P e on the lane group, then
+// (after a grid barrier) the post-smoothing from t; returns b.y
+template <typename TV>
+__device__ __forceinline__ void sa0_prolong_t(const Sa0<TV>& A, const TV* __restrict__ x0, const TV* __restrict__ e,
+                                              int Pc, TV* __restrict__ t, int i, int j0, bool act) {
+    constexpr int V = SaVec<TV>::n;
+    if (!act) return;
+    const int c = i * A.P + j0;
+    const SaVec<TV> xv = sa_ld(x0 + c), po = sa_ld(A.pO + c), ph = sa_ld(A.pH + c), pv = sa_ld(A.pV + c);
+    const int I = (i - 1) / 3 + 1, sv = sa_side(i) * Pc;
+    SaVec<TV> o;
+#pragma unroll
+    for (int k = 0; k < V; ++k) {
+        const int jj = j0 + k;
+        TV tk = (TV)0;
+        if (jj >= 1 && jj <= A.nJ) {
+            const TV* er = e + I * Pc + (jj - 1) / 3 + 1;
+            tk = xv.v[k] + po.v[k] * er[0] + ph.v[k] * er[sa_side(jj)] + pv.v[k] * er[sv];
+        }
+        o.v[k] = tk;
+    }
+    sa_st(t + c, o);
+}
+template <typename TV>
+__device__ __forceinline__ double sa0_smooth(const Sa0<TV>& A, TV om, const TV* __restrict__ b,
+                                             const TV* __restrict__ t, TV* __restrict__ y, int i, int j0, bool act,
+                                             int lane) {
+    constexpr int V = SaVec<TV>::n;
+    const int P = A.P, c = i * P + j0;
+    SaVec<TV> tc = sa_zero<TV>(), tn = tc, ts = tc, bb = tc, di = tc, fe = tc, fn = tc, fs = tc;
+    if (act) {
+        tc = sa_ld(t + c);
+        tn = sa_ld(t + c + P);
+        ts = sa_ld(t + c - P);
+        bb = sa_ld(b + c);
+        di = sa_ld(A.dinv + c);
+        fe = sa_ld(A.fE + c);
+        fn = sa_ld(A.fN + c);
+        fs = sa_ld(A.fN + c - P);
+    }
+    TV tw = sa_from_west(tc.v[V - 1]), te = sa_from_east(tc.v[0]), fw = sa_from_west(fe.v[V - 1]);
+    if (lane == 0) {
+        const bool h = act && j0 > 0;
+        tw = h ? t[c - 1] : (TV)0;
+        fw = h ? A.fE[c - 1] : (TV)0;
+    }
+    if (lane == 31) te = act ? t[c + V] : (TV)0;
+    SaVec<TV> yv;
+    double acc = 0.0;
+#pragma unroll
+    for (int k = 0; k < V; ++k) {
+        const TV W = k ? tc.v[k - 1] : tw, E = k < V - 1 ? tc.v[k + 1] : te, FW = k ? fe.v[k - 1] : fw;
+        TV yk = ((TV)1 - om) * tc.v[k] +
+                om * di.v[k] * (bb.v[k] + fe.v[k] * E + FW * W + fn.v[k] * tn.v[k] + fs.v[k] * ts.v[k]);
+        if (j0 + k < 1 || j0 + k > A.nJ) yk = (TV)0;
+        yv.v[k] = yk;
+        acc += (double)bb.v[k] * (double)yk;
+    }
+    if (act) sa_st(y + c, yv);
+    return acc;
 }
 
 // ---------------------------------------------------------------- the solver
@@ -438,7 +821,7 @@ __global__ void __launch_bounds__(512, 1) k_pcg_sa(KParams k, Status* st, const 
     const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = G * blockDim.x;
     const SaSplit all{tid, nth}, cta{(int)threadIdx.x, (int)blockDim.x};
     const double rho = k.rho, hx = k.hx, hy = k.hy, om = H.omega;
-    const TV omT = (TV)om, w0T = (TV)H.w0;
+    const TV omT = (TV)om;
     unsigned target = 0;
     double* partA = part;
     double* partB = part + G;
@@ -448,13 +831,14 @@ __global__ void __launch_bounds__(512, 1) k_pcg_sa(KParams k, Status* st, const 
         if (!grid_barrier(bar, target, &st->err)) return;           \
     } while (0)
     // the coarse operators are rebuilt every H.reuse outer iterations (they
-    // only precondition: the CG matvec always uses the current level 0), and
-    // whenever the stored ones are not the forward's
+    // only precondition: the CG matvec and level 0's smoother and
+    // prolongation always use the current operator), and whenever the stored
+    // ones are not the forward's
     const bool rebuild = H.force || *(volatile int*)H.dirty || H.reuse <= 1 || (st->iter % H.reuse) == 0;
 
     SaLevel<TV> L0 = H.lv[0];
     L0.b = B.r;
-    const Sa0<TV> A0f{B.fE, B.fN, B.d, M - 1, w, d.P};
+    const Sa0<TV> A0f{B.fE, B.fN, B.d, H.dinv0, L0.pw[0], L0.pw[1], L0.pw[2], M - 1, w, d.P};
     const Stencil5<TV> A0{B.fE, B.fN, B.d, M - 1, w, d.P};
     auto stencil = [&](int l) { return Stencil9<TV>{H.lv[l].c, H.lv[l].nI, H.lv[l].nJ, H.lv[l].P}; };
     auto wgt = [&](int l) { return l == 0 ? H.w0 : H.wc; };
@@ -467,8 +851,8 @@ __global__ void __launch_bounds__(512, 1) k_pcg_sa(KParams k, Status* st, const 
         }
     };
 
-    // ---- set-up: level-0 operator (the reference's formulas), x = 0, r = b,
-    // x0 = omega r / d
+    // ---- set-up: level-0 operator (the reference's formulas), its inverse
+    // diagonal and prolongation weights, x = 0, r = b, x0 = omega r / d
     double bb[1] = {0.0};
     for (int t = tid; t < n; t += nth) {
         const int i = 1 + t / w, j = 1 + t % w;
@@ -482,6 +866,19 @@ __global__ void __launch_bounds__(512, 1) k_pcg_sa(KParams k, Status* st, const 
         B.fE[c] = (TV)aE;
         B.fN[c] = (TV)aN;
         B.d[c] = (TV)aP;
+        // faces towards unknowns of the own aggregate, and towards the
+        // horizontal / vertical neighbour aggregate (the east face of the
+        // last column is the Dirichlet outlet, with no unknown behind it)
+        const int ri = (i - 1) % 3, rj = (j - 1) % 3;
+        const double eIn = (j < w) ? aE : 0.0;
+        const double same = (rj != 2 ? eIn : 0.0) + (rj != 0 ? aW : 0.0) + (ri != 2 ? aN : 0.0) + (ri != 0 ? aS : 0.0);
+        const double fh = rj == 0 ? aW : (rj == 2 ? eIn : 0.0);
+        const double fv = ri == 0 ? aS : (ri == 2 ? aN : 0.0);
+        const double sc = H.w0 / aP;
+        H.dinv0[c] = (TV)(1.0 / aP);
+        L0.pw[0][c] = (TV)(1.0 - sc * (aP - same));
+        L0.pw[1][c] = (TV)(sc * fh);
+        L0.pw[2][c] = (TV)(sc * fv);
         B.x[c] = (TV)0;
         const TV rt = B.rhs[c];
         B.r[c] = rt;
@@ -496,15 +893,28 @@ __global__ void __launch_bounds__(512, 1) k_pcg_sa(KParams k, Status* st, const 
     const double rTol = k.pTol * sqrt(bnorm2[0]);
     tick(SA_P_SETUP);
 
-    // ---- set-up: coarse operators by coloured probes (when rebuilt)
+    // ---- set-up: coarse operators by coloured probes (when rebuilt), with
+    // the prolongation weights of the grid-wide coarse levels
     if (rebuild) {
         for (int l = 0; l < H.L - 1; ++l) {
             const bool grid = l < H.Lg;
             if (!grid && blockIdx.x != 0) continue;
             const SaSplit sp = grid ? all : cta;
             const SaLevel<TV>& f = H.lv[l];
-            if (l == 0) sa_cells(sp, f.nI, f.nJ, [&](int i, int j) { sa_probe_cell(A0, f.P, H.Y, wgt(l), i, j); });
-            else sa_cells(sp, f.nI, f.nJ, [&](int i, int j) { sa_probe_cell(stencil(l), f.P, H.Y, wgt(l), i, j); });
+            if (l == 0) {
+                sa_cells(sp, f.nI, f.nJ, [&](int i, int j) { sa_probe_cell(A0, f.P, H.Y, wgt(l), i, j); });
+            } else {
+                sa_cells(sp, f.nI, f.nJ, [&](int i, int j) {
+                    sa_probe_cell(stencil(l), f.P, H.Y, wgt(l), i, j);
+                    if (grid) {
+                        double pw[4];
+                        sa_pweights(stencil(l), i, j, wgt(l), pw);
+                        const size_t q = (size_t)i * f.P + j;
+#pragma unroll
+                        for (int m = 0; m < 4; ++m) f.pw[m][q] = (TV)pw[m];
+                    }
+                });
+            }
             if (grid) SA_SYNC(); else __syncthreads();
             const SaLevel<TV>& C = H.lv[l + 1];
             if (l == 0)
@@ -519,65 +929,125 @@ __global__ void __launch_bounds__(512, 1) k_pcg_sa(KParams k, Status* st, const 
     }
     tick(SA_P_GALERKIN);
 
-    // levels >= 1: restriction l -> l+1 and prolongation l+1 -> l with
-    // post-smoothing, two passes each, on the grid or on CTA 0
-    auto restrict_level = [&](int l, bool grid) -> bool {
-        const SaSplit sp = grid ? all : cta;
+    // ---- CTA 0 stages levels [Lg, L) (operators copied, vectors zeroed,
+    // frames included) and the dense inverse in shared memory
+    TV* const smb = reinterpret_cast<TV*>(dsm);
+    TV* sInv = nullptr;
+    if (blockIdx.x == 0) {
+        for (int l = H.Lg; l < H.L; ++l) {
+            const SaLevel<TV>& g = H.lv[l];
+            const SaSm<TV> f = sa_sm(H, smb, l);
+            for (int e = threadIdx.x; e < 9 * f.ne; e += blockDim.x) {
+                const int q = e / f.ne, r = e - q * f.ne, ii = r / f.P, jj = r - ii * f.P;
+                f.s[e] = g.c[q][(size_t)ii * g.P + jj];
+            }
+            for (int e = 9 * f.ne + threadIdx.x; e < 13 * f.ne; e += blockDim.x) f.s[e] = (TV)0;
+            sInv = f.s + 13 * f.ne;
+        }
+        const int nd = H.lv[H.L - 1].nI * H.lv[H.L - 1].nJ;
+        for (int e = threadIdx.x; e < nd * nd; e += blockDim.x) sInv[e] = H.dense[e];
+        __syncthreads();
+    }
+
+    // grid-wide coarse levels: restriction l -> l+1 and prolongation
+    // l+1 -> l with post-smoothing, two passes each
+    auto restrict_level = [&](int l) -> bool {
         const SaLevel<TV>& f = H.lv[l];
         const SaLevel<TV>& C = H.lv[l + 1];
-        sa_cells(sp, f.nI, f.nJ, [&](int i, int j) { sa_resid_cell(stencil(l), f, i, j); });
-        if (grid) { target += G; if (!grid_barrier(bar, target, &st->err)) return false; } else __syncthreads();
-        sa_cells(sp, C.nI, C.nJ, [&](int I, int J) { sa_restrict_cell(stencil(l), f, C, wgt(l), om, I, J); });
-        if (grid) { target += G; if (!grid_barrier(bar, target, &st->err)) return false; } else __syncthreads();
-        return true;
+        sa_cells(all, f.nI, f.nJ, [&](int i, int j) { sa_resid_cell(f, i, j); });
+        target += G;
+        if (!grid_barrier(bar, target, &st->err)) return false;
+        sa_cells(all, C.nI, C.nJ, [&](int I, int J) { sa_restrict_w<TV, true>(f, C, om, I, J); });
+        target += G;
+        return grid_barrier(bar, target, &st->err);
     };
-    auto prolong_level = [&](int l, bool grid) -> bool {
-        const SaSplit sp = grid ? all : cta;
+    auto prolong_level = [&](int l) -> bool {
         const SaLevel<TV>& f = H.lv[l];
         const SaLevel<TV>& C = H.lv[l + 1];
-        sa_cells(sp, f.nI, f.nJ, [&](int i, int j) { sa_prolong_cell(stencil(l), f, C.y, C.P, wgt(l), i, j); });
-        if (grid) { target += G; if (!grid_barrier(bar, target, &st->err)) return false; } else __syncthreads();
-        sa_cells(sp, f.nI, f.nJ, [&](int i, int j) { sa_smooth_cell(stencil(l), f, om, i, j); });
-        if (grid) { target += G; if (!grid_barrier(bar, target, &st->err)) return false; } else __syncthreads();
-        return true;
+        sa_cells(all, f.nI, f.nJ, [&](int i, int j) { sa_prolong_w(f, C.y, C.P, i, j); });
+        target += G;
+        if (!grid_barrier(bar, target, &st->err)) return false;
+        sa_cells(all, f.nI, f.nJ, [&](int i, int j) { sa_smooth_cell(f, om, i, j); });
+        target += G;
+        return grid_barrier(bar, target, &st->err);
     };
-    // ---- z = M r (V-cycle) with r = L0.b; level 0's residual half (t, y)
-    // is done already (by the CG update, or by `first`); z in L0.y is
-    // overwritten by the prolongation; rz = r.z
+    // CTA 0: levels [Lg, L) in shared memory, between the copy of level Lg's
+    // rhs and pre-smoothed iterate in and of its corrected iterate out
+    auto cta_levels = [&]() {
+        const SaLevel<TV>& Gl = H.lv[H.Lg];
+        const SaSm<TV> S0 = sa_sm(H, smb, H.Lg);
+        for (int a = threadIdx.x; a < Gl.nI * Gl.nJ; a += blockDim.x) {
+            const int i = 1 + a / Gl.nJ, j = 1 + a % Gl.nJ;
+            S0.b()[i * S0.P + j] = Gl.b[(size_t)i * Gl.P + j];
+            S0.x()[i * S0.P + j] = Gl.x[(size_t)i * Gl.P + j];
+        }
+        __syncthreads();
+        const TV wc = (TV)H.wc, omc = (TV)om;
+        for (int l = H.Lg; l < H.L - 1; ++l) {
+            const SaSm<TV> f = sa_sm(H, smb, l), C = sa_sm(H, smb, l + 1);
+            sa_cells(cta, f.nI, f.nJ, [&](int i, int j) { sa_sm_resid(f, i, j); });
+            __syncthreads();
+            sa_cells(cta, f.nI, f.nJ, [&](int i, int j) { sa_sm_smoothres(f, wc, i, j); });
+            __syncthreads();
+            sa_cells(cta, C.nI, C.nJ, [&](int I, int J) { sa_sm_aggsum(f, C, omc, I, J); });
+            __syncthreads();
+        }
+        sa_sm_dense(sa_sm(H, smb, H.L - 1), sInv);
+        for (int l = H.L - 2; l >= H.Lg; --l) {
+            const SaSm<TV> f = sa_sm(H, smb, l), C = sa_sm(H, smb, l + 1);
+            sa_cells(cta, f.nI, f.nJ, [&](int i, int j) { sa_sm_prolong(f, C, wc, i, j); });
+            __syncthreads();
+            sa_cells(cta, f.nI, f.nJ, [&](int i, int j) { sa_sm_smooth(f, omc, i, j); });
+            __syncthreads();
+        }
+        for (int a = threadIdx.x; a < Gl.nI * Gl.nJ; a += blockDim.x) {
+            const int i = 1 + a / Gl.nJ, j = 1 + a % Gl.nJ;
+            Gl.y[(size_t)i * Gl.P + j] = S0.y()[i * S0.P + j];
+        }
+    };
+    // ---- z = M r (V-cycle) with r = L0.b; level 0's residual half t is done
+    // already (by the CG update, or here when `first`); z goes to L0.y;
+    // rz = r.z
     const SaLevel<TV>& C1 = H.lv[1];
-    auto vcycle = [&](double& rz, bool first) -> bool {
+    auto vcycle = [&](double& rz, bool first) __attribute__((always_inline)) -> bool {
         if (first) {
-            sa_cells(all, L0.nI, L0.nJ, [&](int i, int j) { sa0_resid(A0f, omT, L0.b, L0.x, L0.t, L0.y, i, j); });
+            sa_rows<TV>(L0.nI, L0.nJ, [&](int i, int j0, bool act, int lane) {
+                sa0_resid(A0f, omT, L0.b, L0.x, L0.t, i, j0, act, lane);
+            });
             target += G;
             if (!grid_barrier(bar, target, &st->err)) return false;
         }
-        sa_cells(all, C1.nI, C1.nJ, [&](int I, int J) { sa0_restrict(A0f, L0.t, L0.y, C1, w0T, om, I, J); });
+        sa_cells(all, C1.nI, C1.nJ, [&](int I, int J) { sa_restrict_w<TV, false>(L0, C1, om, I, J); });
         target += G;
         if (!grid_barrier(bar, target, &st->err)) return false;
         tick(SA_P_DOWN);
         for (int l = 1; l < H.Lg; ++l) {
-            if (!restrict_level(l, true)) return false;
+            if (!restrict_level(l)) return false;
             tick(SA_P_DOWN + l);
         }
-        if (blockIdx.x == 0) {
-            for (int l = H.Lg; l < H.L - 1; ++l) restrict_level(l, false);
-            sa_dense_solve(H.lv[H.L - 1], H.dense);
-            for (int l = H.L - 2; l >= H.Lg; --l) prolong_level(l, false);
-        }
+        if (blockIdx.x == 0) cta_levels();
         target += G;
         if (!grid_barrier(bar, target, &st->err)) return false;
         tick(SA_P_CTA);
         for (int l = H.Lg - 1; l >= 1; --l) {
-            if (!prolong_level(l, true)) return false;
+            if (!prolong_level(l)) return false;
             tick(SA_P_UP + l);
         }
         double acc[1] = {0.0};
-        sa_cells(all, L0.nI, L0.nJ, [&](int i, int j) {
-            const TV y = sa0_prolong(A0f, L0.x, L0.b, C1.y, C1.P, w0T, omT, i, j);
-            const int c = i * L0.P + j;
-            L0.y[c] = y;
-            acc[0] += (double)L0.b[c] * (double)y;
-        });
+        if (H.split0) {
+            sa_rows<TV>(L0.nI, L0.nJ, [&](int i, int j0, bool act, int lane) {
+                sa0_prolong_t(A0f, L0.x, C1.y, C1.P, L0.t, i, j0, act);
+            });
+            target += G;
+            if (!grid_barrier(bar, target, &st->err)) return false;
+            sa_rows<TV>(L0.nI, L0.nJ, [&](int i, int j0, bool act, int lane) {
+                acc[0] += sa0_smooth(A0f, omT, L0.b, L0.t, L0.y, i, j0, act, lane);
+            });
+        } else {
+            sa_rows<TV>(L0.nI, L0.nJ, [&](int i, int j0, bool act, int lane) {
+                acc[0] += sa0_prolong(A0f, L0.x, L0.b, C1.y, C1.P, omT, L0.y, i, j0, act, lane);
+            });
+        }
         block_sum<1>(acc, sm);
         if (threadIdx.x == 0) partB[2 * blockIdx.x + 1] = acc[0];
         target += G;
@@ -596,13 +1066,14 @@ __global__ void __launch_bounds__(512, 1) k_pcg_sa(KParams k, Status* st, const 
     TV* pbuf[2] = {B.pa, B.pb};
     TV* rbuf[2] = {B.r, H.r2};
     for (; it < k.maxP; ++it) {
-        TV* __restrict__ pnew = pbuf[it & 1];
+        TV* pnew = pbuf[it & 1];
         const TV* pold = pbuf[(it + 1) & 1];
         const TV bt = (TV)beta;
         const bool first = it == 0;
         double accA[1] = {0.0};
-        sa_cells(all, L0.nI, L0.nJ,
-                 [&](int i, int j) { accA[0] += sa0_matvec(A0f, L0.y, pold, bt, first, pnew, B.Ap, i, j); });
+        sa_rows<TV>(L0.nI, L0.nJ, [&](int i, int j0, bool act, int lane) {
+            accA[0] += sa0_matvec(A0f, L0.y, pold, bt, first, pnew, B.Ap, i, j0, act, lane);
+        });
         block_sum<1>(accA, sm);
         if (threadIdx.x == 0) partA[blockIdx.x] = accA[0];
         SA_SYNC();
@@ -614,8 +1085,8 @@ __global__ void __launch_bounds__(512, 1) k_pcg_sa(KParams k, Status* st, const 
         const TV* rold = rbuf[it & 1];
         TV* rnew = rbuf[(it + 1) & 1];
         double accB[1] = {0.0};
-        sa_cells(all, L0.nI, L0.nJ, [&](int i, int j) {
-            accB[0] += sa0_update(A0f, al, omT, pnew, B.Ap, B.x, rold, rnew, L0.x, L0.t, L0.y, i, j);
+        sa_rows<TV>(L0.nI, L0.nJ, [&](int i, int j0, bool act, int lane) {
+            accB[0] += sa0_update(A0f, al, omT, pnew, B.Ap, B.x, rold, rnew, L0.x, L0.t, i, j0, act, lane);
         });
         L0.b = rnew;
         block_sum<1>(accB, sm);

@@ -111,12 +111,17 @@ struct cp_ctx {
     bool useSa = false;
     int saL = 0, saLg = 0;
     int saNI[kSaMaxLevels] = {}, saNJ[kSaMaxLevels] = {}, saP[kSaMaxLevels] = {};
-    void* saArr[kSaMaxLevels][13] = {};     // c[0..8] x y b t (level 0: x y t only)
+    // per level: c[0..8] x y b t pw[0..3] (level 0: x y b t and pw[0..2];
+    // pw only on levels that run grid-wide and have a coarser one)
+    void* saArr[kSaMaxLevels][17] = {};
+    void* saDinv0 = nullptr;                 // level-0 inverse diagonal
+    size_t saSmem = 0;                       // k_pcg_sa's dynamic shared memory (bytes)
     void* saY[9] = {};
     void* saDense = nullptr;
     double saOmega = 0.9, saW0 = 2.0 / 3.0, saWc = 0.8;
     unsigned long long* saProf = nullptr;    // per-phase timers when CP_SA_PROFILE is set
     int saReuse = 8;                         // outer iterations between coarse-operator rebuilds
+    int saSplit0 = 1;                        // level-0 prolongation in two passes
     int* saDirty = nullptr;                  // device flag: rebuild the coarse operators on the next solve
     MgMaps mgMaps;                           // TMA tensor maps of the level-0 tile phases
     // adjoint buffers (allocated on first use, double)
@@ -491,7 +496,9 @@ SaHier<TV> sa_hier(cp_ctx* c) {
     H.dense = (TV*)c->saDense;
     H.prof = c->saProf;
     H.r2 = (TV*)c->saArr[0][11];
+    H.dinv0 = (TV*)c->saDinv0;
     H.reuse = c->saReuse;
+    H.split0 = c->saSplit0;
     H.force = 0;
     H.dirty = c->saDirty;
     for (int q = 0; q < 9; ++q) H.Y[q] = (TV*)c->saY[q];
@@ -501,17 +508,21 @@ SaHier<TV> sa_hier(cp_ctx* c) {
         TV** a = reinterpret_cast<TV**>(c->saArr[l]);
         for (int q = 0; q < 9; ++q) v.c[q] = a[q];
         v.x = a[9]; v.y = a[10]; v.b = a[11]; v.t = a[12];
+        for (int q = 0; q < 4; ++q) v.pw[q] = a[13 + q];
     }
     return H;
 }
 
-// dynamic shared memory of k_pcg_sa: the dense set-up workspace
+// dynamic shared memory of k_pcg_sa: the dense set-up workspace, then CTA
+// 0's staged levels (at most kSaSmemBudget bytes)
 constexpr size_t kSaDynSmem = sizeof(double) * (size_t)(kSaDense * 2 * kSaDense + kSaDense);
-static_assert(kSaDynSmem + 4096 <= 227 * 1024, "k_pcg_sa's dynamic shared memory exceeds a block's limit");
+constexpr size_t kSaSmemMax = kSaDynSmem > kSaSmemBudget ? kSaDynSmem : kSaSmemBudget;
+static_assert(kSaSmemMax + 4096 <= 227 * 1024, "k_pcg_sa's dynamic shared memory exceeds a block's limit");
 
 // Level sizes of the smoothed aggregation: 3 x 3 aggregates (rounding up)
-// until at most kSaDense unknowns; levels above kSaCtaCells unknowns (and
-// always level 0) run grid-wide.
+// until at most kSaDense unknowns.  Level 0 and the levels above kSaCtaCells
+// unknowns run grid-wide, and so do further levels until the rest fits CTA
+// 0's shared-memory budget.
 cp_status sa_build(cp_ctx* c) {
     int nI = c->d.M - 1, nJ = c->d.N - 2;
     int L = 0;
@@ -524,14 +535,19 @@ cp_status sa_build(cp_ctx* c) {
     }
     c->saL = L;
     int Lg = 1;
-    while (Lg < L && (long long)c->saNI[Lg] * c->saNJ[Lg] > kSaCtaCells) ++Lg;
+    while (Lg < L - 1 && ((long long)c->saNI[Lg] * c->saNJ[Lg] > kSaCtaCells ||
+                          sa_cta_elems(c->saNI, c->saNJ, Lg, L) * c->es > kSaSmemBudget))
+        ++Lg;
     c->saLg = Lg;
+    c->saSmem = std::max(kSaDynSmem, sa_cta_elems(c->saNI, c->saNJ, Lg, L) * c->es);
+    if (c->saSmem > kSaSmemMax) return fail(CP_ERR_BAD_PARAM, "smoothed-aggregation coarsest level too large");
     c->saP[0] = c->d.P;
     cp_status s;
     // level 0: pre-smoothed iterate, corrected iterate, the second CG
     // residual buffer (its rhs is the CG residual), scratch
-    for (int q = 9; q <= 12; ++q)
+    for (int q = 9; q <= 15; ++q)
         if ((s = dalloc_bytes(c, &c->saArr[0][q], c->nElem * c->es)) != CP_OK) return s;
+    if ((s = dalloc_bytes(c, &c->saDinv0, c->nElem * c->es)) != CP_OK) return s;
     if ((s = dalloc(c, &c->saDirty, 1)) != CP_OK) return s;
     const int one = 1;
     CK(cudaMemcpyAsync(c->saDirty, &one, sizeof(int), cudaMemcpyHostToDevice, c->stream));
@@ -539,7 +555,8 @@ cp_status sa_build(cp_ctx* c) {
     for (int l = 1; l < L; ++l) {
         c->saP[l] = ((c->saNJ[l] + 2 + 31) / 32) * 32;
         const size_t ne = (size_t)(c->saNI[l] + 2) * c->saP[l];
-        for (int q = 0; q < 13; ++q)
+        const int nq = (l < Lg && l < L - 1) ? 17 : 13;
+        for (int q = 0; q < nq; ++q)
             if ((s = dalloc_bytes(c, &c->saArr[l][q], ne * c->es)) != CP_OK) return s;
     }
     for (int q = 0; q < 9; ++q)
@@ -549,14 +566,15 @@ cp_status sa_build(cp_ctx* c) {
     if (const char* e = getenv("CP_SA_W0")) c->saW0 = atof(e);
     if (const char* e = getenv("CP_SA_WC")) c->saWc = atof(e);
     if (const char* e = getenv("CP_SA_REUSE")) c->saReuse = std::max(atoi(e), 1);
+    if (const char* e = getenv("CP_SA_SPLIT0")) c->saSplit0 = atoi(e) != 0;
     if (getenv("CP_SA_PROFILE") && (s = dalloc(c, &c->saProf, (size_t)SA_P_COUNT)) != CP_OK) return s;
     int nb = 0;
     if (c->prm.precision == CP_PREC_MIXED) {
-        cudaFuncSetAttribute(k_pcg_sa<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSaDynSmem);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_pcg_sa<float>, kMgThreads, kSaDynSmem);
+        cudaFuncSetAttribute(k_pcg_sa<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSaSmemMax);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_pcg_sa<float>, kMgThreads, c->saSmem);
     } else {
-        cudaFuncSetAttribute(k_pcg_sa<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSaDynSmem);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_pcg_sa<double>, kMgThreads, kSaDynSmem);
+        cudaFuncSetAttribute(k_pcg_sa<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSaSmemMax);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_pcg_sa<double>, kMgThreads, c->saSmem);
     }
     if (nb < 1) return fail(CP_ERR_CUDA, "smoothed-aggregation PCG kernel does not fit on an SM");
     return CP_OK;
@@ -606,7 +624,7 @@ cp_status enqueue_pressure(cp_ctx* c, EvRec* rec = nullptr) {
     REC_BEGIN(rec, CP_K_PCG);
     if (c->useSa) {
         SaHier<TV> H = sa_hier<TV>(c);
-        CK(launch_coop_cfg(k_pcg_sa<TV>, c->gMg, kMgThreads, kSaDynSmem, c->stream, c->k, c->st,
+        CK(launch_coop_cfg(k_pcg_sa<TV>, c->gMg, kMgThreads, c->saSmem, c->stream, c->k, c->st,
                            (const double*)c->dE, (const double*)c->dN, B, H, c->pStar, c->partP, c->barP));
     } else if (c->useMg) {
         MgHier<TV> H = mg_hier<TV>(c);
@@ -1211,7 +1229,7 @@ cp_status adjoint_pcg(cp_ctx* c, const KParams& k, const double* dE, const doubl
     if (c->useSa) {
         SaHier<TV> H = sa_hier<TV>(c);
         H.force = 1;   // the adjoint's operator: rebuild, and leave the forward's marked stale
-        CK(launch_coop_cfg(k_pcg_sa<TV>, c->gMg, kMgThreads, kSaDynSmem, c->stream, k, c->adjSt, dE, dN, B, H, out,
+        CK(launch_coop_cfg(k_pcg_sa<TV>, c->gMg, kMgThreads, c->saSmem, c->stream, k, c->adjSt, dE, dN, B, H, out,
                            c->adjPart, c->adjBar));
     } else if (c->useMg) {
         MgHier<TV> H = mg_hier<TV>(c);
