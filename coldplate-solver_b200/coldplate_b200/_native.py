@@ -128,6 +128,8 @@ SIGNATURES = {
     "cp_momentum_v": (_I, [_vp, _dp, _ip]),
     "cp_pressure": (_I, [_vp, _ip, _dp]),
     "cp_adjoint_dp_dgamma": (_I, [_vp, _dp, _L, _L, _L, _L, _I, _D, ctypes.POINTER(CpAdjointReport)]),
+    "cp_adjoint_probe_len": (ctypes.c_size_t, [_vp]),
+    "cp_adjoint_probe": (_I, [_vp, _I, _dp, _dp, _I, _D, _ip, ctypes.POINTER(CpAdjointReport)]),
     "cp_batch_create": (_I, [ctypes.POINTER(_vp), _I, ctypes.POINTER(_vp)]),
     "cp_batch_destroy": (_I, [_vp]),
     "cp_batch_set_tile": (_I, [_vp, _I, _I]),

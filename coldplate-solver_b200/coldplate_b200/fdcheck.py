@@ -14,15 +14,15 @@ the cell's γ raised by h and one with it lowered by h, and steps them in
 lockstep with an unperturbed solve until the DIFFERENCE D = ΔP(+h) - ΔP(-h)
 is stationary to ``--dtol`` (relative change over 100 iterations).
 
-Where velocities sit on the reference's +-3 max(U_in, 0.1) clamp, the
-pressure on either side of a clamped passage is coupled only through the
-Brinkman leak of the surrounding solid, and the iteration's error along that
-near-null pressure mode decays very slowly.  Restarted from the base state,
-the +h and -h solves settle with the same offset along it, so the one-sided
-quotients against the base differ by a term in |h| that does not shrink with
-h, while their average, the central difference, is the derivative of the
-fixed point.  The tool reports both; the adjoint is compared with the
-central difference.  Cells are drawn with a seeded generator from γ in
+Where the flow has faces with zero flux (a jet's symmetry plane, stagnant
+corners; the clamped passages of the reference's +-3 max(U_in, 0.1) velocity
+clamp create them), the upwind switch of those faces, and the clamp of face
+averages between clamped velocities, sit exactly on their kink: the +h and
+-h solves take different branches there, so the one-sided quotients against
+the base differ by a term that does not shrink with h, while their average,
+the central difference, is the mean of the branches' derivatives, which the
+adjoint takes at such faces.  The tool reports both; the adjoint is compared
+with the central difference.  Cells are drawn with a seeded generator from γ in
 [0.05, 0.95], at least 3 cells from the walls and away from the inlet and
 outlet buffers.  Prints one line per cell and a JSON summary line.
 """

@@ -192,6 +192,43 @@ class Simple:
                                                    ctypes.byref(rep)))
         return g, {name: getattr(rep, name) for name, _ in rep._fields_}
 
+    def adjoint_probe(self, op: int, x: dict | None = None, max_iter: int = 2000,
+                      tol: float = 1e-10) -> tuple[dict, dict]:
+        """Verification of the adjoint at the current state (cp_adjoint_probe):
+        op 0 J_X^T x, op 1 dJ/dX, op 2 the adjoint solution lambda.  x and the
+        result are dicts of staggered arrays 'u' (M+1, N), 'v' (M, N+1) and
+        'p' (M+1, N+1), zero outside the unknowns."""
+        n = int(self._lib.cp_adjoint_probe_len(self._h))
+        info = (ctypes.c_int * 4)()
+        # the layout needs the pitch: ask with op 1 first when x must be packed
+        y = np.zeros(n, dtype=np.float64)
+        rep = nat.CpAdjointReport()
+        M, N = self.M, self.N
+        shapes = {"u": (M + 1, N), "v": (M, N + 1), "p": (M + 1, N + 1)}
+        xin = None
+        if op == 0:
+            nat.check(self._lib.cp_adjoint_probe(self._h, 1, None, _dptr(y), 1, 1.0,
+                                                  ctypes.cast(info, ctypes.POINTER(ctypes.c_int)), None))
+            P = info[3]
+            xin = np.zeros(n, dtype=np.float64)
+            for b, f in enumerate(("u", "v", "p")):
+                blk = xin[b * n // 3:(b + 1) * n // 3].reshape(-1, P)
+                r, c = shapes[f]
+                blk[:r, :c] = x[f]
+        nat.check(self._lib.cp_adjoint_probe(self._h, int(op), None if xin is None else _dptr(xin), _dptr(y),
+                                              int(max_iter), float(tol),
+                                              ctypes.cast(info, ctypes.POINTER(ctypes.c_int)), ctypes.byref(rep)))
+        P = info[3]
+        out = {}
+        for b, f in enumerate(("u", "v", "p")):
+            blk = y[b * n // 3:(b + 1) * n // 3].reshape(-1, P)
+            r, c = shapes[f]
+            out[f] = blk[:r, :c].copy()
+        meta = {"model": info[0], "sweepsU": info[1], "sweepsV": info[2], "pitch": P}
+        if op == 2:
+            meta.update({name: getattr(rep, name) for name, _ in rep._fields_})
+        return out, meta
+
     # -------------------------------------------------------------- dispatch boundary
     def solveUMomentumImplicit(self) -> tuple[int, float]:
         r, it = ctypes.c_double(), ctypes.c_int()

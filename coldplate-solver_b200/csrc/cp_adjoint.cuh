@@ -91,20 +91,37 @@ struct FaceW {
     double lo, lolo, hi, hihi, val;
 };
 
+// Kinks.  A face whose velocity is zero up to rounding (|x| <= kKinkRel
+// maxVel: the symmetry plane of a jet, a stagnant corner) sits on the upwind
+// switch, and the sign the rounding gives it picks a branch at random.  There
+// the derivative is the mean of the two branches', the one central
+// differences of the converged solve measure: F phi and its derivative in F
+// take both branches' weights halved (F phi itself is zero there), and the
+// coefficients max(0, +-F) change with slope 1/2.  Likewise a face average on
+// the clamp (|x| = maxVel, between two clamped velocities) has clamp slope
+// 1/2.
+constexpr double kKinkRel = 1e-9;
+__device__ __forceinline__ bool kink0(double x, double mv) { return fabs(x) <= kKinkRel * mv; }
+// d max(0, F) / dF and d max(0, -F) / d(-F) at the face velocity x
+__device__ __forceinline__ double upw_pos(double x, double mv) { return kink0(x, mv) ? 0.5 : (x > 0.0 ? 1.0 : 0.0); }
+__device__ __forceinline__ double upw_neg(double x, double mv) { return kink0(x, mv) ? 0.5 : (x < 0.0 ? 1.0 : 0.0); }
+
 __device__ __forceinline__ FaceW face_phi(double F, double lo, double lolo, double hi, double hihi, bool souLo,
-                                          bool souHi) {
+                                          bool souHi, bool kink = false) {
     FaceW w{0, 0, 0, 0, 0};
-    if (F >= 0.0) {
-        if (souLo) { w.lo = 1.5; w.lolo = -0.5; } else { w.lo = 1.0; }
-    } else {
-        if (souHi) { w.hi = 1.5; w.hihi = -0.5; } else { w.hi = 1.0; }
-    }
+    const double wl = kink ? 0.5 : (F >= 0.0 ? 1.0 : 0.0), wh = 1.0 - wl;
+    if (souLo) { w.lo = 1.5 * wl; w.lolo = -0.5 * wl; } else { w.lo = wl; }
+    if (souHi) { w.hi = 1.5 * wh; w.hihi = -0.5 * wh; } else { w.hi = wh; }
     w.val = w.lo * lo + w.lolo * lolo + w.hi * hi + w.hihi * hihi;
     return w;
 }
 
-// clamp derivative: 1 inside [-maxVel, maxVel], 0 where the clamp acts
-__device__ __forceinline__ double clampd(double x, double m) { return (x < -m || m < x) ? 0.0 : 1.0; }
+// clamp derivative: 1 inside [-maxVel, maxVel], 0 where the clamp acts, 1/2
+// on it
+__device__ __forceinline__ double clampd(double x, double m) {
+    const double ax = fabs(x);
+    return ax > m * (1.0 + 1e-12) ? 0.0 : (ax >= m * (1.0 - 1e-12) ? 0.5 : 1.0);
+}
 
 struct AdjCtx {
     KParams k;
@@ -152,10 +169,10 @@ __device__ double adj_row_u(const AdjCtx& a, int i, int j, double lam, AdjVecs V
     const double gN = 0.5 * cN * clampd(xn, mv), gS = 0.5 * cN * clampd(xs, mv);
     const bool sou = k.sou;
     // faces: east (lo = P, hi = E), west (lo = W, hi = P), north (lo = P, hi = N), south (lo = S, hi = P)
-    const FaceW pe = face_phi(Fe, uP, uW, uE, uEE, sou && j >= 2, sou && j + 2 < N);
-    const FaceW pw = face_phi(Fw, uW, uWW, uP, uE, sou && j >= 2, sou && j + 1 < N);
-    const FaceW pn = face_phi(Fn, uP, uS, uN, uNN, sou && i >= 1, sou && i + 2 <= M);
-    const FaceW ps = face_phi(Fs, uS, uSS, uP, uN, sou && i >= 2, sou && i + 1 <= M);
+    const FaceW pe = face_phi(Fe, uP, uW, uE, uEE, sou && j >= 2, sou && j + 2 < N, kink0(xe, mv));
+    const FaceW pw = face_phi(Fw, uW, uWW, uP, uE, sou && j >= 2, sou && j + 1 < N, kink0(xw, mv));
+    const FaceW pn = face_phi(Fn, uP, uS, uN, uNN, sou && i >= 1, sou && i + 2 <= M, kink0(xn, mv));
+    const FaceW ps = face_phi(Fs, uS, uSS, uP, uN, sou && i >= 2, sou && i + 1 <= M, kink0(xs, mv));
     // half-cell wall flags (boundaries.cpp:148-171), as in the assembly
     const double gF = 0.5 * (a.gamma[at(d, i - 1, j - 1)] + a.gamma[at(d, i - 1, j)]);
     const double vt = 1e-8;
@@ -237,10 +254,10 @@ __device__ double adj_row_v(const AdjCtx& a, int i, int j, double lam, AdjVecs V
     const double gE = 0.5 * cE * clampd(xe, mv), gW = 0.5 * cE * clampd(xw, mv);
     const double gN = 0.5 * cN * clampd(xn, mv), gS = 0.5 * cN * clampd(xs, mv);
     const bool sou = k.sou;
-    const FaceW pe = face_phi(Fe, vP, vW, vE, vEE, sou && j >= 2, sou && j + 2 <= N);
-    const FaceW pw = face_phi(Fw, vW, vWW, vP, vE, sou && j >= 2, sou && j + 1 <= N);
-    const FaceW pn = face_phi(Fn, vP, vS, vN, vNN, sou && i >= 1, sou && i + 2 < M);
-    const FaceW ps = face_phi(Fs, vS, vSS, vP, vN, sou && i >= 2, sou && i + 1 < M);
+    const FaceW pe = face_phi(Fe, vP, vW, vE, vEE, sou && j >= 2, sou && j + 2 <= N, kink0(xe, mv));
+    const FaceW pw = face_phi(Fw, vW, vWW, vP, vE, sou && j >= 2, sou && j + 1 <= N, kink0(xw, mv));
+    const FaceW pn = face_phi(Fn, vP, vS, vN, vNN, sou && i >= 1, sou && i + 2 < M, kink0(xn, mv));
+    const FaceW ps = face_phi(Fs, vS, vSS, vP, vN, sou && i >= 2, sou && i + 1 < M, kink0(xs, mv));
     const double gF = 0.5 * (a.gamma[at(d, i - 1, j - 1)] + a.gamma[at(d, i, j - 1)]);
     const double vt = 1e-8;
     const bool hW = gF >= 0.999 && j == 1 && !(fabs(k.targetVel) > vt) && fabs(vv(i, 0)) <= vt &&
@@ -462,8 +479,8 @@ __device__ void adj_coef_row(const AdjCtx& a, int i, int j, const AdjSweep& S, A
     }
     const double Fe = cE * dclamp(xe, -mv, mv), Fw = cE * dclamp(xw, -mv, mv);
     const double Fn = cN * dclamp(xn, -mv, mv), Fs = cN * dclamp(xs, -mv, mv);
-    const double sE = Fe < 0.0 ? 1.0 : 0.0, sW = Fw > 0.0 ? 1.0 : 0.0;
-    const double sN = Fn < 0.0 ? 1.0 : 0.0, sS = Fs > 0.0 ? 1.0 : 0.0;
+    const double sE = upw_neg(xe, mv), sW = upw_pos(xw, mv);
+    const double sN = upw_neg(xn, mv), sS = upw_pos(xs, mv);
     const double Feb = (eIn ? -S.eb[c] * sE : 0.0) + ap0b * (1.0 - sE);
     const double Fwb = (wIn ? S.wb[c] * sW : 0.0) + ap0b * (sW - 1.0);
     const double Fnb = (nIn ? -S.nb[c] * sN : 0.0) + ap0b * (1.0 - sN);

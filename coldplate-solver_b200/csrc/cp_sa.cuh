@@ -744,6 +744,73 @@ __device__ __forceinline__ double sa0_prolong(const Sa0<TV>& A, const TV* __rest
     return acc;
 }
 
+// Restriction out of level 0 on aggregate-row segments: lane group g of
+// aggregate row I covers fine columns [12 g, 12 g + 12) and the aggregates
+// J = 4 g + 1 .. 4 g + 4 (own columns 3J-2 .. 3J, ring columns 3J-3 and
+// 3J+1).  Per fine column it sums over the five rows 3I-3 .. 3I+1 the
+// contribution to its own aggregate (pO on the aggregate's rows, pV on the
+// two ring rows) and to its horizontal neighbour (pH); columns 12 g + 12 and
+// 12 g + 13 come from the next lane group.  b_c = (P^T t)_c, x_c =
+// omega b_c / d_c.  Vectors past the row's pitch and rows past the array
+// read as zero; lane groups past the last aggregate (valid false) only
+// supply their first columns to the group before.
+template <typename TV>
+__device__ __forceinline__ void sa0_restrict_seg(const Sa0<TV>& A, const TV* __restrict__ t, const SaLevel<TV>& C,
+                                                 double omega, int I, int g, bool valid, int lane) {
+    constexpr int V = SaVec<TV>::n, NV = 12 / V;
+    const int P = A.P, j0 = 12 * g;
+    TV vo[12], vh[12];
+#pragma unroll
+    for (int k = 0; k < 12; ++k) vo[k] = vh[k] = (TV)0;
+#pragma unroll
+    for (int r = 0; r < 5; ++r) {
+        const int i = 3 * I - 3 + r;
+        if (i > A.nI + 2) break;
+        const bool ring = r == 0 || r == 4;
+        const int q0 = i * P + j0;
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            if (j0 + V * v + V > P) break;
+            const SaVec<TV> tv = sa_ld(t + q0 + V * v);
+            if (ring) {
+                const SaVec<TV> pv = sa_ld(A.pV + q0 + V * v);
+#pragma unroll
+                for (int k = 0; k < V; ++k) vo[V * v + k] += pv.v[k] * tv.v[k];
+            } else {
+                const SaVec<TV> po = sa_ld(A.pO + q0 + V * v), ph = sa_ld(A.pH + q0 + V * v);
+#pragma unroll
+                for (int k = 0; k < V; ++k) {
+                    vo[V * v + k] += po.v[k] * tv.v[k];
+                    vh[V * v + k] += ph.v[k] * tv.v[k];
+                }
+            }
+        }
+    }
+    TV o12 = sa_from_east(vo[0]), h13 = sa_from_east(vh[1]);
+    if (lane == 31) {
+        o12 = (TV)0;
+        h13 = (TV)0;
+        for (int r = 0; r < 5; ++r) {
+            const int i = 3 * I - 3 + r;
+            if (i > A.nI + 2) break;
+            const bool ring = r == 0 || r == 4;
+            const int q = i * P + j0 + 12;
+            if (j0 + 12 < P) o12 += (ring ? A.pV[q] : A.pO[q]) * t[q];
+            if (!ring && j0 + 13 < P) h13 += A.pH[q + 1] * t[q + 1];
+        }
+    }
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        const int J = 4 * g + 1 + a;
+        if (!valid || J > C.nJ) break;
+        const double s = (double)vo[3 * a + 1] + (double)vo[3 * a + 2] + (double)(a == 3 ? o12 : vo[3 * a + 3]) +
+                         (double)vh[3 * a] + (double)(a == 3 ? h13 : vh[3 * a + 4]);
+        const size_t qc = (size_t)I * C.P + J;
+        C.b[qc] = (TV)s;
+        C.x[qc] = (TV)(omega * s / (double)C.c[4][qc]);
+    }
+}
+
 // the same prolongation in two passes: t = x0 + P e on the lane group, then
 // (after a grid barrier) the post-smoothing from t; returns b.y
 template <typename TV>
@@ -1017,7 +1084,16 @@ __global__ void __launch_bounds__(512, 1) k_pcg_sa(KParams k, Status* st, const 
             target += G;
             if (!grid_barrier(bar, target, &st->err)) return false;
         }
-        sa_cells(all, C1.nI, C1.nJ, [&](int I, int J) { sa_restrict_w<TV, false>(L0, C1, om, I, J); });
+        {
+            // aggregate-row segments of 32 lane groups, one segment per warp
+            const int lane = threadIdx.x & 31;
+            const int warp = (int)(tid >> 5), nw = nth >> 5;
+            const int Gr = (C1.nJ + 3) / 4, S = (Gr + 31) >> 5;
+            for (int sg = warp; sg < C1.nI * S; sg += nw) {
+                const int I = 1 + sg / S, g = ((sg % S) << 5) + lane;
+                sa0_restrict_seg(A0f, L0.t, C1, om, I, g, g < Gr, lane);
+            }
+        }
         target += G;
         if (!grid_barrier(bar, target, &st->err)) return false;
         tick(SA_P_DOWN);

@@ -1297,13 +1297,11 @@ cp_status adjoint_prhs(cp_ctx* c, const KParams& k, const double* du, const doub
 
 }  // namespace
 
-extern "C" cp_status cp_adjoint_dp_dgamma(cp_ctx* c, double* grad, long rows, long cols, long rs, long cs,
-                                          int max_iter, double tol, cp_adjoint_report* rep) {
-    if (!c || !grad) return fail(CP_ERR_BAD_PARAM, "NULL argument");
+// The adjoint solve; probeOp >= 0 selects a verification output instead of
+// the gradient (cp_adjoint_probe): 0 y = J_X^T x, 1 y = dJ/dX, 2 y = lambda.
+static cp_status adjoint_impl(cp_ctx* c, double* grad, long rows, long cols, long rs, long cs, int max_iter, double tol,
+                              cp_adjoint_report* rep, int probeOp, const double* px, double* py, int* info) {
     const int M = c->d.M, N = c->d.N;
-    if (rows != M - 1 || cols != N - 1) return fail(CP_ERR_BAD_PARAM, "grad shape %ld x %ld, expected %d x %d",
-                                                    rows, cols, M - 1, N - 1);
-    if (max_iter < 1 || !(tol > 0.0)) return fail(CP_ERR_BAD_PARAM, "max_iter >= 1 and tol > 0 required");
     cp_status s = adjoint_alloc(c);
     if (s != CP_OK) return s;
     CK(cudaEventRecord(c->ev0, c->stream));
@@ -1493,6 +1491,22 @@ extern "C" cp_status cp_adjoint_dp_dgamma(cp_ctx* c, double* grad, long rows, lo
         return CP_OK;
     };
 
+    if (info) {
+        info[0] = model;
+        info[1] = sU;
+        info[2] = sV;
+        info[3] = c->d.P;
+    }
+    if (probeOp == 0 || probeOp == 1) {
+        // y = J^T x (x copied into the work vector W) or y = dJ/dX (x = 0)
+        CK(cudaMemsetAsync(W, 0, L * sizeof(double), c->stream));
+        if (probeOp == 0) CK(cudaMemcpyAsync(W, px, L * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        if ((s = product(W, probeOp == 1 ? 1.0 : 0.0, probeOp == 1 ? 0.0 : -1.0, Vq(0), nullptr, nullptr)) != CP_OK)
+            return s;
+        CK(cudaMemcpyAsync(py, Vq(0), L * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        return CP_OK;
+    }
     double res = 1.0, gnorm = 0.0, rr = 0.0, gg = 0.0;
     int it = 0;
     bool conv = false;
@@ -1570,6 +1584,18 @@ extern "C" cp_status cp_adjoint_dp_dgamma(cp_ctx* c, double* grad, long rows, lo
         beta = std::sqrt(rr);
         res = gnorm > 0.0 ? beta / gnorm : 0.0;
     }
+    if (probeOp == 2) {
+        CK(cudaMemcpyAsync(py, LAM, L * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        if (rep) {
+            rep->iterations = it;
+            rep->converged = conv ? 1 : 0;
+            rep->residual = res;
+            rep->model = model;
+            rep->clampedUnknowns = nClamped;
+        }
+        return CP_OK;
+    }
     // gradient on the Ny x Nx cells (fixed point: from the reverse sweeps of
     // lambda)
     double* gd = A[18];
@@ -1604,6 +1630,27 @@ extern "C" cp_status cp_adjoint_dp_dgamma(cp_ctx* c, double* grad, long rows, lo
         rep->clampedUnknowns = nClamped;
     }
     return CP_OK;
+}
+
+extern "C" cp_status cp_adjoint_dp_dgamma(cp_ctx* c, double* grad, long rows, long cols, long rs, long cs,
+                                          int max_iter, double tol, cp_adjoint_report* rep) {
+    if (!c || !grad) return fail(CP_ERR_BAD_PARAM, "NULL argument");
+    const int M = c->d.M, N = c->d.N;
+    if (rows != M - 1 || cols != N - 1) return fail(CP_ERR_BAD_PARAM, "grad shape %ld x %ld, expected %d x %d",
+                                                    rows, cols, M - 1, N - 1);
+    if (max_iter < 1 || !(tol > 0.0)) return fail(CP_ERR_BAD_PARAM, "max_iter >= 1 and tol > 0 required");
+    return adjoint_impl(c, grad, rows, cols, rs, cs, max_iter, tol, rep, -1, nullptr, nullptr, nullptr);
+}
+
+extern "C" size_t cp_adjoint_probe_len(const cp_ctx* c) { return c ? 3 * c->nElem : 0; }
+
+extern "C" cp_status cp_adjoint_probe(cp_ctx* c, int op, const double* x, double* y, int max_iter, double tol,
+                                      int* info, cp_adjoint_report* rep) {
+    if (!c || !y || !info) return fail(CP_ERR_BAD_PARAM, "NULL argument");
+    if (op < 0 || op > 2) return fail(CP_ERR_BAD_PARAM, "probe op %d (0, 1 or 2)", op);
+    if (op == 0 && !x) return fail(CP_ERR_BAD_PARAM, "probe op 0 needs x");
+    if (op == 2 && (max_iter < 1 || !(tol > 0.0))) return fail(CP_ERR_BAD_PARAM, "max_iter >= 1 and tol > 0 required");
+    return adjoint_impl(c, nullptr, c->d.M - 1, c->d.N - 1, 0, 0, max_iter, tol, rep, op, x, y, info);
 }
 
 // ======================================================================== no-allocation entry point

@@ -277,6 +277,18 @@ typedef struct cp_adjoint_report {
 cp_status cp_adjoint_dp_dgamma(cp_ctx* ctx, double* grad, long rows, long cols, long row_stride,
                                long col_stride, int max_iter, double tol, cp_adjoint_report* rep);
 
+/* Verification of the adjoint (tests): at the current state and with the
+ * model cp_adjoint_dp_dgamma would use, op 0 writes y = J_X^T x, op 1
+ * y = dJ/dX and op 2 the adjoint solution lambda (FGMRES with max_iter /
+ * tol as above; rep filled).  x and y hold cp_adjoint_probe_len(ctx)
+ * doubles: the U, V and continuity (pressure) blocks, each in the solver's
+ * padded layout (row pitch info[3], element (i, j) of the staggered field at
+ * i * pitch + j); entries outside the unknowns are zero in y and ignored in
+ * x.  info[0..2] = model, U and V Jacobi sweep counts of the state. */
+size_t cp_adjoint_probe_len(const cp_ctx* ctx);
+cp_status cp_adjoint_probe(cp_ctx* ctx, int op, const double* x, double* y, int max_iter, double tol, int* info,
+                           cp_adjoint_report* rep);
+
 /* Per-iteration history rows (cp_iter_report layout without device_ms, as
  * doubles: see cp_history_columns()).  Returns the number of rows copied. */
 int cp_history_columns(void);

@@ -1,14 +1,16 @@
 """The adjoint gradient where the reference's velocity clamp is active.
 
 At the converged state of the constricted channel (cases.constricted_channel)
-and of the 256 x 128 density field, velocities sit on the +-3 max(U_in, 0.1)
-clamp.  The adjoint differentiates the fixed point the reference iteration
-reaches there (frozen Jacobi sweep count and clamped set); it must agree with
-central differences (h = 1e-4) of converged FP64 forward solves, restarted
-from the base state and stepped until the difference is stationary, within
-1e-4 relative on every checked cell.  The one-sided quotients are reported:
-on a clamped state they differ from each other by a term in |h| (the slow
-near-null pressure mode the clamp creates), not from the central value.
+velocities sit on the +-3 max(U_in, 0.1) clamp.  The adjoint differentiates
+the fixed point the reference iteration reaches there (frozen Jacobi sweep
+count and clamped set); it must agree with central differences (h = 1e-4) of
+converged FP64 forward solves, restarted from the base state and stepped
+until the difference is stationary, within 1e-4 relative on every checked
+cell.  The one-sided quotients are reported: they differ from each other
+because faces with zero flux in the jet behind the gap sit on the upwind
+switch (and faces between clamped velocities on the clamp), where the map
+has a kink; the central difference and the adjoint take the mean of the two
+branches there.
 """
 import numpy as np
 import pytest
@@ -44,9 +46,9 @@ def _check(case, cells, base_iters, fd_iters, min_clamped):
             r = fdc.cell(i, j, 1e-4, 1e-9, fd_iters)
             fd, fwd, bwd, adj = r["fd"], r["fwd"], r["bwd"], float(grad[i, j])
             smooth = abs(fwd - bwd) <= 1e-2 * abs(fd)
-            ok = abs(adj - fd) <= TOL * abs(fd) or (not smooth and min(fwd, bwd) <= adj <= max(fwd, bwd))
-            out.append(dict(cell=(i, j), fd=fd, adjoint=adj, fwd=fwd, bwd=bwd,
-                            case="smooth" if smooth else "one-sided slopes differ", ok=ok))
+            ok = abs(adj - fd) <= TOL * abs(fd)
+            out.append(dict(cell=(i, j), fd=fd, adjoint=adj, rel=abs(adj - fd) / abs(fd), fwd=fwd, bwd=bwd,
+                            case="smooth" if smooth else "kink: one-sided slopes differ", ok=ok))
     print(out)
     bad = [o for o in out if not o["ok"]]
     assert not bad, (bad, out)
@@ -54,9 +56,8 @@ def _check(case, cells, base_iters, fd_iters, min_clamped):
 
 
 def test_adjoint_on_the_constricted_channel():
-    """Cells on the gamma = 0.5 faces of the block, both sides of the gap.
-    Each cell passes if the adjoint is within 1e-4 of the central
-    difference, or, where the one-sided quotients differ by more than 1 %
-    (the case the test records), if it lies between them."""
+    """Cells on the gamma = 0.5 faces of the block, both sides of the gap:
+    the adjoint within 1e-4 of the central difference on each (the test
+    records whether the one-sided quotients differ, a kink)."""
     case = cases.constricted_channel(32, 96, pressureSolverType=4, maxPressureIter=30, pTol=1e-6)
     _check(case, [(12, 45), (19, 50), (5, 39), (25, 39)], 40000, 40000, min_clamped=50)
