@@ -637,13 +637,16 @@ def main():
     pcg_iters = kt["pcgIterations"] / max(kt["launches"]["pcg"], 1)
     sa = os.environ.get("CP_PRESSURE_CYCLE") != "pairs"
     if sa:
-        # smoothed aggregation: 37 w per unknown per CG iteration: 8 w for the
-        # CG vectors (read x, r, p, dE, dN; write x, r, p), 23 w for level 0 of
-        # the V(1,1) cycle (residual 7, restriction 5, prolongation 5,
-        # post-smoothing 6) and 6 w for the 9-point coarse levels (four passes
-        # over 13 arrays at a ninth of the unknowns, 47 w there, times 9/8 for
+        # smoothed aggregation: 38 w per unknown per CG iteration: 18 w for
+        # the CG passes (matvec: read z, p_old, d, fE, fN, write p, Ap; update
+        # fused with level 0's pre-smoothing and residual: read p, Ap, x, r,
+        # 1/d, fE, fN, write x, r', x0, t), 15 w for the rest of level 0
+        # (restriction: read t and three prolongation weights; prolongation:
+        # read x0 and the weights, write t; post-smoothing: read t, r', 1/d,
+        # fE, fN, write y) and 4.5 w for the 9-point coarse levels (about
+        # 36 w per level-1 unknown, a ninth of the unknowns, times 9/8 for
         # the levels below)
-        words, kname = 37, "k_pcg_sa<float>"
+        words, kname = 38, "k_pcg_sa<float>"
         cap_bytes, cap_iters = PCG_SA_CAPTURE_BYTES, PCG_SA_CAPTURE_ITERS
     else:
         # 2 x 2 aggregation: 23 w per unknown per CG iteration: 8 w for the CG

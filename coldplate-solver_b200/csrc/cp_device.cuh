@@ -187,4 +187,58 @@ __device__ __forceinline__ void atomic_max_nonneg(unsigned long long* addr, doub
     if (v > 0.0) atomicMax(addr, (unsigned long long)__double_as_longlong(v));
 }
 
+// ------------------------------------------------------------ row segments
+// 16 bytes of one row: 4 floats or 2 doubles
+template <typename TV>
+struct Vec16 {
+    static constexpr int n = 16 / (int)sizeof(TV);
+    TV v[n];
+};
+__device__ __forceinline__ Vec16<float> ld16(const float* p) {
+    const float4 f = *reinterpret_cast<const float4*>(p);
+    return {{f.x, f.y, f.z, f.w}};
+}
+__device__ __forceinline__ Vec16<double> ld16(const double* p) {
+    const double2 f = *reinterpret_cast<const double2*>(p);
+    return {{f.x, f.y}};
+}
+__device__ __forceinline__ void st16(float* p, const Vec16<float>& a) {
+    *reinterpret_cast<float4*>(p) = make_float4(a.v[0], a.v[1], a.v[2], a.v[3]);
+}
+__device__ __forceinline__ void st16(double* p, const Vec16<double>& a) {
+    *reinterpret_cast<double2*>(p) = make_double2(a.v[0], a.v[1]);
+}
+template <typename TV>
+__device__ __forceinline__ Vec16<TV> zero16() {
+    Vec16<TV> a;
+#pragma unroll
+    for (int k = 0; k < Vec16<TV>::n; ++k) a.v[k] = (TV)0;
+    return a;
+}
+
+// Row segments of a level in the padded layout (unknowns i in [1, nI],
+// j in [1, nJ], row pitch P): warp w takes segments w, w + nwarps, ... of 32
+// lane groups of one row, lane group g covering columns [g V, g V + V)
+// (V = 16 / sizeof(TV)); fn(i, j0, act, lane) with act false on the groups
+// past the row's last unknown.  The loop is uniform over each warp, so fn
+// may shuffle.  A vector of a group with g V <= nJ stays inside the row
+// (the pitch is a multiple of 32 above nJ), and column g V + V, read by lane
+// 31, is at most the next row's column 0.
+template <typename TV, typename F>
+__device__ __forceinline__ void row_segments(int nI, int nJ, F&& fn) {
+    constexpr int V = Vec16<TV>::n;
+    const int lane = threadIdx.x & 31;
+    const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), nw = (int)((gridDim.x * blockDim.x) >> 5);
+    const int Ga = nJ / V + 1, S = (Ga + 31) >> 5;
+    for (int s = warp; s < nI * S; s += nw) {
+        const int i = 1 + s / S, g = ((s % S) << 5) + lane;
+        fn(i, g * V, g < Ga, lane);
+    }
+}
+
+template <typename TV>
+__device__ __forceinline__ TV from_west(TV v) { return __shfl_up_sync(0xffffffffu, v, 1); }
+template <typename TV>
+__device__ __forceinline__ TV from_east(TV v) { return __shfl_down_sync(0xffffffffu, v, 1); }
+
 }  // namespace cp

@@ -262,8 +262,7 @@ __device__ __forceinline__ bool jacobi_component(const KParams& k, Status* st, c
     const int G = gridDim.x;
     int i1, j1;
     mom_range<IsU>(d, i1, j1);
-    const int w = j1, n = i1 * j1;
-    const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = G * blockDim.x;
+    const int n = i1 * j1;
     const double lim = k.momTol * k.momTol * (double)n;
     TC* xs[2] = {x0, x1};
     cur = -1;
@@ -274,45 +273,57 @@ __device__ __forceinline__ bool jacobi_component(const KParams& k, Status* st, c
         TC* __restrict__ xn = xs[nxt];
         const bool first = cur < 0;
         double acc[1] = {0.0};
-        for (int t0 = tid; t0 < n; t0 += 2 * nth) {
-            TC v[2][11];
-            size_t cc[2];
-            bool ok[2];
-#pragma unroll
-            for (int q = 0; q < 2; ++q) {
-                const int t = t0 + q * nth;
-                ok[q] = t < n;
-                const int tt = ok[q] ? t : t0;
-                const int i = 1 + tt / w, j = 1 + tt % w;
-                const size_t c = at(d, i, j);
-                cc[q] = c;
-                auto X = [&](size_t a) -> TC {
-                    if (first) return Mixed ? (TC)0 : (TC)field[a];
-                    return xc[a];
-                };
-                v[q][0] = S.aP[c]; v[q][1] = S.aE[c]; v[q][2] = S.aW[c]; v[q][3] = S.aN[c]; v[q][4] = S.aS[c];
-                v[q][5] = S.b[c];
-                v[q][6] = X(c);
-                v[q][7] = (i > 1) ? X(c - d.P) : (TC)0;
-                v[q][8] = (j > 1) ? X(c - 1) : (TC)0;
-                v[q][9] = (j < j1) ? X(c + 1) : (TC)0;
-                v[q][10] = (i < i1) ? X(c + d.P) : (TC)0;
+        // row segments: a lane takes 16 bytes of a row (4 floats or 2
+        // doubles); horizontal neighbours from the adjacent lanes
+        constexpr int V = Vec16<TC>::n;
+        row_segments<TC>(i1, j1, [&](int i, int j0, bool act, int lane) {
+            const size_t c = at(d, i, j0);
+            auto Xv = [&](size_t q) -> Vec16<TC> {
+                if (first) {
+                    if constexpr (Mixed) return zero16<TC>();
+                    else return ld16(field + q);
+                }
+                return ld16(xc + q);
+            };
+            auto Xs = [&](size_t q) -> TC {
+                if (first) return Mixed ? (TC)0 : (TC)field[q];
+                return xc[q];
+            };
+            Vec16<TC> aP = zero16<TC>(), aE = aP, aW = aP, aN = aP, aS = aP, b = aP, xP = aP, xN = aP, xS = aP;
+            if (act) {
+                aP = ld16(S.aP + c);
+                aE = ld16(S.aE + c);
+                aW = ld16(S.aW + c);
+                aN = ld16(S.aN + c);
+                aS = ld16(S.aS + c);
+                b = ld16(S.b + c);
+                xP = Xv(c);
+                if (i > 1) xS = Xv(c - d.P);
+                if (i < i1) xN = Xv(c + d.P);
             }
+            TC xw = from_west(xP.v[V - 1]), xe = from_east(xP.v[0]);
+            if (lane == 0) xw = (act && j0 > 0) ? Xs(c - 1) : (TC)0;
+            if (lane == 31) xe = act ? Xs(c + V) : (TC)0;
+            Vec16<TC> o;
 #pragma unroll
-            for (int q = 0; q < 2; ++q) {
-                if (!ok[q]) continue;
+            for (int q = 0; q < V; ++q) {
+                const int j = j0 + q;
+                const bool in = act && j >= 1 && j <= j1;
+                const TC W = (j > 1) ? (q ? xP.v[q - 1] : xw) : (TC)0;
+                const TC E = (j < j1) ? (q < V - 1 ? xP.v[q + 1] : xe) : (TC)0;
                 // S, W, P, E, N order of the reference's CSR rows
                 TC Ax = (TC)0;
-                Ax += (-v[q][4]) * v[q][7];
-                Ax += (-v[q][2]) * v[q][8];
-                Ax += v[q][0] * v[q][6];
-                Ax += (-v[q][1]) * v[q][9];
-                Ax += (-v[q][3]) * v[q][10];
-                const TC r = v[q][5] - Ax;
-                xn[cc[q]] = v[q][6] + r / v[q][0];
-                acc[0] += (double)r * (double)r;
+                Ax += (-aS.v[q]) * xS.v[q];
+                Ax += (-aW.v[q]) * W;
+                Ax += aP.v[q] * xP.v[q];
+                Ax += (-aE.v[q]) * E;
+                Ax += (-aN.v[q]) * xN.v[q];
+                const TC r = b.v[q] - Ax;
+                o.v[q] = in ? (TC)(xP.v[q] + r / aP.v[q]) : (TC)0;
+                if (in) acc[0] += (double)r * (double)r;
             }
-        }
+            if (act) st16(xn + c, o);
+        });
         block_sum<1>(acc, sm);
         double* slot = part + (size_t)(s & 1) * G;
         if (threadIdx.x == 0) slot[blockIdx.x] = acc[0];

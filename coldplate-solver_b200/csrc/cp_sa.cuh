@@ -482,94 +482,42 @@ struct Sa0 {
     int nI, nJ, P;
 };
 
-// 16 bytes of one row: 4 floats or 2 doubles
-template <typename TV>
-struct SaVec {
-    static constexpr int n = 16 / (int)sizeof(TV);
-    TV v[n];
-};
-__device__ __forceinline__ SaVec<float> sa_ld(const float* p) {
-    const float4 f = *reinterpret_cast<const float4*>(p);
-    return {{f.x, f.y, f.z, f.w}};
-}
-__device__ __forceinline__ SaVec<double> sa_ld(const double* p) {
-    const double2 f = *reinterpret_cast<const double2*>(p);
-    return {{f.x, f.y}};
-}
-__device__ __forceinline__ void sa_st(float* p, const SaVec<float>& a) {
-    *reinterpret_cast<float4*>(p) = make_float4(a.v[0], a.v[1], a.v[2], a.v[3]);
-}
-__device__ __forceinline__ void sa_st(double* p, const SaVec<double>& a) {
-    *reinterpret_cast<double2*>(p) = make_double2(a.v[0], a.v[1]);
-}
-template <typename TV>
-__device__ __forceinline__ SaVec<TV> sa_zero() {
-    SaVec<TV> a;
-#pragma unroll
-    for (int k = 0; k < SaVec<TV>::n; ++k) a.v[k] = (TV)0;
-    return a;
-}
-
-// Row segments of level 0: warp w takes segments w, w + nwarps, ... of 32
-// lane groups of one row, lane group g covering columns [g V, g V + V)
-// (V = 16 / sizeof(TV)); fn(i, j0, act, lane) with act false on the groups
-// past the row's last unknown.  The loop is uniform over each warp, so fn
-// may shuffle.  A vector of groups below g V <= nJ stays inside the row
-// (the pitch is a multiple of 32 and at least nJ + 3), and column g V + V,
-// read by lane 31, at most at the next row's column 0.
-template <typename TV, typename F>
-__device__ __forceinline__ void sa_rows(int nI, int nJ, F&& fn) {
-    constexpr int V = SaVec<TV>::n;
-    const int lane = threadIdx.x & 31;
-    const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), nw = (int)((gridDim.x * blockDim.x) >> 5);
-    const int Ga = nJ / V + 1, S = (Ga + 31) >> 5;
-    for (int s = warp; s < nI * S; s += nw) {
-        const int i = 1 + s / S, g = ((s % S) << 5) + lane;
-        fn(i, g * V, g < Ga, lane);
-    }
-}
-
-template <typename TV>
-__device__ __forceinline__ TV sa_from_west(TV v) { return __shfl_up_sync(0xffffffffu, v, 1); }
-template <typename TV>
-__device__ __forceinline__ TV sa_from_east(TV v) { return __shfl_down_sync(0xffffffffu, v, 1); }
-
 // CG matvec on p = z + beta p_old (p_old unused when first): writes p and Ap
 // on one lane group, returns the group's share of p.Ap
 template <typename TV>
 __device__ __forceinline__ double sa0_matvec(const Sa0<TV>& A, const TV* __restrict__ z, const TV* __restrict__ pold,
                                              TV bt, bool first, TV* __restrict__ pnew, TV* __restrict__ Ap, int i,
                                              int j0, bool act, int lane) {
-    constexpr int V = SaVec<TV>::n;
+    constexpr int V = Vec16<TV>::n;
     const int P = A.P, c = i * P + j0;
     auto dir = [&](int q) -> TV { return first ? z[q] : (TV)(z[q] + bt * pold[q]); };
-    auto dirv = [&](int q) -> SaVec<TV> {
-        SaVec<TV> a = sa_ld(z + q);
+    auto dirv = [&](int q) -> Vec16<TV> {
+        Vec16<TV> a = ld16(z + q);
         if (!first) {
-            const SaVec<TV> o = sa_ld(pold + q);
+            const Vec16<TV> o = ld16(pold + q);
 #pragma unroll
             for (int k = 0; k < V; ++k) a.v[k] = (TV)(a.v[k] + bt * o.v[k]);
         }
         return a;
     };
-    SaVec<TV> pc = sa_zero<TV>(), pn = pc, ps = pc, d = pc, fe = pc, fn = pc, fs = pc;
+    Vec16<TV> pc = zero16<TV>(), pn = pc, ps = pc, d = pc, fe = pc, fn = pc, fs = pc;
     if (act) {
         pc = dirv(c);
         pn = dirv(c + P);
         ps = dirv(c - P);
-        d = sa_ld(A.d + c);
-        fe = sa_ld(A.fE + c);
-        fn = sa_ld(A.fN + c);
-        fs = sa_ld(A.fN + c - P);
+        d = ld16(A.d + c);
+        fe = ld16(A.fE + c);
+        fn = ld16(A.fN + c);
+        fs = ld16(A.fN + c - P);
     }
-    TV pw = sa_from_west(pc.v[V - 1]), pe = sa_from_east(pc.v[0]), fw = sa_from_west(fe.v[V - 1]);
+    TV pw = from_west(pc.v[V - 1]), pe = from_east(pc.v[0]), fw = from_west(fe.v[V - 1]);
     if (lane == 0) {
         const bool h = act && j0 > 0;
         pw = h ? dir(c - 1) : (TV)0;
         fw = h ? A.fE[c - 1] : (TV)0;
     }
     if (lane == 31) pe = act ? dir(c + V) : (TV)0;
-    SaVec<TV> ap;
+    Vec16<TV> ap;
     double acc = 0.0;
 #pragma unroll
     for (int k = 0; k < V; ++k) {
@@ -580,8 +528,8 @@ __device__ __forceinline__ double sa0_matvec(const Sa0<TV>& A, const TV* __restr
         acc += (double)pc.v[k] * (double)a;
     }
     if (act) {
-        sa_st(pnew + c, pc);
-        sa_st(Ap + c, ap);
+        st16(pnew + c, pc);
+        st16(Ap + c, ap);
     }
     return acc;
 }
@@ -596,19 +544,19 @@ __device__ __forceinline__ double sa0_update(const Sa0<TV>& A, TV al, TV om, con
                                              const TV* __restrict__ Ap, TV* __restrict__ x, const TV* __restrict__ r,
                                              TV* __restrict__ rn, TV* __restrict__ x0, TV* __restrict__ t, int i,
                                              int j0, bool act, int lane) {
-    constexpr int V = SaVec<TV>::n;
+    constexpr int V = Vec16<TV>::n;
     const int P = A.P, c = i * P + j0;
     auto x0at = [&](int q) -> TV { return om * (r[q] - al * Ap[q]) * A.dinv[q]; };
-    auto x0v = [&](int q) -> SaVec<TV> {
-        const SaVec<TV> rr = sa_ld(r + q), aa = sa_ld(Ap + q), di = sa_ld(A.dinv + q);
-        SaVec<TV> o;
+    auto x0v = [&](int q) -> Vec16<TV> {
+        const Vec16<TV> rr = ld16(r + q), aa = ld16(Ap + q), di = ld16(A.dinv + q);
+        Vec16<TV> o;
 #pragma unroll
         for (int k = 0; k < V; ++k) o.v[k] = om * (rr.v[k] - al * aa.v[k]) * di.v[k];
         return o;
     };
-    SaVec<TV> rc = sa_zero<TV>(), xc = rc, xn = rc, xs = rc, xx = rc, pp = rc, fe = rc, fn = rc, fs = rc;
+    Vec16<TV> rc = zero16<TV>(), xc = rc, xn = rc, xs = rc, xx = rc, pp = rc, fe = rc, fn = rc, fs = rc;
     if (act) {
-        const SaVec<TV> rr = sa_ld(r + c), aa = sa_ld(Ap + c), di = sa_ld(A.dinv + c);
+        const Vec16<TV> rr = ld16(r + c), aa = ld16(Ap + c), di = ld16(A.dinv + c);
 #pragma unroll
         for (int k = 0; k < V; ++k) {
             rc.v[k] = rr.v[k] - al * aa.v[k];
@@ -616,20 +564,20 @@ __device__ __forceinline__ double sa0_update(const Sa0<TV>& A, TV al, TV om, con
         }
         xn = x0v(c + P);
         xs = x0v(c - P);
-        xx = sa_ld(x + c);
-        pp = sa_ld(p + c);
-        fe = sa_ld(A.fE + c);
-        fn = sa_ld(A.fN + c);
-        fs = sa_ld(A.fN + c - P);
+        xx = ld16(x + c);
+        pp = ld16(p + c);
+        fe = ld16(A.fE + c);
+        fn = ld16(A.fN + c);
+        fs = ld16(A.fN + c - P);
     }
-    TV xw = sa_from_west(xc.v[V - 1]), xe = sa_from_east(xc.v[0]), fw = sa_from_west(fe.v[V - 1]);
+    TV xw = from_west(xc.v[V - 1]), xe = from_east(xc.v[0]), fw = from_west(fe.v[V - 1]);
     if (lane == 0) {
         const bool h = act && j0 > 0;
         xw = h ? x0at(c - 1) : (TV)0;
         fw = h ? A.fE[c - 1] : (TV)0;
     }
     if (lane == 31) xe = act ? x0at(c + V) : (TV)0;
-    SaVec<TV> tt;
+    Vec16<TV> tt;
     double acc = 0.0;
 #pragma unroll
     for (int k = 0; k < V; ++k) {
@@ -641,10 +589,10 @@ __device__ __forceinline__ double sa0_update(const Sa0<TV>& A, TV al, TV om, con
         acc += (double)rc.v[k] * (double)rc.v[k];
     }
     if (act) {
-        sa_st(x + c, xx);
-        sa_st(rn + c, rc);
-        sa_st(x0 + c, xc);
-        sa_st(t + c, tt);
+        st16(x + c, xx);
+        st16(rn + c, rc);
+        st16(x0 + c, xc);
+        st16(t + c, tt);
     }
     return acc;
 }
@@ -655,26 +603,26 @@ template <typename TV>
 __device__ __forceinline__ void sa0_resid(const Sa0<TV>& A, TV om, const TV* __restrict__ b,
                                           const TV* __restrict__ x0, TV* __restrict__ t, int i, int j0, bool act,
                                           int lane) {
-    constexpr int V = SaVec<TV>::n;
+    constexpr int V = Vec16<TV>::n;
     const int P = A.P, c = i * P + j0;
-    SaVec<TV> xc = sa_zero<TV>(), xn = xc, xs = xc, bb = xc, fe = xc, fn = xc, fs = xc;
+    Vec16<TV> xc = zero16<TV>(), xn = xc, xs = xc, bb = xc, fe = xc, fn = xc, fs = xc;
     if (act) {
-        xc = sa_ld(x0 + c);
-        xn = sa_ld(x0 + c + P);
-        xs = sa_ld(x0 + c - P);
-        bb = sa_ld(b + c);
-        fe = sa_ld(A.fE + c);
-        fn = sa_ld(A.fN + c);
-        fs = sa_ld(A.fN + c - P);
+        xc = ld16(x0 + c);
+        xn = ld16(x0 + c + P);
+        xs = ld16(x0 + c - P);
+        bb = ld16(b + c);
+        fe = ld16(A.fE + c);
+        fn = ld16(A.fN + c);
+        fs = ld16(A.fN + c - P);
     }
-    TV xw = sa_from_west(xc.v[V - 1]), xe = sa_from_east(xc.v[0]), fw = sa_from_west(fe.v[V - 1]);
+    TV xw = from_west(xc.v[V - 1]), xe = from_east(xc.v[0]), fw = from_west(fe.v[V - 1]);
     if (lane == 0) {
         const bool h = act && j0 > 0;
         xw = h ? x0[c - 1] : (TV)0;
         fw = h ? A.fE[c - 1] : (TV)0;
     }
     if (lane == 31) xe = act ? x0[c + V] : (TV)0;
-    SaVec<TV> tt;
+    Vec16<TV> tt;
 #pragma unroll
     for (int k = 0; k < V; ++k) {
         const TV W = k ? xc.v[k - 1] : xw, E = k < V - 1 ? xc.v[k + 1] : xe, FW = k ? fe.v[k - 1] : fw;
@@ -682,7 +630,7 @@ __device__ __forceinline__ void sa0_resid(const Sa0<TV>& A, TV om, const TV* __r
         if (j0 + k < 1 || j0 + k > A.nJ) t1 = (TV)0;
         tt.v[k] = t1;
     }
-    if (act) sa_st(t + c, tt);
+    if (act) st16(t + c, tt);
 }
 
 // prolongation from level 1 fused with level 0's post-smoothing:
@@ -694,7 +642,7 @@ template <typename TV>
 __device__ __forceinline__ double sa0_prolong(const Sa0<TV>& A, const TV* __restrict__ x0, const TV* __restrict__ b,
                                               const TV* __restrict__ e, int Pc, TV om, TV* __restrict__ y, int i,
                                               int j0, bool act, int lane) {
-    constexpr int V = SaVec<TV>::n;
+    constexpr int V = Vec16<TV>::n;
     const int P = A.P, c = i * P + j0;
     // t at (ii, jj) from its x0 and weights; 0 outside the unknowns
     auto tat = [&](int ii, int jj, TV xv, TV po, TV ph, TV pv) -> TV {
@@ -702,34 +650,34 @@ __device__ __forceinline__ double sa0_prolong(const Sa0<TV>& A, const TV* __rest
         const TV* er = e + ((ii - 1) / 3 + 1) * Pc + (jj - 1) / 3 + 1;
         return xv + po * er[0] + ph * er[sa_side(jj)] + pv * er[sa_side(ii) * Pc];
     };
-    auto trow = [&](int ii) -> SaVec<TV> {
+    auto trow = [&](int ii) -> Vec16<TV> {
         const int q = ii * P + j0;
-        const SaVec<TV> xv = sa_ld(x0 + q), po = sa_ld(A.pO + q), ph = sa_ld(A.pH + q), pv = sa_ld(A.pV + q);
-        SaVec<TV> o;
+        const Vec16<TV> xv = ld16(x0 + q), po = ld16(A.pO + q), ph = ld16(A.pH + q), pv = ld16(A.pV + q);
+        Vec16<TV> o;
 #pragma unroll
         for (int k = 0; k < V; ++k) o.v[k] = tat(ii, j0 + k, xv.v[k], po.v[k], ph.v[k], pv.v[k]);
         return o;
     };
     auto tone = [&](int q, int jj) -> TV { return tat(i, jj, x0[q], A.pO[q], A.pH[q], A.pV[q]); };
-    SaVec<TV> tc = sa_zero<TV>(), tn = tc, ts = tc, bb = tc, di = tc, fe = tc, fn = tc, fs = tc;
+    Vec16<TV> tc = zero16<TV>(), tn = tc, ts = tc, bb = tc, di = tc, fe = tc, fn = tc, fs = tc;
     if (act) {
         tc = trow(i);
         tn = trow(i + 1);
         ts = trow(i - 1);
-        bb = sa_ld(b + c);
-        di = sa_ld(A.dinv + c);
-        fe = sa_ld(A.fE + c);
-        fn = sa_ld(A.fN + c);
-        fs = sa_ld(A.fN + c - P);
+        bb = ld16(b + c);
+        di = ld16(A.dinv + c);
+        fe = ld16(A.fE + c);
+        fn = ld16(A.fN + c);
+        fs = ld16(A.fN + c - P);
     }
-    TV tw = sa_from_west(tc.v[V - 1]), te = sa_from_east(tc.v[0]), fw = sa_from_west(fe.v[V - 1]);
+    TV tw = from_west(tc.v[V - 1]), te = from_east(tc.v[0]), fw = from_west(fe.v[V - 1]);
     if (lane == 0) {
         const bool h = act && j0 > 0;
         tw = h ? tone(c - 1, j0 - 1) : (TV)0;
         fw = h ? A.fE[c - 1] : (TV)0;
     }
     if (lane == 31) te = act ? tone(c + V, j0 + V) : (TV)0;
-    SaVec<TV> yv;
+    Vec16<TV> yv;
     double acc = 0.0;
 #pragma unroll
     for (int k = 0; k < V; ++k) {
@@ -740,7 +688,7 @@ __device__ __forceinline__ double sa0_prolong(const Sa0<TV>& A, const TV* __rest
         yv.v[k] = yk;
         acc += (double)bb.v[k] * (double)yk;
     }
-    if (act) sa_st(y + c, yv);
+    if (act) st16(y + c, yv);
     return acc;
 }
 
@@ -757,7 +705,7 @@ __device__ __forceinline__ double sa0_prolong(const Sa0<TV>& A, const TV* __rest
 template <typename TV>
 __device__ __forceinline__ void sa0_restrict_seg(const Sa0<TV>& A, const TV* __restrict__ t, const SaLevel<TV>& C,
                                                  double omega, int I, int g, bool valid, int lane) {
-    constexpr int V = SaVec<TV>::n, NV = 12 / V;
+    constexpr int V = Vec16<TV>::n, NV = 12 / V;
     const int P = A.P, j0 = 12 * g;
     TV vo[12], vh[12];
 #pragma unroll
@@ -771,13 +719,13 @@ __device__ __forceinline__ void sa0_restrict_seg(const Sa0<TV>& A, const TV* __r
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
             if (j0 + V * v + V > P) break;
-            const SaVec<TV> tv = sa_ld(t + q0 + V * v);
+            const Vec16<TV> tv = ld16(t + q0 + V * v);
             if (ring) {
-                const SaVec<TV> pv = sa_ld(A.pV + q0 + V * v);
+                const Vec16<TV> pv = ld16(A.pV + q0 + V * v);
 #pragma unroll
                 for (int k = 0; k < V; ++k) vo[V * v + k] += pv.v[k] * tv.v[k];
             } else {
-                const SaVec<TV> po = sa_ld(A.pO + q0 + V * v), ph = sa_ld(A.pH + q0 + V * v);
+                const Vec16<TV> po = ld16(A.pO + q0 + V * v), ph = ld16(A.pH + q0 + V * v);
 #pragma unroll
                 for (int k = 0; k < V; ++k) {
                     vo[V * v + k] += po.v[k] * tv.v[k];
@@ -786,7 +734,7 @@ __device__ __forceinline__ void sa0_restrict_seg(const Sa0<TV>& A, const TV* __r
             }
         }
     }
-    TV o12 = sa_from_east(vo[0]), h13 = sa_from_east(vh[1]);
+    TV o12 = from_east(vo[0]), h13 = from_east(vh[1]);
     if (lane == 31) {
         o12 = (TV)0;
         h13 = (TV)0;
@@ -816,12 +764,12 @@ __device__ __forceinline__ void sa0_restrict_seg(const Sa0<TV>& A, const TV* __r
 template <typename TV>
 __device__ __forceinline__ void sa0_prolong_t(const Sa0<TV>& A, const TV* __restrict__ x0, const TV* __restrict__ e,
                                               int Pc, TV* __restrict__ t, int i, int j0, bool act) {
-    constexpr int V = SaVec<TV>::n;
+    constexpr int V = Vec16<TV>::n;
     if (!act) return;
     const int c = i * A.P + j0;
-    const SaVec<TV> xv = sa_ld(x0 + c), po = sa_ld(A.pO + c), ph = sa_ld(A.pH + c), pv = sa_ld(A.pV + c);
+    const Vec16<TV> xv = ld16(x0 + c), po = ld16(A.pO + c), ph = ld16(A.pH + c), pv = ld16(A.pV + c);
     const int I = (i - 1) / 3 + 1, sv = sa_side(i) * Pc;
-    SaVec<TV> o;
+    Vec16<TV> o;
 #pragma unroll
     for (int k = 0; k < V; ++k) {
         const int jj = j0 + k;
@@ -832,33 +780,33 @@ __device__ __forceinline__ void sa0_prolong_t(const Sa0<TV>& A, const TV* __rest
         }
         o.v[k] = tk;
     }
-    sa_st(t + c, o);
+    st16(t + c, o);
 }
 template <typename TV>
 __device__ __forceinline__ double sa0_smooth(const Sa0<TV>& A, TV om, const TV* __restrict__ b,
                                              const TV* __restrict__ t, TV* __restrict__ y, int i, int j0, bool act,
                                              int lane) {
-    constexpr int V = SaVec<TV>::n;
+    constexpr int V = Vec16<TV>::n;
     const int P = A.P, c = i * P + j0;
-    SaVec<TV> tc = sa_zero<TV>(), tn = tc, ts = tc, bb = tc, di = tc, fe = tc, fn = tc, fs = tc;
+    Vec16<TV> tc = zero16<TV>(), tn = tc, ts = tc, bb = tc, di = tc, fe = tc, fn = tc, fs = tc;
     if (act) {
-        tc = sa_ld(t + c);
-        tn = sa_ld(t + c + P);
-        ts = sa_ld(t + c - P);
-        bb = sa_ld(b + c);
-        di = sa_ld(A.dinv + c);
-        fe = sa_ld(A.fE + c);
-        fn = sa_ld(A.fN + c);
-        fs = sa_ld(A.fN + c - P);
+        tc = ld16(t + c);
+        tn = ld16(t + c + P);
+        ts = ld16(t + c - P);
+        bb = ld16(b + c);
+        di = ld16(A.dinv + c);
+        fe = ld16(A.fE + c);
+        fn = ld16(A.fN + c);
+        fs = ld16(A.fN + c - P);
     }
-    TV tw = sa_from_west(tc.v[V - 1]), te = sa_from_east(tc.v[0]), fw = sa_from_west(fe.v[V - 1]);
+    TV tw = from_west(tc.v[V - 1]), te = from_east(tc.v[0]), fw = from_west(fe.v[V - 1]);
     if (lane == 0) {
         const bool h = act && j0 > 0;
         tw = h ? t[c - 1] : (TV)0;
         fw = h ? A.fE[c - 1] : (TV)0;
     }
     if (lane == 31) te = act ? t[c + V] : (TV)0;
-    SaVec<TV> yv;
+    Vec16<TV> yv;
     double acc = 0.0;
 #pragma unroll
     for (int k = 0; k < V; ++k) {
@@ -869,7 +817,7 @@ __device__ __forceinline__ double sa0_smooth(const Sa0<TV>& A, TV om, const TV* 
         yv.v[k] = yk;
         acc += (double)bb.v[k] * (double)yk;
     }
-    if (act) sa_st(y + c, yv);
+    if (act) st16(y + c, yv);
     return acc;
 }
 
@@ -1078,7 +1026,7 @@ __global__ void __launch_bounds__(512, 1) k_pcg_sa(KParams k, Status* st, const 
     const SaLevel<TV>& C1 = H.lv[1];
     auto vcycle = [&](double& rz, bool first) __attribute__((always_inline)) -> bool {
         if (first) {
-            sa_rows<TV>(L0.nI, L0.nJ, [&](int i, int j0, bool act, int lane) {
+            row_segments<TV>(L0.nI, L0.nJ, [&](int i, int j0, bool act, int lane) {
                 sa0_resid(A0f, omT, L0.b, L0.x, L0.t, i, j0, act, lane);
             });
             target += G;
@@ -1111,16 +1059,16 @@ __global__ void __launch_bounds__(512, 1) k_pcg_sa(KParams k, Status* st, const 
         }
         double acc[1] = {0.0};
         if (H.split0) {
-            sa_rows<TV>(L0.nI, L0.nJ, [&](int i, int j0, bool act, int lane) {
+            row_segments<TV>(L0.nI, L0.nJ, [&](int i, int j0, bool act, int lane) {
                 sa0_prolong_t(A0f, L0.x, C1.y, C1.P, L0.t, i, j0, act);
             });
             target += G;
             if (!grid_barrier(bar, target, &st->err)) return false;
-            sa_rows<TV>(L0.nI, L0.nJ, [&](int i, int j0, bool act, int lane) {
+            row_segments<TV>(L0.nI, L0.nJ, [&](int i, int j0, bool act, int lane) {
                 acc[0] += sa0_smooth(A0f, omT, L0.b, L0.t, L0.y, i, j0, act, lane);
             });
         } else {
-            sa_rows<TV>(L0.nI, L0.nJ, [&](int i, int j0, bool act, int lane) {
+            row_segments<TV>(L0.nI, L0.nJ, [&](int i, int j0, bool act, int lane) {
                 acc[0] += sa0_prolong(A0f, L0.x, L0.b, C1.y, C1.P, omT, L0.y, i, j0, act, lane);
             });
         }
@@ -1147,7 +1095,7 @@ __global__ void __launch_bounds__(512, 1) k_pcg_sa(KParams k, Status* st, const 
         const TV bt = (TV)beta;
         const bool first = it == 0;
         double accA[1] = {0.0};
-        sa_rows<TV>(L0.nI, L0.nJ, [&](int i, int j0, bool act, int lane) {
+        row_segments<TV>(L0.nI, L0.nJ, [&](int i, int j0, bool act, int lane) {
             accA[0] += sa0_matvec(A0f, L0.y, pold, bt, first, pnew, B.Ap, i, j0, act, lane);
         });
         block_sum<1>(accA, sm);
@@ -1161,7 +1109,7 @@ __global__ void __launch_bounds__(512, 1) k_pcg_sa(KParams k, Status* st, const 
         const TV* rold = rbuf[it & 1];
         TV* rnew = rbuf[(it + 1) & 1];
         double accB[1] = {0.0};
-        sa_rows<TV>(L0.nI, L0.nJ, [&](int i, int j0, bool act, int lane) {
+        row_segments<TV>(L0.nI, L0.nJ, [&](int i, int j0, bool act, int lane) {
             accB[0] += sa0_update(A0f, al, omT, pnew, B.Ap, B.x, rold, rnew, L0.x, L0.t, i, j0, act, lane);
         });
         L0.b = rnew;
