@@ -78,6 +78,8 @@ def parse():
     ap.add_argument("--batch-adjoint-fields", type=int, default=64,
                     help="fields of the batch whose adjoint is timed after the run")
     ap.add_argument("--no-thermal", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true",
+                    help="skip the adjoint after the timed mixed solves (profiling runs)")
     ap.add_argument("--only", choices=["thermal", "batch"], default=None,
                     help="run one leg alone and print its JSON object (profiling runs)")
     ap.add_argument("--thermal-ny", type=int, default=512)
@@ -619,11 +621,12 @@ def main():
         return out, dp_end, adj
 
     with ClockSampler(local) as clk:
-        t_mix, dp_mix_k, adj_reps = timed_solves("mixed", kmix, args.warmup, args.steps, adjoint=True)
+        t_mix, dp_mix_k, adj_reps = timed_solves("mixed", kmix, args.warmup, args.steps,
+                                                 adjoint=not args.no_adjoint)
         t_64, dp_64_k, _ = timed_solves("fp64", k64, 1, 1)
     clocks = clk.summary()
     t_mixed = max(t_mix)
-    t_adj = max(r["device_ms"] for r in adj_reps) / 1e3
+    t_adj = max(r["device_ms"] for r in adj_reps) / 1e3 if adj_reps else None
     t_mixed = max_over_ranks(t_mixed, dist, "cuda")
 
     # ---- per-kernel device times and the roofline of the dominant kernel
@@ -739,15 +742,18 @@ def main():
             "e2e": {"value": float(np.mean(e2e_t)), "unit": "s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
             "clocks": clocks,
-            "adjoint": {"t_s": t_adj, "over_forward_mixed": t_adj / t_mixed, "over_forward_fp64": t_adj / t_fp64,
-                        "iterations": int(max(r["iterations"] for r in adj_reps)),
-                        "residual": float(max(r["residual"] for r in adj_reps)), "tol": ADJ_TOL},
             "dp_star_pa": dp_star,
             "k_fp64": k64, "k_mixed": kmix,
             "dp_rel_err_fp64_at_k": abs(dp_64_k - dp_star) / abs(dp_star),
             "dp_rel_err_mixed_at_k": abs(dp_mix_k - dp_star) / abs(dp_star),
             "dp_rel_err_mixed_final": abs(dp_mix_final - dp_star) / abs(dp_star),
             "t_fp64_s": t_fp64, "t_mixed_s": t_mixed, "mixed_over_fp64": t_mixed / t_fp64,
+            "adjoint": None if not adj_reps else {
+                "t_s": t_adj, "over_forward_mixed": t_adj / t_mixed, "over_forward_fp64": t_adj / t_fp64,
+                "iterations": int(max(r["iterations"] for r in adj_reps)),
+                "residual": float(max(r["residual"] for r in adj_reps)), "tol": ADJ_TOL,
+                "model": {1: "equations", 2: "fixed point"}.get(int(adj_reps[0]["model"])),
+                "clamped_velocities": int(adj_reps[0]["clampedUnknowns"])},
         }
         print(json.dumps(rounded(line)))
     if dist:
