@@ -51,8 +51,8 @@ ADJ_MAX_ITER = 2000
 # ncu captures of the dominant kernels (profiles/): DRAM bytes read + written
 PCG_MG_CAPTURE_BYTES = (850.3 + 1406.4) * 1e6     # k_pcg_mg<float>, one launch
 PCG_MG_CAPTURE_ITERS = 30
-PCG_SA_CAPTURE_BYTES = None                        # k_pcg_sa<float>, one launch (not captured yet)
-PCG_SA_CAPTURE_ITERS = 1
+PCG_SA_CAPTURE_BYTES = (1780.3 + 1050.5) * 1e6    # k_pcg_sa<float>, one launch of 16 CG iterations
+PCG_SA_CAPTURE_ITERS = 16
 THERMAL_CAPTURE_BYTES_PER_CELL_ITER = 702.0        # k_th_bicgstab, 512 x 256 x 12 capture
 
 
@@ -471,6 +471,45 @@ def batch_leg(Simple, torch, args, rank: int = 0, world: int = 1, dist=None) -> 
 # ------------------------------------------------------------------ 3-D thermal solve + p-norm adjoint
 THERMAL_FLOW_ITERS = 300
 THERMAL_P = 8.0
+# the thermal leg's CPU sample: the same assembled system on a smaller plane
+# (the reference's solver, AMGCL, is not vendored)
+THERMAL_CPU_NY, THERMAL_CPU_NX = 64, 128
+
+
+def thermal_cpu_baseline(Simple, args) -> dict:
+    """The thermal system of the reference (thermal_solver.cpp:437-528, as
+    restated in oracle/thermal_oracle.py) at 128 x 64 x 12 on a flow of the
+    same workload, solved on the host by SciPy BiCGStab (rtol 1e-6, the leg's
+    tolerance) preconditioned by an incomplete LU (drop 1e-4, fill 5): the
+    stand-in BASELINE.md plans for the reference's AMGCL IDR(8) solve.  A
+    bounded sample (about 10-20 s on one core); it reports the solve time and
+    unknowns per second."""
+    import scipy.sparse.linalg as spl
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import thermal_oracle as tho
+    from coldplate_b200 import cases
+    from coldplate_b200.thermal import inputs_from_flow
+    Ny, Nx = THERMAL_CPU_NY, THERMAL_CPU_NX
+    c = cases.density_field(Ny, Nx, seed=args.seed, **BENCH_KNOBS)
+    with Simple(cellType=c.cellType, **c.params(precision="mixed", maxIterations=THERMAL_FLOW_ITERS + 2,
+                                                 epsilon=1e-30)) as s:
+        s.step(THERMAL_FLOW_ITERS)
+        fl = inputs_from_flow(s, c.cellType)
+    q0 = cases.power_map(Ny, Nx, args.seed) * 1e4
+    p = tho.ThermalParams(Nx=Nx, Ny=Ny, dx=c.hx, dy=c.hy, **cases.THERMAL_3D)
+    A, b = tho.assemble(p, fl["gamma"], fl["u_xy"], fl["v_xy"], q0)
+    t0 = time.perf_counter()
+    ilu = spl.spilu(A.tocsc(), drop_tol=1e-4, fill_factor=5)
+    M = spl.LinearOperator(A.shape, ilu.solve)
+    its = [0]
+    x, info = spl.bicgstab(A, b, rtol=1e-6, maxiter=5000, M=M, callback=lambda xk: its.__setitem__(0, its[0] + 1))
+    t = time.perf_counter() - t0
+    res = float(np.linalg.norm(b - A @ x) / np.linalg.norm(b))
+    return {"value": t, "unit": "s", "cores": 1, "kind": "port",
+            "sample": f"the reference's thermal system at {Nx}x{Ny}x{p.Nz} ({A.shape[0]} unknowns, assembled by "
+                      f"oracle/thermal_oracle.py) solved by SciPy BiCGStab + ILU (drop 1e-4, fill 5) to rtol 1e-6: "
+                      f"{its[0]} iterations, residual {res:.1e}; a stand-in for AMGCL IDR(8), which is not vendored",
+            "unknowns_per_s": A.shape[0] / t}
 
 
 def thermal_leg(Simple, torch, args) -> dict:
@@ -684,6 +723,8 @@ def main():
     thermal_line = None
     if not args.no_thermal:
         thermal_line = thermal_leg(Simple, torch, args)
+        if not args.no_cpu_baseline:
+            thermal_line["cpu_baseline"] = thermal_cpu_baseline(Simple, args)
 
     # ---- end to end through the public API with host buffers
     e2e_t = []

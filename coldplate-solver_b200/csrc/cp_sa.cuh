@@ -73,10 +73,10 @@ struct SaHier {
     TV* dense;              // inverse of the coarsest operator
     double omega, w0, wc;   // Jacobi damping, prolongator smoothing weights
     TV* r2;                 // second CG residual buffer (the residual ping-pongs)
-    int reuse;              // rebuild the coarse operators every `reuse` outer iterations
+    int reuse;              // rebuild the coarse operators every `reuse` outer iterations (0: only when
+                            // the flag says they are stale)
     int split0;             // level-0 prolongation and post-smoothing as two passes
-    int force;              // 1: rebuild now and leave the hierarchy marked stale
-    int* dirty;             // device flag: the stored hierarchy is not the forward's
+    int* dirty;             // device flag: the stored hierarchy is stale (cleared by a rebuild)
     unsigned long long* prof;  // optional per-phase device time (ns, block 0's view), or null
 };
 
@@ -847,9 +847,12 @@ __global__ void __launch_bounds__(512, 1) k_pcg_sa(KParams k, Status* st, const 
     } while (0)
     // the coarse operators are rebuilt every H.reuse outer iterations (they
     // only precondition: the CG matvec and level 0's smoother and
-    // prolongation always use the current operator), and whenever the stored
-    // ones are not the forward's
-    const bool rebuild = H.force || *(volatile int*)H.dirty || H.reuse <= 1 || (st->iter % H.reuse) == 0;
+    // prolongation always use the current operator), after a solve that
+    // reached the iteration cap with them (early in a run the operator moves
+    // fast), and whenever the stored ones are stale (the operator changed
+    // from the host, or another solve such as the adjoint's stored its own)
+    const bool rebuild = *(volatile int*)H.dirty ||
+                         (H.reuse > 0 && (H.reuse == 1 || (st->iter % H.reuse) == 0 || st->itersP >= k.maxP));
 
     SaLevel<TV> L0 = H.lv[0];
     L0.b = B.r;
@@ -1133,8 +1136,7 @@ __global__ void __launch_bounds__(512, 1) k_pcg_sa(KParams k, Status* st, const 
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         st->itersP = it;
-        if (H.force) *H.dirty = 1;
-        else if (rebuild) *H.dirty = 0;
+        if (rebuild) *H.dirty = 0;
     }
 #undef SA_SYNC
 }

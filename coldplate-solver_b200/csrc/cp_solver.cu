@@ -123,6 +123,7 @@ struct cp_ctx {
     int saReuse = 8;                         // outer iterations between coarse-operator rebuilds
     int saSplit0 = 1;                        // level-0 prolongation in two passes
     int* saDirty = nullptr;                  // device flag: rebuild the coarse operators on the next solve
+    int* saDirtyAdj = nullptr;               // the same flag for the adjoint's pressure-like solves
     MgMaps mgMaps;                           // TMA tensor maps of the level-0 tile phases
     // adjoint buffers (allocated on first use, double)
     double* adj[40] = {};
@@ -499,7 +500,6 @@ SaHier<TV> sa_hier(cp_ctx* c) {
     H.dinv0 = (TV*)c->saDinv0;
     H.reuse = c->saReuse;
     H.split0 = c->saSplit0;
-    H.force = 0;
     H.dirty = c->saDirty;
     for (int q = 0; q < 9; ++q) H.Y[q] = (TV*)c->saY[q];
     for (int l = 0; l < c->saL; ++l) {
@@ -534,9 +534,11 @@ cp_status sa_build(cp_ctx* c) {
         nI = sa_coarse(nI); nJ = sa_coarse(nJ);
     }
     c->saL = L;
+    size_t budget = kSaSmemBudget;
+    if (const char* e = getenv("CP_SA_SMEM_KB")) budget = std::min(budget, (size_t)std::max(atoi(e), 1) * 1024);
     int Lg = 1;
     while (Lg < L - 1 && ((long long)c->saNI[Lg] * c->saNJ[Lg] > kSaCtaCells ||
-                          sa_cta_elems(c->saNI, c->saNJ, Lg, L) * c->es > kSaSmemBudget))
+                          sa_cta_elems(c->saNI, c->saNJ, Lg, L) * c->es > budget))
         ++Lg;
     c->saLg = Lg;
     c->saSmem = std::max(kSaDynSmem, sa_cta_elems(c->saNI, c->saNJ, Lg, L) * c->es);
@@ -549,6 +551,7 @@ cp_status sa_build(cp_ctx* c) {
         if ((s = dalloc_bytes(c, &c->saArr[0][q], c->nElem * c->es)) != CP_OK) return s;
     if ((s = dalloc_bytes(c, &c->saDinv0, c->nElem * c->es)) != CP_OK) return s;
     if ((s = dalloc(c, &c->saDirty, 1)) != CP_OK) return s;
+    if ((s = dalloc(c, &c->saDirtyAdj, 1)) != CP_OK) return s;
     const int one = 1;
     CK(cudaMemcpyAsync(c->saDirty, &one, sizeof(int), cudaMemcpyHostToDevice, c->stream));
     CK(cudaStreamSynchronize(c->stream));
@@ -1228,7 +1231,11 @@ cp_status adjoint_pcg(cp_ctx* c, const KParams& k, const double* dE, const doubl
     CK(cudaMemsetAsync(c->adjBar, 0, sizeof(unsigned), c->stream));
     if (c->useSa) {
         SaHier<TV> H = sa_hier<TV>(c);
-        H.force = 1;   // the adjoint's operator: rebuild, and leave the forward's marked stale
+        // the adjoint's operator is fixed over one adjoint solve: built by its
+        // first pressure-like solve, reused by the rest (the caller marks both
+        // flags stale at the start)
+        H.dirty = c->saDirtyAdj;
+        H.reuse = 0;
         CK(launch_coop_cfg(k_pcg_sa<TV>, c->gMg, kMgThreads, c->saSmem, c->stream, k, c->adjSt, dE, dN, B, H, out,
                            c->adjPart, c->adjBar));
     } else if (c->useMg) {
@@ -1304,6 +1311,13 @@ static cp_status adjoint_impl(cp_ctx* c, double* grad, long rows, long cols, lon
     const int M = c->d.M, N = c->d.N;
     cp_status s = adjoint_alloc(c);
     if (s != CP_OK) return s;
+    // the adjoint's pressure-like solves store their own coarse operators:
+    // built once for this solve, and the forward's rebuilt after it
+    if (c->saDirtyAdj) {
+        static const int one = 1;
+        CK(cudaMemcpyAsync(c->saDirtyAdj, &one, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+        if ((s = mark_sa_stale(c)) != CP_OK) return s;
+    }
     CK(cudaEventRecord(c->ev0, c->stream));
     // vectors
     double** A = c->adj;
