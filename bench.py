@@ -49,11 +49,11 @@ BENCH_KNOBS = dict(pressureSolverType=4, maxPressureIter=30, pTol=1e-6)
 ADJ_TOL = 1e-6
 ADJ_MAX_ITER = 2000
 # ncu captures of the dominant kernels (profiles/): DRAM bytes read + written
-PCG_MG_CAPTURE_BYTES = (850.3 + 1406.4) * 1e6     # k_pcg_mg<float>, one launch
+PCG_MG_CAPTURE_BYTES = (762.0 + 1447.7) * 1e6     # k_pcg_mg<float>, one launch (32 x 64 tiles)
 PCG_MG_CAPTURE_ITERS = 30
 PCG_SA_CAPTURE_BYTES = (1780.3 + 1050.5) * 1e6    # k_pcg_sa<float>, one launch of 16 CG iterations
 PCG_SA_CAPTURE_ITERS = 16
-THERMAL_CAPTURE_BYTES_PER_CELL_ITER = 702.0        # k_th_bicgstab, 512 x 256 x 12 capture
+THERMAL_CAPTURE_BYTES_PER_CELL_ITER = 693.0        # k_th_bicgstab, 512 x 256 x 12 capture (78 iterations)
 
 
 def parse():
@@ -587,7 +587,7 @@ def thermal_leg(Simple, torch, args) -> dict:
                          "kernel": "k_th_bicgstab<false> (assembly and factorisation inside the time)",
                          "traffic": THERMAL_CAPTURE_BYTES_PER_CELL_ITER * n * its_f,
                          "algorithmic_bytes": bytes_iter * its_f,
-                         "traffic_source": "ncu capture at 512x256x12 (10 iterations), scaled by cells x iterations; "
+                         "traffic_source": "ncu capture at 512x256x12 (78 iterations), scaled by cells x iterations; "
                                            "L2 holds more of the smaller case, so this is a lower bound",
                          "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"},
             "e2e": {"value": float(np.mean(e2e)), "unit": "s", "h2d_bytes_per_step": int(4 * 8 * Nx * Ny),
