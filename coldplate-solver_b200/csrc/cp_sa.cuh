@@ -209,6 +209,24 @@ __device__ __forceinline__ double sa_pk(const St& A, int i, int j, int I, int J,
     return (in_agg(i, j) ? 1.0 : 0.0) - w * s / A(i, j, 4);
 }
 
+// coarse row (I, J) from its entries towards the coarse unknowns of each
+// colour c (the colour-c neighbour sits at offsets in {-1, 0, 1} with
+// matching residues)
+template <typename TV>
+__device__ __forceinline__ void sa_store_row(const SaLevel<TV>& C, int I, int J, const double (&ac)[9]) {
+    const size_t qc = (size_t)I * C.P + J;
+    const int ai = (I - 1) % 3, aj = (J - 1) % 3;
+#pragma unroll
+    for (int c = 0; c < 9; ++c) {
+        const int di = ((c / 3 - ai + 4) % 3) - 1, dj = ((c % 3 - aj + 4) % 3) - 1;
+        const int k = (di + 1) * 3 + (dj + 1);
+        const bool in = I + di >= 1 && I + di <= C.nI && J + dj >= 1 && J + dj <= C.nJ;
+        double v = in ? ac[c] : 0.0;
+        if (k == 4 && !(v > 0.0)) v = 1.0;   // guard: an isolated coarse unknown
+        C.c[k][qc] = (TV)v;
+    }
+}
+
 // coarse row (I, J) of A_c = P^T A P from the probes of the fine level
 template <typename TV, class St>
 __device__ __forceinline__ void sa_galerkin_cell(const St& A, int Pf, TV* const* Y, const SaLevel<TV>& C, double w,
@@ -227,18 +245,7 @@ __device__ __forceinline__ void sa_galerkin_cell(const St& A, int Pf, TV* const*
             for (int c = 0; c < 9; ++c) ac[c] += p * (double)Y[c][q];
         }
     }
-    const size_t qc = (size_t)I * C.P + J;
-    const int ai = (I - 1) % 3, aj = (J - 1) % 3;
-#pragma unroll
-    for (int c = 0; c < 9; ++c) {
-        // the neighbour of colour c: offsets in {-1, 0, 1} with matching residues
-        const int di = ((c / 3 - ai + 4) % 3) - 1, dj = ((c % 3 - aj + 4) % 3) - 1;
-        const int k = (di + 1) * 3 + (dj + 1);
-        const bool in = I + di >= 1 && I + di <= C.nI && J + dj >= 1 && J + dj <= C.nJ;
-        double v = in ? ac[c] : 0.0;
-        if (k == 4 && !(v > 0.0)) v = 1.0;   // guard: an isolated coarse unknown
-        C.c[k][qc] = (TV)v;
-    }
+    sa_store_row(C, I, J, ac);
 }
 
 // ---------------------------------------------------------------- prolongation weights
@@ -271,6 +278,65 @@ __device__ __forceinline__ void sa_pweights(const St& A, int i, int j, double w,
     pw[1] = -sc * s[1];
     pw[2] = -sc * s[2];
     pw[3] = -sc * s[3];
+}
+
+// The same probes and Galerkin rows from the stored prolongation weights of
+// the fine level f (its own, horizontal, vertical and diagonal aggregate;
+// Diag false on the 5-point level 0, which has no diagonal weight):
+// Y_c(i, j) = sum over the stencil of A_(ij),m P(m, agg) [colour(agg) = c],
+// and row (I, J) = sum over the 5 x 5 support of P(m, (I, J)) Y_c(m).
+template <typename TV, class St, bool Diag>
+__device__ __forceinline__ void sa_probe_w(const St& A, const SaLevel<TV>& f, TV* const* Y, int i, int j) {
+    double y[9];
+#pragma unroll
+    for (int c = 0; c < 9; ++c) y[c] = 0.0;
+    auto add = [&](int cc, double v) {
+#pragma unroll
+        for (int c = 0; c < 9; ++c) y[c] += (c == cc) ? v : 0.0;
+    };
+#pragma unroll
+    for (int a = 0; a < St::kN; ++a) {
+        const int k = St::k_of(a);
+        const int mi = i + sa_di(k), mj = j + sa_dj(k);
+        if (mi < 1 || mi > A.nI || mj < 1 || mj > A.nJ) continue;
+        const double akm = A(i, j, k);
+        if (akm == 0.0) continue;
+        const size_t qm = (size_t)mi * f.P + mj;
+        const int ci = (mi - 1) / 3 % 3, cj = (mj - 1) / 3 % 3;
+        const int cjh = (cj + sa_side(mj) + 3) % 3, civ = (ci + sa_side(mi) + 3) % 3;
+        add(ci * 3 + cj, akm * (double)f.pw[0][qm]);
+        add(ci * 3 + cjh, akm * (double)f.pw[1][qm]);
+        add(civ * 3 + cj, akm * (double)f.pw[2][qm]);
+        if (Diag) add(civ * 3 + cjh, akm * (double)f.pw[3][qm]);
+    }
+    const size_t q = (size_t)i * f.P + j;
+#pragma unroll
+    for (int c = 0; c < 9; ++c) Y[c][q] = (TV)y[c];
+}
+template <typename TV, bool Corners>
+__device__ __forceinline__ void sa_galerkin_w(const SaLevel<TV>& f, TV* const* Y, const SaLevel<TV>& C, int I,
+                                              int J) {
+    double ac[9];
+#pragma unroll
+    for (int c = 0; c < 9; ++c) ac[c] = 0.0;
+    const int i0 = 3 * I - 3, j0 = 3 * J - 3;
+#pragma unroll
+    for (int a = 0; a < 5; ++a) {
+        const int ii = i0 + a;
+        const int ra = (a == 0 || a == 4) ? 1 : 0;
+#pragma unroll
+        for (int b = 0; b < 5; ++b) {
+            const int rb = (b == 0 || b == 4) ? 1 : 0;
+            if (!Corners && ra && rb) continue;
+            const int jj = j0 + b;
+            if (ii < 1 || ii > f.nI || jj < 1 || jj > f.nJ) continue;
+            const size_t q = (size_t)ii * f.P + jj;
+            const double p = (double)f.pw[2 * ra + rb][q];
+#pragma unroll
+            for (int c = 0; c < 9; ++c) ac[c] += p * (double)Y[c][q];
+        }
+    }
+    sa_store_row(C, I, J, ac);
 }
 
 // ---------------------------------------------------------------- cycle pieces
@@ -914,33 +980,38 @@ __global__ void __launch_bounds__(512, 1) k_pcg_sa(KParams k, Status* st, const 
     // ---- set-up: coarse operators by coloured probes (when rebuilt), with
     // the prolongation weights of the grid-wide coarse levels
     if (rebuild) {
+        // every level grid-wide; levels with stored prolongation weights
+        // (level 0 from the set-up, the grid-wide coarse levels from a pass
+        // of their own) probe and contract with them
         for (int l = 0; l < H.L - 1; ++l) {
-            const bool grid = l < H.Lg;
-            if (!grid && blockIdx.x != 0) continue;
-            const SaSplit sp = grid ? all : cta;
             const SaLevel<TV>& f = H.lv[l];
-            if (l == 0) {
-                sa_cells(sp, f.nI, f.nJ, [&](int i, int j) { sa_probe_cell(A0, f.P, H.Y, wgt(l), i, j); });
-            } else {
-                sa_cells(sp, f.nI, f.nJ, [&](int i, int j) {
-                    sa_probe_cell(stencil(l), f.P, H.Y, wgt(l), i, j);
-                    if (grid) {
-                        double pw[4];
-                        sa_pweights(stencil(l), i, j, wgt(l), pw);
-                        const size_t q = (size_t)i * f.P + j;
-#pragma unroll
-                        for (int m = 0; m < 4; ++m) f.pw[m][q] = (TV)pw[m];
-                    }
-                });
-            }
-            if (grid) SA_SYNC(); else __syncthreads();
             const SaLevel<TV>& C = H.lv[l + 1];
+            const bool wts = l < H.Lg;
+            if (wts && l > 0) {
+                sa_cells(all, f.nI, f.nJ, [&](int i, int j) {
+                    double pw[4];
+                    sa_pweights(stencil(l), i, j, wgt(l), pw);
+                    const size_t q = (size_t)i * f.P + j;
+#pragma unroll
+                    for (int m = 0; m < 4; ++m) f.pw[m][q] = (TV)pw[m];
+                });
+                SA_SYNC();
+            }
             if (l == 0)
-                sa_cells(sp, C.nI, C.nJ, [&](int I, int J) { sa_galerkin_cell(A0, f.P, H.Y, C, wgt(l), I, J); });
+                sa_cells(all, f.nI, f.nJ, [&](int i, int j) { sa_probe_w<TV, Stencil5<TV>, false>(A0, L0, H.Y, i, j); });
+            else if (wts)
+                sa_cells(all, f.nI, f.nJ, [&](int i, int j) { sa_probe_w<TV, Stencil9<TV>, true>(stencil(l), f, H.Y, i, j); });
             else
-                sa_cells(sp, C.nI, C.nJ,
+                sa_cells(all, f.nI, f.nJ, [&](int i, int j) { sa_probe_cell(stencil(l), f.P, H.Y, wgt(l), i, j); });
+            SA_SYNC();
+            if (l == 0)
+                sa_cells(all, C.nI, C.nJ, [&](int I, int J) { sa_galerkin_w<TV, false>(L0, H.Y, C, I, J); });
+            else if (wts)
+                sa_cells(all, C.nI, C.nJ, [&](int I, int J) { sa_galerkin_w<TV, true>(f, H.Y, C, I, J); });
+            else
+                sa_cells(all, C.nI, C.nJ,
                          [&](int I, int J) { sa_galerkin_cell(stencil(l), f.P, H.Y, C, wgt(l), I, J); });
-            if (grid) SA_SYNC(); else __syncthreads();
+            SA_SYNC();
         }
         if (blockIdx.x == 0) sa_dense_setup(H.lv[H.L - 1], H.dense, dsm);
         SA_SYNC();

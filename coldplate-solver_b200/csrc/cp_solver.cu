@@ -120,7 +120,7 @@ struct cp_ctx {
     void* saDense = nullptr;
     double saOmega = 0.9, saW0 = 2.0 / 3.0, saWc = 0.8;
     unsigned long long* saProf = nullptr;    // per-phase timers when CP_SA_PROFILE is set
-    int saReuse = 8;                         // outer iterations between coarse-operator rebuilds
+    int saReuse = 4;                         // outer iterations between coarse-operator rebuilds
     int saSplit0 = 1;                        // level-0 prolongation in two passes
     int* saDirty = nullptr;                  // device flag: rebuild the coarse operators on the next solve
     int* saDirtyAdj = nullptr;               // the same flag for the adjoint's pressure-like solves
@@ -235,11 +235,9 @@ void fill_kparams(cp_ctx* c) {
 
 // density -> gamma (1 - clamp(cellType)) with the padded row/column copied,
 // alpha by RAMP (SIMPLE.cpp:667-676, 707-729, 766-772); all M x N, double.
-void build_density(const cp_ctx* c, const std::vector<double>& cellTypePadded, std::vector<double>& gamma,
-                   std::vector<double>& alpha) {
+void build_density(const cp_ctx* c, const std::vector<double>& cellTypePadded, std::vector<double>& gamma) {
     const int M = c->d.M, N = c->d.N, pr = M - 1, pc = N - 1;
     gamma.assign((size_t)M * N, 1.0);
-    alpha.assign((size_t)M * N, 0.0);
     for (int i = 0; i < pr; ++i)
         for (int j = 0; j < pc; ++j) {
             const double val = cellTypePadded[(size_t)i * N + j];
@@ -248,11 +246,16 @@ void build_density(const cp_ctx* c, const std::vector<double>& cellTypePadded, s
         }
     for (int i = 0; i < pr; ++i) gamma[(size_t)i * N + pc] = gamma[(size_t)i * N + pc - 1];
     for (int j = 0; j < N; ++j) gamma[(size_t)pr * N + j] = gamma[(size_t)(pr - 1) * N + std::min(j, pc - 1)];
-    const double amax = c->prm.eta / std::max(c->prm.brinkmanKMin, 1e-20);
-    const double q = c->prm.brinkmanQ;
-    for (size_t k = 0; k < (size_t)M * N; ++k) {
-        const double g = gamma[k];
-        alpha[k] = amax * (1.0 - g) / (1.0 + q * g + 1e-10);
+}
+
+// RAMP interpolation alpha = alpha_max (1 - gamma) / (1 + q gamma + 1e-10)
+// (SIMPLE.cpp:770) over the M x N cells, rounded step by step as the host
+// formula (no fused multiply-add)
+__global__ void k_alpha(const double* gamma, double* alpha, int M, int N, int P, double amax, double q) {
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < M * N; t += gridDim.x * blockDim.x) {
+        const int i = t / N, j = t - i * N;
+        const double g = gamma[(size_t)i * P + j];
+        alpha[(size_t)i * P + j] = __ddiv_rn(__dmul_rn(amax, 1.0 - g), __dadd_rn(__dadd_rn(1.0, __dmul_rn(q, g)), 1e-10));
     }
 }
 
@@ -265,12 +268,13 @@ cp_status mark_sa_stale(cp_ctx* c) {
     return CP_OK;
 }
 
-cp_status upload_cells(cp_ctx* c, const std::vector<double>& g, const std::vector<double>& a) {
+cp_status upload_cells(cp_ctx* c, const std::vector<double>& g) {
     const int M = c->d.M, N = c->d.N;
     CK(cudaMemcpy2DAsync(c->gamma, (size_t)c->d.P * 8, g.data(), (size_t)N * 8, (size_t)N * 8, M,
                          cudaMemcpyHostToDevice, c->stream));
-    CK(cudaMemcpy2DAsync(c->alpha, (size_t)c->d.P * 8, a.data(), (size_t)N * 8, (size_t)N * 8, M,
-                         cudaMemcpyHostToDevice, c->stream));
+    const double amax = c->prm.eta / std::max(c->prm.brinkmanKMin, 1e-20);
+    k_alpha<<<c->gElem, kThreads, 0, c->stream>>>(c->gamma, c->alpha, M, N, c->d.P, amax, c->prm.brinkmanQ);
+    CK(cudaGetLastError());
     cp_status s = mark_sa_stale(c);
     if (s != CP_OK) return s;
     CK(cudaStreamSynchronize(c->stream));
@@ -949,9 +953,9 @@ cp_status cp_create(const cp_params* prm, cp_ctx** out) {
     memset(c->stHost, 0, sizeof(Status));
     // all fluid until a geometry is set (SIMPLE.cpp:267-269)
     c->cellTypeHost.assign((size_t)M * N, 0.0);
-    std::vector<double> g, a;
-    build_density(c, c->cellTypeHost, g, a);
-    if ((s = upload_cells(c, g, a)) != CP_OK) return bail(s);
+    std::vector<double> g;
+    build_density(c, c->cellTypeHost, g);
+    if ((s = upload_cells(c, g)) != CP_OK) return bail(s);
     if (cudaStreamSynchronize(c->stream) != cudaSuccess) return bail(fail(CP_ERR_CUDA, "initialisation failed"));
     *out = c;
     return CP_OK;
@@ -995,9 +999,9 @@ cp_status cp_set_cell_type(cp_ctx* c, const double* ct, long rows, long cols, lo
     // pad the extra row/column by copy (SIMPLE.cpp:667-676)
     for (int i = 0; i < pr; ++i) P[(size_t)i * N + pc] = P[(size_t)i * N + pc - 1];
     for (int j = 0; j < N; ++j) P[(size_t)pr * N + j] = P[(size_t)(pr - 1) * N + std::min(j, pc - 1)];
-    std::vector<double> g, a;
-    build_density(c, P, g, a);
-    return upload_cells(c, g, a);
+    std::vector<double> g;
+    build_density(c, P, g);
+    return upload_cells(c, g);
 }
 
 cp_status cp_set_gamma(cp_ctx* c, const double* gm, long rows, long cols, long rs, long cs) {
@@ -1029,6 +1033,13 @@ cp_status cp_get_field(cp_ctx* c, cp_field which, double* host, long rows, long 
     int R = 0, C = 0;
     if (!field_shape(c, which, &dp, &R, &C)) return fail(CP_ERR_BAD_PARAM, "unknown field %d", (int)which);
     if (rows != R || cols != C) return fail(CP_ERR_BAD_PARAM, "shape %ld x %ld, expected %d x %d", rows, cols, R, C);
+    if (which != CP_FIELD_CELLTYPE && cs == 1 && rs >= C) {
+        // rows of the caller's array directly (pinned memory goes by DMA)
+        CK(cudaMemcpy2DAsync(host, (size_t)rs * 8, dp, (size_t)c->d.P * 8, (size_t)C * 8, R, cudaMemcpyDeviceToHost,
+                             c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        return CP_OK;
+    }
     std::vector<double> dense((size_t)R * C);
     if (which == CP_FIELD_CELLTYPE) {
         dense = c->cellTypeHost;
