@@ -75,7 +75,6 @@ struct SaHier {
     TV* r2;                 // second CG residual buffer (the residual ping-pongs)
     int reuse;              // rebuild the coarse operators every `reuse` outer iterations (0: only when
                             // the flag says they are stale)
-    int split0;             // level-0 prolongation and post-smoothing as two passes
     int* dirty;             // device flag: the stored hierarchy is stale (cleared by a rebuild)
     unsigned long long* prof;  // optional per-phase device time (ns, block 0's view), or null
 };
@@ -359,11 +358,11 @@ __device__ __forceinline__ void sa_resid_cell(const SaLevel<TV>& f, int i, int j
     f.t[q] = (TV)((double)f.b[q] - sa9_av(f, f.x, q));
 }
 
-// restriction, part 2 with stored weights (coarse unknown): b_c = (P^T t)_c
-// over the aggregate's 5 x 5 support (the ring rows / columns weigh in with
-// their vertical / horizontal / diagonal weights; no diagonal ones with
-// Corners false), and the pre-smoothed x_c = omega b_c / d_c
-template <typename TV, bool Corners>
+// restriction, part 2 with stored weights (coarse unknown of a 9-point
+// level): b_c = (P^T t)_c over the aggregate's 5 x 5 support (the ring rows
+// / columns weigh in with their vertical / horizontal / diagonal weights),
+// and the pre-smoothed x_c = omega b_c / d_c
+template <typename TV>
 __device__ __forceinline__ void sa_restrict_w(const SaLevel<TV>& f, const SaLevel<TV>& C, double omega, int I,
                                               int J) {
     const int i0 = 3 * I - 3, j0 = 3 * J - 3;
@@ -375,7 +374,6 @@ __device__ __forceinline__ void sa_restrict_w(const SaLevel<TV>& f, const SaLeve
 #pragma unroll
         for (int b = 0; b < 5; ++b) {
             const int rb = (b == 0 || b == 4) ? 1 : 0;
-            if (!Corners && ra && rb) continue;
             const int jj = j0 + b;
             if (ii < 1 || ii > f.nI || jj < 1 || jj > f.nJ) continue;
             const size_t q = (size_t)ii * f.P + jj;
@@ -699,65 +697,6 @@ __device__ __forceinline__ void sa0_resid(const Sa0<TV>& A, TV om, const TV* __r
     if (act) st16(t + c, tt);
 }
 
-// prolongation from level 1 fused with level 0's post-smoothing:
-// t = x0 + P e on the lane group and its neighbours (P e = pO e(own) +
-// pH e(horizontal) + pV e(vertical)), then
-// y = t + omega (b - A t) / d = (1 - omega) t + omega (b + sum f t(nb)) / d.
-// Writes y, returns the group's share of b.y.
-template <typename TV>
-__device__ __forceinline__ double sa0_prolong(const Sa0<TV>& A, const TV* __restrict__ x0, const TV* __restrict__ b,
-                                              const TV* __restrict__ e, int Pc, TV om, TV* __restrict__ y, int i,
-                                              int j0, bool act, int lane) {
-    constexpr int V = Vec16<TV>::n;
-    const int P = A.P, c = i * P + j0;
-    // t at (ii, jj) from its x0 and weights; 0 outside the unknowns
-    auto tat = [&](int ii, int jj, TV xv, TV po, TV ph, TV pv) -> TV {
-        if (ii < 1 || ii > A.nI || jj < 1 || jj > A.nJ) return (TV)0;
-        const TV* er = e + ((ii - 1) / 3 + 1) * Pc + (jj - 1) / 3 + 1;
-        return xv + po * er[0] + ph * er[sa_side(jj)] + pv * er[sa_side(ii) * Pc];
-    };
-    auto trow = [&](int ii) -> Vec16<TV> {
-        const int q = ii * P + j0;
-        const Vec16<TV> xv = ld16(x0 + q), po = ld16(A.pO + q), ph = ld16(A.pH + q), pv = ld16(A.pV + q);
-        Vec16<TV> o;
-#pragma unroll
-        for (int k = 0; k < V; ++k) o.v[k] = tat(ii, j0 + k, xv.v[k], po.v[k], ph.v[k], pv.v[k]);
-        return o;
-    };
-    auto tone = [&](int q, int jj) -> TV { return tat(i, jj, x0[q], A.pO[q], A.pH[q], A.pV[q]); };
-    Vec16<TV> tc = zero16<TV>(), tn = tc, ts = tc, bb = tc, di = tc, fe = tc, fn = tc, fs = tc;
-    if (act) {
-        tc = trow(i);
-        tn = trow(i + 1);
-        ts = trow(i - 1);
-        bb = ld16(b + c);
-        di = ld16(A.dinv + c);
-        fe = ld16(A.fE + c);
-        fn = ld16(A.fN + c);
-        fs = ld16(A.fN + c - P);
-    }
-    TV tw = from_west(tc.v[V - 1]), te = from_east(tc.v[0]), fw = from_west(fe.v[V - 1]);
-    if (lane == 0) {
-        const bool h = act && j0 > 0;
-        tw = h ? tone(c - 1, j0 - 1) : (TV)0;
-        fw = h ? A.fE[c - 1] : (TV)0;
-    }
-    if (lane == 31) te = act ? tone(c + V, j0 + V) : (TV)0;
-    Vec16<TV> yv;
-    double acc = 0.0;
-#pragma unroll
-    for (int k = 0; k < V; ++k) {
-        const TV W = k ? tc.v[k - 1] : tw, E = k < V - 1 ? tc.v[k + 1] : te, FW = k ? fe.v[k - 1] : fw;
-        TV yk = ((TV)1 - om) * tc.v[k] +
-                om * di.v[k] * (bb.v[k] + fe.v[k] * E + FW * W + fn.v[k] * tn.v[k] + fs.v[k] * ts.v[k]);
-        if (j0 + k < 1 || j0 + k > A.nJ) yk = (TV)0;
-        yv.v[k] = yk;
-        acc += (double)bb.v[k] * (double)yk;
-    }
-    if (act) st16(y + c, yv);
-    return acc;
-}
-
 // Restriction out of level 0 on aggregate-row segments: lane group g of
 // aggregate row I covers fine columns [12 g, 12 g + 12) and the aggregates
 // J = 4 g + 1 .. 4 g + 4 (own columns 3J-2 .. 3J, ring columns 3J-3 and
@@ -825,8 +764,13 @@ __device__ __forceinline__ void sa0_restrict_seg(const Sa0<TV>& A, const TV* __r
     }
 }
 
-// the same prolongation in two passes: t = x0 + P e on the lane group, then
-// (after a grid barrier) the post-smoothing from t; returns b.y
+// prolongation from level 1 and level 0's post-smoothing, two passes:
+// t = x0 + P e on the lane group (P e = pO e(own) + pH e(horizontal) +
+// pV e(vertical)); then, after a grid barrier,
+// y = t + omega (b - A t) / d = (1 - omega) t + omega (b + sum f t(nb)) / d,
+// which returns the group's share of b.y.  (One fused pass that recomputes
+// t at the neighbour rows measured slower: 30.6 against 22.9 us a cycle at
+// 2048 x 1024.)
 template <typename TV>
 __device__ __forceinline__ void sa0_prolong_t(const Sa0<TV>& A, const TV* __restrict__ x0, const TV* __restrict__ e,
                                               int Pc, TV* __restrict__ t, int i, int j0, bool act) {
@@ -1046,7 +990,7 @@ __global__ void __launch_bounds__(512, 1) k_pcg_sa(KParams k, Status* st, const 
         sa_cells(all, f.nI, f.nJ, [&](int i, int j) { sa_resid_cell(f, i, j); });
         target += G;
         if (!grid_barrier(bar, target, &st->err)) return false;
-        sa_cells(all, C.nI, C.nJ, [&](int I, int J) { sa_restrict_w<TV, true>(f, C, om, I, J); });
+        sa_cells(all, C.nI, C.nJ, [&](int I, int J) { sa_restrict_w(f, C, om, I, J); });
         target += G;
         return grid_barrier(bar, target, &st->err);
     };
@@ -1132,20 +1076,14 @@ __global__ void __launch_bounds__(512, 1) k_pcg_sa(KParams k, Status* st, const 
             tick(SA_P_UP + l);
         }
         double acc[1] = {0.0};
-        if (H.split0) {
-            row_segments<TV>(L0.nI, L0.nJ, [&](int i, int j0, bool act, int lane) {
-                sa0_prolong_t(A0f, L0.x, C1.y, C1.P, L0.t, i, j0, act);
-            });
-            target += G;
-            if (!grid_barrier(bar, target, &st->err)) return false;
-            row_segments<TV>(L0.nI, L0.nJ, [&](int i, int j0, bool act, int lane) {
-                acc[0] += sa0_smooth(A0f, omT, L0.b, L0.t, L0.y, i, j0, act, lane);
-            });
-        } else {
-            row_segments<TV>(L0.nI, L0.nJ, [&](int i, int j0, bool act, int lane) {
-                acc[0] += sa0_prolong(A0f, L0.x, L0.b, C1.y, C1.P, omT, L0.y, i, j0, act, lane);
-            });
-        }
+        row_segments<TV>(L0.nI, L0.nJ, [&](int i, int j0, bool act, int lane) {
+            sa0_prolong_t(A0f, L0.x, C1.y, C1.P, L0.t, i, j0, act);
+        });
+        target += G;
+        if (!grid_barrier(bar, target, &st->err)) return false;
+        row_segments<TV>(L0.nI, L0.nJ, [&](int i, int j0, bool act, int lane) {
+            acc[0] += sa0_smooth(A0f, omT, L0.b, L0.t, L0.y, i, j0, act, lane);
+        });
         block_sum<1>(acc, sm);
         if (threadIdx.x == 0) partB[2 * blockIdx.x + 1] = acc[0];
         target += G;

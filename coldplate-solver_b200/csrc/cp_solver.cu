@@ -121,7 +121,6 @@ struct cp_ctx {
     double saOmega = 0.9, saW0 = 2.0 / 3.0, saWc = 0.8;
     unsigned long long* saProf = nullptr;    // per-phase timers when CP_SA_PROFILE is set
     int saReuse = 4;                         // outer iterations between coarse-operator rebuilds
-    int saSplit0 = 1;                        // level-0 prolongation in two passes
     int* saDirty = nullptr;                  // device flag: rebuild the coarse operators on the next solve
     int* saDirtyAdj = nullptr;               // the same flag for the adjoint's pressure-like solves
     MgMaps mgMaps;                           // TMA tensor maps of the level-0 tile phases
@@ -503,7 +502,6 @@ SaHier<TV> sa_hier(cp_ctx* c) {
     H.r2 = (TV*)c->saArr[0][11];
     H.dinv0 = (TV*)c->saDinv0;
     H.reuse = c->saReuse;
-    H.split0 = c->saSplit0;
     H.dirty = c->saDirty;
     for (int q = 0; q < 9; ++q) H.Y[q] = (TV*)c->saY[q];
     for (int l = 0; l < c->saL; ++l) {
@@ -573,7 +571,6 @@ cp_status sa_build(cp_ctx* c) {
     if (const char* e = getenv("CP_SA_W0")) c->saW0 = atof(e);
     if (const char* e = getenv("CP_SA_WC")) c->saWc = atof(e);
     if (const char* e = getenv("CP_SA_REUSE")) c->saReuse = std::max(atoi(e), 1);
-    if (const char* e = getenv("CP_SA_SPLIT0")) c->saSplit0 = atoi(e) != 0;
     if (getenv("CP_SA_PROFILE") && (s = dalloc(c, &c->saProf, (size_t)SA_P_COUNT)) != CP_OK) return s;
     int nb = 0;
     if (c->prm.precision == CP_PREC_MIXED) {
@@ -986,32 +983,39 @@ cp_status cp_destroy(cp_ctx* c) {
     return CP_OK;
 }
 
-cp_status cp_set_cell_type(cp_ctx* c, const double* ct, long rows, long cols, long rs, long cs) {
+// The padded cell types (the extra row and column copied, SIMPLE.cpp:667-676)
+// from a strided host array of cell types or, with fromGamma, of densities
+// (cellType = 1 - gamma), checked for non-finite values before anything
+// changes; then the density field on the device.
+static cp_status set_cells(cp_ctx* c, const double* src, long rows, long cols, long rs, long cs, bool fromGamma) {
     if (!c) return fail(CP_ERR_BAD_PARAM, "ctx is NULL");
+    if (!src) return fail(CP_ERR_BAD_PARAM, "host pointer is NULL");
     const int M = c->d.M, N = c->d.N, pr = M - 1, pc = N - 1;
-    std::vector<double> dense;
-    cp_status s = strided_to_dense(ct, rows, cols, rs, cs, pr, pc, dense);
-    if (s != CP_OK) return s;
-    std::vector<double>& P = c->cellTypeHost;
-    P.assign((size_t)M * N, 0.0);
-    for (int i = 0; i < pr; ++i)
-        for (int j = 0; j < pc; ++j) P[(size_t)i * N + j] = dense[(size_t)i * pc + j];
-    // pad the extra row/column by copy (SIMPLE.cpp:667-676)
+    if (rows != pr || cols != pc) return fail(CP_ERR_BAD_PARAM, "shape %ld x %ld, expected %d x %d", rows, cols, pr, pc);
+    std::vector<double> P((size_t)M * N, 0.0);
+    for (long i = 0; i < rows; ++i) {
+        const double* row = src + i * rs;
+        double* out = P.data() + (size_t)i * N;
+        for (long j = 0; j < cols; ++j) {
+            const double x = row[j * cs];
+            if (!std::isfinite(x)) return fail(CP_ERR_NONFINITE, "non-finite input at (%ld, %ld)", i, j);
+            out[j] = fromGamma ? 1.0 - x : x;
+        }
+    }
     for (int i = 0; i < pr; ++i) P[(size_t)i * N + pc] = P[(size_t)i * N + pc - 1];
     for (int j = 0; j < N; ++j) P[(size_t)pr * N + j] = P[(size_t)(pr - 1) * N + std::min(j, pc - 1)];
+    c->cellTypeHost.swap(P);
     std::vector<double> g;
-    build_density(c, P, g);
+    build_density(c, c->cellTypeHost, g);
     return upload_cells(c, g);
 }
 
+cp_status cp_set_cell_type(cp_ctx* c, const double* ct, long rows, long cols, long rs, long cs) {
+    return set_cells(c, ct, rows, cols, rs, cs, false);
+}
+
 cp_status cp_set_gamma(cp_ctx* c, const double* gm, long rows, long cols, long rs, long cs) {
-    if (!c) return fail(CP_ERR_BAD_PARAM, "ctx is NULL");
-    const int pr = c->d.M - 1, pc = c->d.N - 1;
-    std::vector<double> dense;
-    cp_status s = strided_to_dense(gm, rows, cols, rs, cs, pr, pc, dense);
-    if (s != CP_OK) return s;
-    for (double& x : dense) x = 1.0 - x;  // gamma -> cellType
-    return cp_set_cell_type(c, dense.data(), pr, pc, pc, 1);
+    return set_cells(c, gm, rows, cols, rs, cs, true);
 }
 
 cp_status cp_read_geometry(cp_ctx* c, const char* path) {
