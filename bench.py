@@ -52,9 +52,9 @@ ADJ_MAX_ITER = 2000
 # solves (coldplate_b200.fdcheck and the -m gpu adjoint tests); the timed
 # state here (dP within 1e-5) is not a fixed point of the iteration, so the
 # adjoint there differentiates the discretisation (equations model)
-ADJ_FD_NOTE = ("not checked at this state; fixed-point model vs central FD: constricted channel 32x96 "
-               "1.2e-6..7.1e-6, density 512x256 at its fixed point (8327 clamped) median 1.4e-6 max 4.1e-5; "
-               "equations model without clamps (density 256x128) median 6.1e-5")
+ADJ_FD_NOTE = ("not checked at this state; vs central FD (h 1e-4) at converged states: equations model, "
+               "density 256x128, 32 cells <= 1.5e-7; fixed-point model, constricted channel 32x96 "
+               "1.2e-6..7.1e-6, density 512x256 at its fixed point (8327 clamped) median 1.4e-6 max 4.1e-5")
 # ncu captures of the dominant kernels (profiles/): DRAM bytes read + written
 PCG_MG_CAPTURE_BYTES = (762.0 + 1447.7) * 1e6     # k_pcg_mg<float>, one launch (32 x 64 tiles)
 PCG_MG_CAPTURE_ITERS = 30

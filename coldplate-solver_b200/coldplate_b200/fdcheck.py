@@ -2,6 +2,7 @@
 
     PYTHONPATH=coldplate-solver_b200 python -m coldplate_b200.fdcheck \
         [--case density|constricted] [--ny 256 --nx 512 --seed 0 --cells 32 --h 1e-4]
+        [--ptol 1e-6 --momentum-tol T --max-momentum-iter K]
 
 Works on the density workload of ``cases.density_field`` (or the
 constricted channel of ``cases.constricted_channel``), FP64 form,
@@ -22,7 +23,17 @@ averages between clamped velocities, sit exactly on their kink: the +h and
 the base differ by a term that does not shrink with h, while their average,
 the central difference, is the mean of the branches' derivatives, which the
 adjoint takes at such faces.  The tool reports both; the adjoint is compared
-with the central difference.  Cells are drawn with a seeded generator from γ in
+with the central difference.
+
+The inner solves' tolerances (``--ptol``, ``--momentum-tol`` and their
+iteration caps) do not move the fixed point, but with loose ones the
+iteration may never settle on it: at 256 x 128 with pTol 1e-6 and the
+default momentum tolerance, the state keeps wandering by about 1e-6 Pa of
+ΔP (the pressure and momentum stop rules switch between counts from one
+outer iteration to the next), which is about 1e-4 of the difference D at
+h = 1e-4.  With pTol 1e-12 and momentumTol 1e-14 it reaches its fixed point
+exactly (the same ΔP to 2e-12) and D is stationary to the bit.  Cells are
+drawn with a seeded generator from γ in
 [0.05, 0.95], at least 3 cells from the walls and away from the inlet and
 outlet buffers.  Prints one line per cell and a JSON summary line.
 """
@@ -113,10 +124,14 @@ class FiniteDifferences:
                 "iters": n, "d_stationary": drel}
 
 
-def make_case(name: str, ny: int, nx: int, seed: int):
+def make_case(name: str, ny: int, nx: int, seed: int, **knobs):
+    """The FD workloads, FP64 form, pressureSolverType 4; `knobs` override
+    the inner tolerances (pTol, maxPressureIter, momentumTol, ...)."""
+    kw = dict(pressureSolverType=4, maxPressureIter=30, pTol=1e-6)
+    kw.update(knobs)
     if name == "constricted":
-        return cases.constricted_channel(ny, nx, pressureSolverType=4, maxPressureIter=30, pTol=1e-6)
-    return cases.density_field(ny, nx, seed=seed, pressureSolverType=4, maxPressureIter=30, pTol=1e-6)
+        return cases.constricted_channel(ny, nx, **kw)
+    return cases.density_field(ny, nx, seed=seed, **kw)
 
 
 def main(argv=None) -> dict:
@@ -133,9 +148,18 @@ def main(argv=None) -> dict:
     ap.add_argument("--dtol", type=float, default=1e-7)
     ap.add_argument("--adjoint-tol", type=float, default=1e-10)
     ap.add_argument("--adjoint-model", type=int, default=0, help="cp_adjoint_model: 0 auto, 1 equations, 2 fixed point")
+    ap.add_argument("--ptol", type=float, default=1e-6)
+    ap.add_argument("--max-pressure-iter", type=int, default=30)
+    ap.add_argument("--momentum-tol", type=float, default=None, help="default: the SIMPLE.h value")
+    ap.add_argument("--max-momentum-iter", type=int, default=None, help="default: the SIMPLE.h value")
     a = ap.parse_args(argv)
 
-    case = make_case(a.case, a.ny, a.nx, a.seed)
+    knobs = dict(pTol=a.ptol, maxPressureIter=a.max_pressure_iter)
+    if a.momentum_tol is not None:
+        knobs["momentumTol"] = a.momentum_tol
+    if a.max_momentum_iter is not None:
+        knobs["maxMomentumIter"] = a.max_momentum_iter
+    case = make_case(a.case, a.ny, a.nx, a.seed, **knobs)
     gamma = 1.0 - case.cellType
     cap = max(a.base_iters, a.fd_iters) + 200
     prm = case.params(precision="fp64", maxIterations=cap + 10, epsilon=1e-30, historyCapacity=cap + 10,
