@@ -401,9 +401,10 @@ def batch_fields(args, rank: int = 0, world: int = 1):
     ranks by cells x outer iterations (partition_fields), each rank
     advancing its own fields with no exchange."""
     from coldplate_b200 import cases, partition_fields
-    # the batched kernel runs the 2 x 2 aggregation cycle (pressureSolverType
-    # 2); the sequential comparison runs the same solver type
-    cs = cases.batch(args.batch_fields, seed=args.seed, **{**BENCH_KNOBS, "pressureSolverType": 2})
+    # pressureSolverType 4: the batch runs in team mode (each team of CTAs
+    # runs whole fields through the single-field smoothed-aggregation
+    # iteration); the sequential comparison runs the same solver type
+    cs = cases.batch(args.batch_fields, seed=args.seed, **BENCH_KNOBS)
     cells = [c.cellType.shape[0] * c.cellType.shape[1] for c in cs]
     mine = partition_fields([n * args.batch_outer for n in cells], world)[rank]
     return cs, cells, mine
@@ -412,7 +413,7 @@ def batch_fields(args, rank: int = 0, world: int = 1):
 def batch_leg(Simple, torch, args, rank: int = 0, world: int = 1, dist=None) -> dict:
     """This rank's share of the batch workload, mixed precision, epsilon
     1e-6, advanced by the batched kernel for --batch-outer outer iterations
-    (200) with the autotuned tile; then the adjoint dP/dgamma of every field
+    (200) with the autotuned team size; then the adjoint dP/dgamma of every field
     at its state; against the same fields solved one after the other
     (BATCH_SINGLE_OUTER iterations each).  Most of these fields never reach
     epsilon 1e-6 with the reference's SIMPLE iteration (their residual RMS
@@ -465,7 +466,7 @@ def batch_leg(Simple, torch, args, rank: int = 0, world: int = 1, dist=None) -> 
                         f"{args.seed}, mixed, {nout} outer iterations; adjoint of each field after the batch"
                         + (f"; fields split over {world} ranks by cells" if world > 1 else ""),
             "cells": int(sum(cells_all)), "fields_this_rank": len(cs), "t_s": t, "launches": rep["launches"],
-            "tile": [rep["tileRows"], rep["tileCols"]], "autotune_trial_ms": tune["device_ms"],
+            "team_ctas": rep["teamCtas"], "autotune_trial_ms": tune["device_ms"],
             "cell_iterations_per_s": work / t,
             "sequential_single_cell_iterations_per_s": work1 / t1,
             "speedup_vs_sequential": (work / t) / (work1 / t1),

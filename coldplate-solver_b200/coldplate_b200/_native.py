@@ -85,7 +85,8 @@ class CpAdjointReport(ctypes.Structure):
 
 class CpBatchReport(ctypes.Structure):
     _fields_ = [("outerIterations", ctypes.c_int), ("fieldsDone", ctypes.c_int), ("launches", ctypes.c_int),
-                ("tileRows", ctypes.c_int), ("tileCols", ctypes.c_int), ("device_ms", ctypes.c_double)]
+                ("tileRows", ctypes.c_int), ("tileCols", ctypes.c_int), ("device_ms", ctypes.c_double),
+                ("teamCtas", ctypes.c_int)]
 
 
 class CpThermalParams(ctypes.Structure):
@@ -133,6 +134,7 @@ SIGNATURES = {
     "cp_batch_create": (_I, [ctypes.POINTER(_vp), _I, ctypes.POINTER(_vp)]),
     "cp_batch_destroy": (_I, [_vp]),
     "cp_batch_set_tile": (_I, [_vp, _I, _I]),
+    "cp_batch_set_team": (_I, [_vp, _I]),
     "cp_batch_run": (_I, [_vp, _I, ctypes.POINTER(CpBatchReport)]),
     "cp_batch_autotune": (_I, [_vp, _I, ctypes.POINTER(CpBatchReport)]),
     "cp_thermal_params_default": (None, [ctypes.POINTER(CpThermalParams)]),

@@ -269,7 +269,10 @@ class Batch:
     (cp_batch_run).  Each field keeps its own stop rules, history and state:
     after ``run`` read results from the ``Simple`` objects as usual.  The
     fields must use pressureSolverType 2 or 4 and one precision, and must
-    stay open while the batch exists."""
+    stay open while the batch exists.  When every field is type 4 the batch
+    runs in team mode (teams of CTAs take whole fields from a queue and run
+    the single-field smoothed-aggregation iteration); otherwise every field
+    runs the 2 x 2 aggregation cycle over cell tiles."""
 
     def __init__(self, fields: list[Simple]):
         self._lib = nat.lib()
@@ -282,8 +285,13 @@ class Batch:
     def set_tile(self, rows: int, cols: int) -> None:
         nat.check(self._lib.cp_batch_set_tile(self._h, int(rows), int(cols)))
 
+    def set_team(self, ctas: int) -> None:
+        """CTAs per team (team mode only)."""
+        nat.check(self._lib.cp_batch_set_team(self._h, int(ctas)))
+
     def autotune(self, trial_outer: int = 4) -> dict:
-        """Pick the fastest cell tile on trial_outer iterations; resets every field."""
+        """Pick the fastest cell tile (team mode: team size) on trial_outer
+        iterations; resets every field."""
         r = nat.CpBatchReport()
         nat.check(self._lib.cp_batch_autotune(self._h, int(trial_outer), ctypes.byref(r)))
         return {name: getattr(r, name) for name, _ in r._fields_}

@@ -25,6 +25,7 @@
 #pragma once
 
 #include "cp_mg.cuh"
+#include "cp_sa.cuh"
 
 namespace cp {
 
@@ -63,6 +64,12 @@ struct BState {
     double mass[4];      // sum du^2, sum dv^2, sum b^2, max |b| (the k_mass quantities)
 };
 
+// CP_BATCH_PROFILE: device time of each phase (barrier to barrier, as seen
+// by block 0), summed over the launch
+enum BatchPhase { BP_BC = 0, BP_ASM, BP_JAC, BP_JACRED, BP_SCAT, BP_BCSTAR, BP_MASS, BP_MASSRED, BP_COARSE,
+                  BP_COARSECTA, BP_RESTR, BP_VCTA, BP_PROL, BP_VRED, BP_MATVEC, BP_MVRED, BP_UPD, BP_UPDRED,
+                  BP_PSTAR, BP_CORR, BP_BC2, BP_FIN, BP_COUNT };
+
 struct BatchArgs {
     int nf;              // fields
     int R, C;            // cell tile: R rows x C columns
@@ -75,6 +82,7 @@ struct BatchArgs {
     unsigned* bar;       // grid barrier counter (zeroed before the launch)
     int* err;            // first device error of the batch (barrier time-out)
     int* allDone;        // 1 when every field has stopped
+    unsigned long long* prof;   // [BP_COUNT] or null
 };
 
 // One Jacobi update of a momentum unknown (x+ = x + (b - A x) / aP, the
@@ -131,9 +139,16 @@ __global__ void __launch_bounds__(kBatchThreads, 1) k_batch(BatchArgs a, const B
     if (threadIdx.x == 0) fsIdx = -1;
     __syncthreads();
     unsigned target = 0;
-    auto sync = [&]() -> bool {
+    unsigned long long tp = (a.prof && blockIdx.x == 0 && threadIdx.x == 0) ? globaltimer_ns() : 0ull;
+    auto sync = [&](int ph) -> bool {
         target += G;
-        return grid_barrier(a.bar, target, a.err);
+        const bool ok = grid_barrier(a.bar, target, a.err);
+        if (tp) {
+            const unsigned long long t = globaltimer_ns();
+            a.prof[ph] += t - tp;
+            tp = t;
+        }
+        return ok;
     };
     // make fs hold field f (block-uniform call)
     auto load_field = [&](int f) {
@@ -218,7 +233,7 @@ __global__ void __launch_bounds__(kBatchThreads, 1) k_batch(BatchArgs a, const B
             }
             if (on) apply_bc(fs.k, fs.st->iter, fs.u, fs.v, fs.p, fs.gamma, threadIdx.x, blockDim.x);
         });
-        if (!sync()) return;
+        if (!sync(BP_BC)) return;
         {
             int any = 0;
             for (int f = 0; f < nf; ++f) any |= ldi(&a.bs[f].on);
@@ -231,7 +246,7 @@ __global__ void __launch_bounds__(kBatchThreads, 1) k_batch(BatchArgs a, const B
             if (i <= d.M - 1 && j <= d.N - 2) assemble_one<TC, Mixed, true>(fs.k, fl, fs.U, fs.dE, i, j, tVel);
             if (i <= d.M - 2 && j <= d.N - 1) assemble_one<TC, Mixed, false>(fs.k, fl, fs.V, fs.dN, i, j, tVel);
         }, noFin);
-        if (!sync()) return;
+        if (!sync(BP_ASM)) return;
         // ---- Jacobi sweeps of U and V together; each component of each field
         // stops on its own rule (jacobi_solver.cpp:44-67)
         for (int s = 0; s < a.maxMom; ++s) {
@@ -256,7 +271,7 @@ __global__ void __launch_bounds__(kBatchThreads, 1) k_batch(BatchArgs a, const B
                 write_part(g, acc, 2);
                 acc[0] = acc[1] = 0.0;
             });
-            if (!sync()) return;
+            if (!sync(BP_JAC)) return;
             for_my_fields([&](int f) { return isOn(f) && (ldi(&a.bs[f].jacU) || ldi(&a.bs[f].jacV)); },
                           [&](int f) {
                 double tot[kBatchPartStride];
@@ -276,7 +291,7 @@ __global__ void __launch_bounds__(kBatchThreads, 1) k_batch(BatchArgs a, const B
                     }
                 }
             });
-            if (!sync()) return;
+            if (!sync(BP_JACRED)) return;
             int any = 0;
             for (int f = 0; f < nf; ++f) any |= ldi(&a.bs[f].jacU) | ldi(&a.bs[f].jacV);
             if (!any) break;
@@ -308,7 +323,7 @@ __global__ void __launch_bounds__(kBatchThreads, 1) k_batch(BatchArgs a, const B
                 mu = mv = 0.0;
             });
         }
-        if (!sync()) return;
+        if (!sync(BP_SCAT)) return;
         // ---- BCs on u*, v*; the sweep counts
         for_my_fields(isOn, [&](int f) {
             if (threadIdx.x == 0) {
@@ -317,7 +332,7 @@ __global__ void __launch_bounds__(kBatchThreads, 1) k_batch(BatchArgs a, const B
             }
             apply_bc(fs.k, fs.st->iter, fs.uStar, fs.vStar, nullptr, fs.gamma, threadIdx.x, blockDim.x);
         });
-        if (!sync()) return;
+        if (!sync(BP_BCSTAR)) return;
         // ---- mass imbalance and RMS changes (iterations.cpp:499-533,
         // pressure_solver.cpp:471-488, 733-742), fused with the level-0
         // operator of the pressure correction, x = 0, r = b
@@ -376,7 +391,7 @@ __global__ void __launch_bounds__(kBatchThreads, 1) k_batch(BatchArgs a, const B
                 for (int q = 0; q < kBatchPartStride; ++q) acc[q] = 0.0;
             });
         }
-        if (!sync()) return;
+        if (!sync(BP_MASS)) return;
         for_my_fields(isOn, [&](int f) {
             const int* to = s_toff;
             double tot[kBatchPartStride];
@@ -398,14 +413,14 @@ __global__ void __launch_bounds__(kBatchThreads, 1) k_batch(BatchArgs a, const B
                 b.beta = 0.0;
             }
         });
-        if (!sync()) return;
+        if (!sync(BP_MASSRED)) return;
         // ---- coarse operators: grid-wide levels, then the CTA levels and the
         // dense inverse on the field's reducer block
         for (int l = 1; l < a.maxLg; ++l) {
             for_tiles(l, [&](int f) { return isOn(f) && l < F[f].H.Lg; }, [&](int I, int J) {
                 mg_coarsen_cell(fs.H.lv[l - 1], fs.H.lv[l], I, J);
             }, noFin);
-            if (!sync()) return;
+            if (!sync(BP_COARSE)) return;
         }
         for_my_fields(isOn, [&](int) {
             for (int l = fs.H.Lg - 1; l < fs.H.L - 1; ++l) {
@@ -415,7 +430,7 @@ __global__ void __launch_bounds__(kBatchThreads, 1) k_batch(BatchArgs a, const B
             }
             mg_dense_setup(fs.H.lv[fs.H.L - 1], fs.H.dense, dsm);
         });
-        if (!sync()) return;
+        if (!sync(BP_COARSECTA)) return;
         // ---- V-cycle z = M r of the fields whose CG runs; per-tile r.z partials
         auto vcycle = [&]() -> bool {
             for (int l = 0; l < a.maxLg; ++l) {
@@ -423,13 +438,13 @@ __global__ void __launch_bounds__(kBatchThreads, 1) k_batch(BatchArgs a, const B
                     if (l == 0) mg_restrict0x_cell(fs.H.lv[0], fs.H.lv[1], I, J, fs.H.omega);
                     else mg_restrict_cell(fs.H.lv[l], fs.H.lv[l + 1], I, J, fs.H.omega);
                 }, noFin);
-                if (!sync()) return false;
+                if (!sync(BP_RESTR)) return false;
             }
             for_my_fields(cgOn, [&](int) {
                 if (fs.H.Lg < fs.H.L - 1) mg_cta_cycle(fs.H);
                 else mg_dense_solve(fs.H.lv[fs.H.L - 1], fs.H.dense);
             });
-            if (!sync()) return false;
+            if (!sync(BP_VCTA)) return false;
             for (int l = a.maxLg - 1; l >= 0; --l) {
                 double acc[1] = {0.0};
                 for_tiles(l, [&](int f) { return cgOn(f) && l < F[f].H.Lg; }, [&](int i, int j) {
@@ -450,7 +465,7 @@ __global__ void __launch_bounds__(kBatchThreads, 1) k_batch(BatchArgs a, const B
                         acc[0] = 0.0;
                     }
                 });
-                if (!sync()) return false;
+                if (!sync(BP_PROL)) return false;
             }
             return true;
         };
@@ -460,7 +475,7 @@ __global__ void __launch_bounds__(kBatchThreads, 1) k_batch(BatchArgs a, const B
             tile_sum(f, tot, 1);
             if (threadIdx.x == 0) bsv(f).rz = tot[0];
         });
-        if (!sync()) return;
+        if (!sync(BP_VRED)) return;
         // ---- CG (pressure_solver.cpp:121-184 recurrences; AMGCL's relative stop)
         for (int it = 0; it < a.maxP; ++it) {
             const bool first = (it == 0);
@@ -495,7 +510,7 @@ __global__ void __launch_bounds__(kBatchThreads, 1) k_batch(BatchArgs a, const B
                     acc[0] = 0.0;
                 });
             }
-            if (!sync()) return;
+            if (!sync(BP_MATVEC)) return;
             for_my_fields(cgOn, [&](int f) {
                 double tot[kBatchPartStride];
                 tile_sum(f, tot, 1);
@@ -505,7 +520,7 @@ __global__ void __launch_bounds__(kBatchThreads, 1) k_batch(BatchArgs a, const B
                     else b.alpha = b.rz / tot[0];
                 }
             });
-            if (!sync()) return;
+            if (!sync(BP_MVRED)) return;
             {
                 double acc[1] = {0.0};
                 double tAlpha = 0.0;
@@ -529,7 +544,7 @@ __global__ void __launch_bounds__(kBatchThreads, 1) k_batch(BatchArgs a, const B
                     acc[0] = 0.0;
                 });
             }
-            if (!sync()) return;
+            if (!sync(BP_UPD)) return;
             for_my_fields(cgOn, [&](int f) {
                 double tot[kBatchPartStride];
                 tile_sum(f, tot, 1);
@@ -539,7 +554,7 @@ __global__ void __launch_bounds__(kBatchThreads, 1) k_batch(BatchArgs a, const B
                     else if (it + 1 >= fs.k.maxP) { b.cgOn = 0; b.cgIt = fs.k.maxP; }
                 }
             });
-            if (!sync()) return;
+            if (!sync(BP_UPDRED)) return;
             {
                 int any = 0;
                 for (int f = 0; f < nf; ++f) any |= ldi(&a.bs[f].cgOn);
@@ -555,7 +570,7 @@ __global__ void __launch_bounds__(kBatchThreads, 1) k_batch(BatchArgs a, const B
                     b.rz = tot[0];
                 }
             });
-            if (!sync()) return;
+            if (!sync(BP_VRED)) return;
         }
         // ---- p' (pressure_solver.cpp:814: p'(:, N-1) = 0)
         for_tiles(0, isOn, [&](int i, int j) {
@@ -565,7 +580,7 @@ __global__ void __launch_bounds__(kBatchThreads, 1) k_batch(BatchArgs a, const B
             fs.pStar[c] = (double)fs.B.x[c];
             if (j == d.N - 2) fs.pStar[c + 1] = 0.0;
         }, noFin);
-        if (!sync()) return;
+        if (!sync(BP_PSTAR)) return;
         // ---- correction (iterations.cpp:556-597)
         for_tiles(0, onVel, [&](int i, int j) {
             const Dims d = fs.k.d;
@@ -585,23 +600,173 @@ __global__ void __launch_bounds__(kBatchThreads, 1) k_batch(BatchArgs a, const B
                 fs.v[c] = dmax(-maxVel, dmin(maxVel, fs.vStar[c] + dv));
             }
         }, noFin);
-        if (!sync()) return;
+        if (!sync(BP_CORR)) return;
         // ---- BCs, then sampling, history row and stop rules of each field
         for_my_fields(isOn, [&](int f) {
             apply_bc(fs.k, fs.st->iter, fs.u, fs.v, fs.p, fs.gamma, threadIdx.x, blockDim.x);
             if (threadIdx.x == 0) fs.st->itersP = ldi(&a.bs[f].cgIt);
         });
-        if (!sync()) return;
+        if (!sync(BP_BC2)) return;
         for_my_fields(isOn, [&](int f) {
             FinalizeArgs fa{fs.u, fs.v, fs.p, fs.gamma, a.bs[f].mass, 1, fs.hist, fs.histCap, fs.dpWin};
             finalize_block(fs.k, fs.st, fa);
         });
-        if (!sync()) return;
+        if (!sync(BP_FIN)) return;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         int all = 1;
         for (int f = 0; f < nf; ++f) all &= (__ldcg(&F[f].st->done) != 0);
         *a.allDone = all;
+    }
+}
+
+// ======================================================================== teams of CTAs
+// The batched kernel of smoothed-aggregation fields (pressureSolverType 4).
+// The grid is cut into teams of consecutive CTAs; each team takes the next
+// field from a queue (largest first) and runs that field's outer iterations
+// on its own, with its own bounded barrier, through the same device code as
+// the single-field kernels (k_bc, k_assemble, k_jacobi, k_mass, k_pcg_sa,
+// k_correct, k_finalize): fields never wait for each other, no field idles
+// the SMs of another, and a team's barriers cost what a few CTAs' arrivals
+// cost.  The partial sums of a phase are per team rank, summed in rank order.
+
+// Everything one field's solve touches (device pointers of a single-field
+// context plus its parameter block and hierarchy); copied into shared
+// memory by the team's CTAs when they take the field.
+template <typename TC>
+struct BFieldSa {
+    KParams k;
+    Status* st;
+    double *u, *v, *p, *uStar, *vStar, *pStar, *dE, *dN;
+    const double *alpha, *gamma;
+    MomSys<TC> U, V;
+    TC *xU0, *xU1, *xV0, *xV1;
+    PcgBufs<TC> B;
+    SaHier<TC> H;
+    double *partJ, *partM, *partP;   // the context's partial-sum scratch (>= 4 x team size doubles)
+    double* hist;
+    int histCap;
+    double* dpWin;
+};
+
+constexpr int kTeamStride = 32;   // unsigned words between two teams' barrier counters (128 B)
+
+struct TeamArgs {
+    int nf;              // fields
+    int team;            // CTAs per team
+    int nTeams;          // teams (the CTAs past nTeams x team exit at once)
+    int nOuter;          // outer iterations a field may run in this launch
+    const int* order;    // [nf] queue order: field indices, largest first
+    unsigned* tbar;      // [nTeams * kTeamStride] team barrier counters (zeroed before the launch)
+    int* queue;          // [1 + 2 nTeams]: next queue position, then each team's last two picks
+    int* err;            // first device error of the batch (barrier time-out)
+    int* running;        // fields left running after this launch (zeroed before the launch)
+};
+
+// One outer iteration of field f on team T: the single-field sequence
+// (enqueue_iteration) with each kernel's grid replaced by the team.
+template <typename TC, bool Mixed>
+__device__ __forceinline__ bool team_outer(const Team& T, unsigned& target, const BFieldSa<TC>& f) {
+    const KParams& k = f.k;
+    Status* st = f.st;
+    const int tid = T.tid(), nth = T.nth();
+    const int iter = __ldcg(&st->iter);
+    // ---- k_bc (boundaries.cpp:50-146), max-change counters reset
+    if (T.lead()) {
+        st->maxDU = 0ull;
+        st->maxDV = 0ull;
+    }
+    apply_bc(k, iter, f.u, f.v, f.p, f.gamma, tid, nth);
+    if (!team_sync(T, target)) return false;
+    // ---- k_assemble (momentum_solver.cpp:197-314)
+    const double maxVel = max_vel(inlet_velocity(k, iter));
+    {
+        const Fields fl{f.u, f.v, f.p, f.alpha, f.gamma};
+        const Dims d = k.d;
+        const int nU = k.nU, nV = k.nV, wU = d.N - 2, wV = d.N - 1;
+        for (int t = tid; t < nU + nV; t += nth) {
+            if (t < nU) assemble_one<TC, Mixed, true>(k, fl, f.U, f.dE, 1 + t / wU, 1 + t % wU, maxVel);
+            else assemble_one<TC, Mixed, false>(k, fl, f.V, f.dN, 1 + (t - nU) / wV, 1 + (t - nU) % wV, maxVel);
+        }
+    }
+    if (!team_sync(T, target)) return false;
+    // ---- k_jacobi: U sweeps, V sweeps, scatter with clamps, BCs on u*, v*
+    {
+        int curU = -1, curV = -1, itU = 0, itV = 0;
+        if (!jacobi_component<TC, Mixed, true>(k, f.U, f.u, f.xU0, f.xU1, f.partJ, T, target, curU, itU))
+            return false;
+        if (!jacobi_component<TC, Mixed, false>(k, f.V, f.v, f.xV0, f.xV1, f.partJ + 2 * T.size, T, target, curV,
+                                                itV))
+            return false;
+        double mu = jacobi_scatter<TC, Mixed, true>(k, f.u, curU < 0 ? nullptr : (curU ? f.xU1 : f.xU0), f.uStar,
+                                                    maxVel, tid, nth);
+        double mv = jacobi_scatter<TC, Mixed, false>(k, f.v, curV < 0 ? nullptr : (curV ? f.xV1 : f.xV0), f.vStar,
+                                                     maxVel, tid, nth);
+        mu = warp_max(mu);
+        mv = warp_max(mv);
+        if ((threadIdx.x & 31) == 0) {
+            atomic_max_nonneg(&st->maxDU, mu);
+            atomic_max_nonneg(&st->maxDV, mv);
+        }
+        if (T.lead()) {
+            st->itersU = itU;
+            st->itersV = itV;
+        }
+        if (!team_sync(T, target)) return false;
+        apply_bc(k, iter, f.uStar, f.vStar, nullptr, f.gamma, tid, nth);
+    }
+    if (!team_sync(T, target)) return false;
+    // ---- k_mass, then the smoothed-aggregation PCG (k_pcg_sa)
+    mass_pass<TC>(k, f.u, f.v, f.uStar, f.vStar, f.B.rhs, tid, nth, f.partM + (size_t)T.rank * 4);
+    if (!team_sync(T, target)) return false;
+    if (!pcg_sa<TC>(T, target, k, st, f.dE, f.dN, f.B, f.H, f.pStar, f.partP)) return false;
+    if (!team_sync(T, target)) return false;
+    // ---- k_correct (iterations.cpp:556-597), k_bc, k_finalize
+    correct_cells(k, iter, f.u, f.v, f.p, f.uStar, f.vStar, f.pStar, f.dE, f.dN, tid, nth);
+    if (!team_sync(T, target)) return false;
+    apply_bc(k, iter, f.u, f.v, f.p, f.gamma, tid, nth);
+    if (!team_sync(T, target)) return false;
+    if (T.rank == 0) {
+        const FinalizeArgs fa{f.u, f.v, f.p, f.gamma, f.partM, T.size, f.hist, f.histCap, f.dpWin};
+        finalize_block(k, st, fa);
+    }
+    return team_sync(T, target);
+}
+
+template <typename TC, bool Mixed>
+__global__ void __launch_bounds__(kBatchThreads, 1) k_batch_team(TeamArgs a, const BFieldSa<TC>* __restrict__ F) {
+    __shared__ __align__(16) BFieldSa<TC> fs;
+    const int team = blockIdx.x / a.team;
+    if (team >= a.nTeams) return;
+    const Team T{(int)blockIdx.x - team * a.team, a.team, a.tbar + (size_t)team * kTeamStride, a.err};
+    int* pick = a.queue + 1 + 2 * team;
+    unsigned target = 0;
+    for (int n = 0;; ++n) {
+        // the team's next field: drawn by its lead thread, read by every CTA
+        // after the barrier (two slots, so a slow CTA still reads its pick
+        // while the lead draws the next one)
+        if (T.lead()) pick[n & 1] = atomicAdd(a.queue, 1);
+        if (!team_sync(T, target)) return;
+        const int q = __ldcg(pick + (n & 1));
+        if (q >= a.nf) break;
+        const BFieldSa<TC>* src = F + __ldg(a.order + q);
+        {
+            const int* from = reinterpret_cast<const int*>(src);
+            int* to = reinterpret_cast<int*>(&fs);
+            for (int e = threadIdx.x; e < (int)(sizeof(BFieldSa<TC>) / sizeof(int)); e += blockDim.x)
+                to[e] = __ldg(from + e);
+            __syncthreads();
+        }
+        int o = 0;
+        for (; o < a.nOuter; ++o) {
+            // st->done is written by finalize on rank 0 before the barrier that
+            // ends the iteration (or by an earlier call), so every CTA reads
+            // the same value
+            if (__ldcg(&fs.st->done)) break;
+            if (!team_outer<TC, Mixed>(T, target, fs)) return;
+        }
+        if (T.lead() && o == a.nOuter && !__ldcg(&fs.st->done)) atomicAdd(a.running, 1);
+        __syncthreads();
     }
 }
 

@@ -182,6 +182,28 @@ __device__ __forceinline__ bool grid_barrier(unsigned* counter, unsigned target,
     return s_ok != 0;
 }
 
+// A team of CTAs that runs one phase sequence together, synchronised by its
+// own bounded barrier: the whole grid of a single-field launch, or a group
+// of consecutive CTAs of the batched kernel that solves one field at a time.
+// Partial sums are written per team rank and summed over the team's size.
+struct Team {
+    int rank, size;      // CTA index in the team, CTAs in the team
+    unsigned* bar;       // the team's barrier counter (grows during a launch)
+    int* err;            // first device error (barrier time-out)
+    __device__ __forceinline__ int tid() const { return rank * (int)blockDim.x + (int)threadIdx.x; }
+    __device__ __forceinline__ int nth() const { return size * (int)blockDim.x; }
+    __device__ __forceinline__ bool lead() const { return rank == 0 && threadIdx.x == 0; }
+};
+
+__device__ __forceinline__ Team grid_team(unsigned* bar, int* err) {
+    return Team{(int)blockIdx.x, (int)gridDim.x, bar, err};
+}
+
+__device__ __forceinline__ bool team_sync(const Team& T, unsigned& target) {
+    target += (unsigned)T.size;
+    return grid_barrier(T.bar, target, T.err);
+}
+
 __device__ __forceinline__ void atomic_max_nonneg(unsigned long long* addr, double v) {
     // non-negative IEEE doubles order like their bit patterns
     if (v > 0.0) atomicMax(addr, (unsigned long long)__double_as_longlong(v));
@@ -225,15 +247,19 @@ __device__ __forceinline__ Vec16<TV> zero16() {
 // (the pitch is a multiple of 32 above nJ), and column g V + V, read by lane
 // 31, is at most the next row's column 0.
 template <typename TV, typename F>
-__device__ __forceinline__ void row_segments(int nI, int nJ, F&& fn) {
+__device__ __forceinline__ void row_segments(const Team& T, int nI, int nJ, F&& fn) {
     constexpr int V = Vec16<TV>::n;
     const int lane = threadIdx.x & 31;
-    const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), nw = (int)((gridDim.x * blockDim.x) >> 5);
+    const int warp = T.tid() >> 5, nw = T.nth() >> 5;
     const int Ga = nJ / V + 1, S = (Ga + 31) >> 5;
     for (int s = warp; s < nI * S; s += nw) {
         const int i = 1 + s / S, g = ((s % S) << 5) + lane;
         fn(i, g * V, g < Ga, lane);
     }
+}
+template <typename TV, typename F>
+__device__ __forceinline__ void row_segments(int nI, int nJ, F&& fn) {
+    row_segments<TV>(Team{(int)blockIdx.x, (int)gridDim.x, nullptr, nullptr}, nI, nJ, static_cast<F&&>(fn));
 }
 
 template <typename TV>

@@ -254,12 +254,12 @@ __global__ void k_assemble(KParams k, const Status* st, Fields f, MomSys<TC> U, 
 // buffer index holding the result (-1: the initial iterate) and the sweep
 // count, or false if a barrier gave up.
 template <typename TC, bool Mixed, bool IsU>
-__device__ __forceinline__ bool jacobi_component(const KParams& k, Status* st, const MomSys<TC>& S,
-                                                 const double* field, TC* x0, TC* x1, double* part,
-                                                 unsigned* bar, unsigned& target, int& cur, int& its) {
+__device__ __forceinline__ bool jacobi_component(const KParams& k, const MomSys<TC>& S, const double* field,
+                                                 TC* x0, TC* x1, double* part, const Team& T, unsigned& target,
+                                                 int& cur, int& its) {
     __shared__ double sm[32];
     const Dims d = k.d;
-    const int G = gridDim.x;
+    const int G = T.size;
     int i1, j1;
     mom_range<IsU>(d, i1, j1);
     const int n = i1 * j1;
@@ -276,7 +276,7 @@ __device__ __forceinline__ bool jacobi_component(const KParams& k, Status* st, c
         // row segments: a lane takes 16 bytes of a row (4 floats or 2
         // doubles); horizontal neighbours from the adjacent lanes
         constexpr int V = Vec16<TC>::n;
-        row_segments<TC>(i1, j1, [&](int i, int j0, bool act, int lane) {
+        row_segments<TC>(T, i1, j1, [&](int i, int j0, bool act, int lane) {
             const size_t c = at(d, i, j0);
             auto Xv = [&](size_t q) -> Vec16<TC> {
                 if (first) {
@@ -326,9 +326,8 @@ __device__ __forceinline__ bool jacobi_component(const KParams& k, Status* st, c
         });
         block_sum<1>(acc, sm);
         double* slot = part + (size_t)(s & 1) * G;
-        if (threadIdx.x == 0) slot[blockIdx.x] = acc[0];
-        target += G;
-        if (!grid_barrier(bar, target, &st->err)) return false;
+        if (threadIdx.x == 0) slot[T.rank] = acc[0];
+        if (!team_sync(T, target)) return false;
         double tot[1];
         sum_partials<1>(slot, G, 1, tot, sm);
         cur = nxt;
@@ -380,10 +379,11 @@ __global__ void __launch_bounds__(256) k_jacobi(KParams k, Status* st, MomSys<TC
     const double maxVel = max_vel(inlet_velocity(k, iter));
     const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = G * blockDim.x;
     unsigned target = 0;
+    const Team T = grid_team(bar, &st->err);
     int curU = -1, curV = -1, itU = 0, itV = 0;
-    if (doU && !jacobi_component<TC, Mixed, true>(k, st, U, u, xU0, xU1, part, bar, target, curU, itU)) return;
+    if (doU && !jacobi_component<TC, Mixed, true>(k, U, u, xU0, xU1, part, T, target, curU, itU)) return;
     // V uses its own partial slots: blocks may still read U's last sums
-    if (doV && !jacobi_component<TC, Mixed, false>(k, st, V, v, xV0, xV1, part + 2 * G, bar, target, curV, itV))
+    if (doV && !jacobi_component<TC, Mixed, false>(k, V, v, xV0, xV1, part + 2 * G, T, target, curV, itV))
         return;
     double mu = 0.0, mv = 0.0;
     if (doU) mu = jacobi_scatter<TC, Mixed, true>(k, u, curU < 0 ? nullptr : (curU ? xU1 : xU0), out.uStar, maxVel, tid, nth);
@@ -412,9 +412,8 @@ __global__ void __launch_bounds__(256) k_jacobi(KParams k, Status* st, MomSys<TC
 // the pressure unknowns j <= N-2 (pressure_solver.cpp:733-742).
 // part[b*4 + {0,1,2,3}] = {sum du^2, sum dv^2, sum b^2, max |b|}.
 template <typename TV>
-__global__ void k_mass(KParams k, const Status* st, const double* u, const double* v, const double* uStar,
-                       const double* vStar, TV* rhs, double* part) {
-    if (st->done) return;
+__device__ __forceinline__ void mass_pass(const KParams& k, const double* u, const double* v, const double* uStar,
+                                          const double* vStar, TV* rhs, int tid, int nth, double* o) {
     __shared__ double sm[128];
     const Dims d = k.d;
     const int M = d.M, N = d.N, w = N - 1;
@@ -422,7 +421,7 @@ __global__ void k_mass(KParams k, const Status* st, const double* u, const doubl
     double acc[3] = {0.0, 0.0, 0.0};
     double mmax = 0.0;
     const int n = (M - 1) * w;
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    for (int t = tid; t < n; t += nth) {
         const int i = 1 + t / w, j = 1 + t % w;
         const size_t c = at(d, i, j);
         const double massE = rho * uStar[c] * hy, massW = rho * uStar[c - 1] * hy;
@@ -448,9 +447,16 @@ __global__ void k_mass(KParams k, const Status* st, const double* u, const doubl
     if (threadIdx.x == 0) {
         double m = 0.0;
         for (int q = 0; q < (int)((blockDim.x + 31) >> 5); ++q) m = dmax(m, sm[96 + q]);
-        double* o = part + (size_t)blockIdx.x * 4;
         o[0] = acc[0]; o[1] = acc[1]; o[2] = acc[2]; o[3] = m;
     }
+}
+
+template <typename TV>
+__global__ void k_mass(KParams k, const Status* st, const double* u, const double* v, const double* uStar,
+                       const double* vStar, TV* rhs, double* part) {
+    if (st->done) return;
+    mass_pass<TV>(k, u, v, uStar, vStar, rhs, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x,
+                  part + (size_t)blockIdx.x * 4);
 }
 
 // ------------------------------------------------------------------ PCG
@@ -585,14 +591,14 @@ __global__ void __launch_bounds__(256) k_pcg(KParams k, Status* st, const double
 // ------------------------------------------------------------------ correction
 // p += pAlpha p' on [1,M-1] x [1,N-1]; u = clamp(u* + clamp(dE (p'_ij - p'_i,j+1)))
 // on U unknowns and the same for v (iterations.cpp:558-597).
-__global__ void k_correct(KParams k, const Status* st, double* u, double* v, double* p, const double* uStar,
-                          const double* vStar, const double* pStar, const double* dE, const double* dN) {
-    if (st->done) return;
+__device__ __forceinline__ void correct_cells(const KParams& k, int iter, double* u, double* v, double* p,
+                                              const double* uStar, const double* vStar, const double* pStar,
+                                              const double* dE, const double* dN, int tid, int nth) {
     const Dims d = k.d;
     const int M = d.M, N = d.N, w = N - 1;
-    const double maxVel = max_vel(inlet_velocity(k, st->iter));
+    const double maxVel = max_vel(inlet_velocity(k, iter));
     const int n = (M - 1) * w;
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    for (int t = tid; t < n; t += nth) {
         const int i = 1 + t / w, j = 1 + t % w;
         const size_t c = at(d, i, j);
         const double ps = pStar[c];
@@ -610,6 +616,13 @@ __global__ void k_correct(KParams k, const Status* st, double* u, double* v, dou
             v[c] = dmax(-maxVel, dmin(maxVel, nv));
         }
     }
+}
+
+__global__ void k_correct(KParams k, const Status* st, double* u, double* v, double* p, const double* uStar,
+                          const double* vStar, const double* pStar, const double* dE, const double* dN) {
+    if (st->done) return;
+    correct_cells(k, st->iter, u, v, p, uStar, vStar, pStar, dE, dN, blockIdx.x * blockDim.x + threadIdx.x,
+                  gridDim.x * blockDim.x);
 }
 
 // ------------------------------------------------------------------ finalize

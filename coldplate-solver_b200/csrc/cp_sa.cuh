@@ -832,28 +832,29 @@ __device__ __forceinline__ double sa0_smooth(const Sa0<TV>& A, TV om, const TV* 
 }
 
 // ---------------------------------------------------------------- the solver
+// The PCG of one pressure-correction solve on a team of CTAs (the whole grid
+// in k_pcg_sa, a group of CTAs in the batched kernel); returns false if a
+// barrier gave up.  Ends without a barrier after writing p'.
 template <typename TV>
-__global__ void __launch_bounds__(512, 1) k_pcg_sa(KParams k, Status* st, const double* dE, const double* dN,
-                                                PcgBufs<TV> B, SaHier<TV> H, double* pStar, double* part,
-                                                unsigned* bar) {
-    if (st->done) return;
+__device__ __forceinline__ bool pcg_sa(const Team& T, unsigned& target, const KParams& k, Status* st,
+                                       const double* dE, const double* dN, const PcgBufs<TV>& B,
+                                       const SaHier<TV>& H, double* pStar, double* part) {
     extern __shared__ __align__(128) double dsm[];
     __shared__ double sm[96];
     const Dims d = k.d;
     const int M = d.M, N = d.N, w = N - 2;
     const int n = (M - 1) * w;
-    const int G = gridDim.x;
-    const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = G * blockDim.x;
+    const int G = T.size;
+    const int tid = T.tid(), nth = T.nth();
+    const bool cta0 = T.rank == 0;
     const SaSplit all{tid, nth}, cta{(int)threadIdx.x, (int)blockDim.x};
     const double rho = k.rho, hx = k.hx, hy = k.hy, om = H.omega;
     const TV omT = (TV)om;
-    unsigned target = 0;
     double* partA = part;
     double* partB = part + G;
 #define SA_SYNC()                                                   \
     do {                                                            \
-        target += G;                                                \
-        if (!grid_barrier(bar, target, &st->err)) return;           \
+        if (!team_sync(T, target)) return false;                    \
     } while (0)
     // the coarse operators are rebuilt every H.reuse outer iterations (they
     // only precondition: the CG matvec and level 0's smoother and
@@ -870,9 +871,9 @@ __global__ void __launch_bounds__(512, 1) k_pcg_sa(KParams k, Status* st, const 
     const Stencil5<TV> A0{B.fE, B.fN, B.d, M - 1, w, d.P};
     auto stencil = [&](int l) { return Stencil9<TV>{H.lv[l].c, H.lv[l].nI, H.lv[l].nJ, H.lv[l].P}; };
     auto wgt = [&](int l) { return l == 0 ? H.w0 : H.wc; };
-    unsigned long long tp = (H.prof && blockIdx.x == 0 && threadIdx.x == 0) ? globaltimer_ns() : 0ull;
+    unsigned long long tp = (H.prof && T.lead()) ? globaltimer_ns() : 0ull;
     auto tick = [&](int ph) {
-        if (H.prof && blockIdx.x == 0 && threadIdx.x == 0) {
+        if (H.prof && T.lead()) {
             const unsigned long long t = globaltimer_ns();
             atomicAdd(H.prof + ph, t - tp);
             tp = t;
@@ -914,7 +915,7 @@ __global__ void __launch_bounds__(512, 1) k_pcg_sa(KParams k, Status* st, const 
         bb[0] += (double)rt * (double)rt;
     }
     block_sum<1>(bb, sm);
-    if (threadIdx.x == 0) partA[blockIdx.x] = bb[0];
+    if (threadIdx.x == 0) partA[T.rank] = bb[0];
     SA_SYNC();
     double bnorm2[1];
     sum_partials<1>(partA, G, 1, bnorm2, sm);
@@ -957,7 +958,7 @@ __global__ void __launch_bounds__(512, 1) k_pcg_sa(KParams k, Status* st, const 
                          [&](int I, int J) { sa_galerkin_cell(stencil(l), f.P, H.Y, C, wgt(l), I, J); });
             SA_SYNC();
         }
-        if (blockIdx.x == 0) sa_dense_setup(H.lv[H.L - 1], H.dense, dsm);
+        if (cta0) sa_dense_setup(H.lv[H.L - 1], H.dense, dsm);
         SA_SYNC();
     }
     tick(SA_P_GALERKIN);
@@ -966,7 +967,7 @@ __global__ void __launch_bounds__(512, 1) k_pcg_sa(KParams k, Status* st, const 
     // frames included) and the dense inverse in shared memory
     TV* const smb = reinterpret_cast<TV*>(dsm);
     TV* sInv = nullptr;
-    if (blockIdx.x == 0) {
+    if (cta0) {
         for (int l = H.Lg; l < H.L; ++l) {
             const SaLevel<TV>& g = H.lv[l];
             const SaSm<TV> f = sa_sm(H, smb, l);
@@ -988,21 +989,17 @@ __global__ void __launch_bounds__(512, 1) k_pcg_sa(KParams k, Status* st, const 
         const SaLevel<TV>& f = H.lv[l];
         const SaLevel<TV>& C = H.lv[l + 1];
         sa_cells(all, f.nI, f.nJ, [&](int i, int j) { sa_resid_cell(f, i, j); });
-        target += G;
-        if (!grid_barrier(bar, target, &st->err)) return false;
+        if (!team_sync(T, target)) return false;
         sa_cells(all, C.nI, C.nJ, [&](int I, int J) { sa_restrict_w(f, C, om, I, J); });
-        target += G;
-        return grid_barrier(bar, target, &st->err);
+        return team_sync(T, target);
     };
     auto prolong_level = [&](int l) -> bool {
         const SaLevel<TV>& f = H.lv[l];
         const SaLevel<TV>& C = H.lv[l + 1];
         sa_cells(all, f.nI, f.nJ, [&](int i, int j) { sa_prolong_w(f, C.y, C.P, i, j); });
-        target += G;
-        if (!grid_barrier(bar, target, &st->err)) return false;
+        if (!team_sync(T, target)) return false;
         sa_cells(all, f.nI, f.nJ, [&](int i, int j) { sa_smooth_cell(f, om, i, j); });
-        target += G;
-        return grid_barrier(bar, target, &st->err);
+        return team_sync(T, target);
     };
     // CTA 0: levels [Lg, L) in shared memory, between the copy of level Lg's
     // rhs and pre-smoothed iterate in and of its corrected iterate out
@@ -1044,11 +1041,10 @@ __global__ void __launch_bounds__(512, 1) k_pcg_sa(KParams k, Status* st, const 
     const SaLevel<TV>& C1 = H.lv[1];
     auto vcycle = [&](double& rz, bool first) __attribute__((always_inline)) -> bool {
         if (first) {
-            row_segments<TV>(L0.nI, L0.nJ, [&](int i, int j0, bool act, int lane) {
+            row_segments<TV>(T, L0.nI, L0.nJ, [&](int i, int j0, bool act, int lane) {
                 sa0_resid(A0f, omT, L0.b, L0.x, L0.t, i, j0, act, lane);
             });
-            target += G;
-            if (!grid_barrier(bar, target, &st->err)) return false;
+            if (!team_sync(T, target)) return false;
         }
         {
             // aggregate-row segments of 32 lane groups, one segment per warp
@@ -1060,34 +1056,30 @@ __global__ void __launch_bounds__(512, 1) k_pcg_sa(KParams k, Status* st, const 
                 sa0_restrict_seg(A0f, L0.t, C1, om, I, g, g < Gr, lane);
             }
         }
-        target += G;
-        if (!grid_barrier(bar, target, &st->err)) return false;
+        if (!team_sync(T, target)) return false;
         tick(SA_P_DOWN);
         for (int l = 1; l < H.Lg; ++l) {
             if (!restrict_level(l)) return false;
             tick(SA_P_DOWN + l);
         }
-        if (blockIdx.x == 0) cta_levels();
-        target += G;
-        if (!grid_barrier(bar, target, &st->err)) return false;
+        if (cta0) cta_levels();
+        if (!team_sync(T, target)) return false;
         tick(SA_P_CTA);
         for (int l = H.Lg - 1; l >= 1; --l) {
             if (!prolong_level(l)) return false;
             tick(SA_P_UP + l);
         }
         double acc[1] = {0.0};
-        row_segments<TV>(L0.nI, L0.nJ, [&](int i, int j0, bool act, int lane) {
+        row_segments<TV>(T, L0.nI, L0.nJ, [&](int i, int j0, bool act, int lane) {
             sa0_prolong_t(A0f, L0.x, C1.y, C1.P, L0.t, i, j0, act);
         });
-        target += G;
-        if (!grid_barrier(bar, target, &st->err)) return false;
-        row_segments<TV>(L0.nI, L0.nJ, [&](int i, int j0, bool act, int lane) {
+        if (!team_sync(T, target)) return false;
+        row_segments<TV>(T, L0.nI, L0.nJ, [&](int i, int j0, bool act, int lane) {
             acc[0] += sa0_smooth(A0f, omT, L0.b, L0.t, L0.y, i, j0, act, lane);
         });
         block_sum<1>(acc, sm);
-        if (threadIdx.x == 0) partB[2 * blockIdx.x + 1] = acc[0];
-        target += G;
-        if (!grid_barrier(bar, target, &st->err)) return false;
+        if (threadIdx.x == 0) partB[2 * T.rank + 1] = acc[0];
+        if (!team_sync(T, target)) return false;
         double t2[2];
         sum_partials<2>(partB, G, 2, t2, sm);
         rz = t2[1];
@@ -1096,7 +1088,7 @@ __global__ void __launch_bounds__(512, 1) k_pcg_sa(KParams k, Status* st, const 
     };
 
     double rz = 0.0;
-    if (!vcycle(rz, true)) return;
+    if (!vcycle(rz, true)) return false;
     double beta = 0.0;
     int it = 0;
     TV* pbuf[2] = {B.pa, B.pb};
@@ -1107,11 +1099,11 @@ __global__ void __launch_bounds__(512, 1) k_pcg_sa(KParams k, Status* st, const 
         const TV bt = (TV)beta;
         const bool first = it == 0;
         double accA[1] = {0.0};
-        row_segments<TV>(L0.nI, L0.nJ, [&](int i, int j0, bool act, int lane) {
+        row_segments<TV>(T, L0.nI, L0.nJ, [&](int i, int j0, bool act, int lane) {
             accA[0] += sa0_matvec(A0f, L0.y, pold, bt, first, pnew, B.Ap, i, j0, act, lane);
         });
         block_sum<1>(accA, sm);
-        if (threadIdx.x == 0) partA[blockIdx.x] = accA[0];
+        if (threadIdx.x == 0) partA[T.rank] = accA[0];
         SA_SYNC();
         double pAp[1];
         sum_partials<1>(partA, G, 1, pAp, sm);
@@ -1121,19 +1113,19 @@ __global__ void __launch_bounds__(512, 1) k_pcg_sa(KParams k, Status* st, const 
         const TV* rold = rbuf[it & 1];
         TV* rnew = rbuf[(it + 1) & 1];
         double accB[1] = {0.0};
-        row_segments<TV>(L0.nI, L0.nJ, [&](int i, int j0, bool act, int lane) {
+        row_segments<TV>(T, L0.nI, L0.nJ, [&](int i, int j0, bool act, int lane) {
             accB[0] += sa0_update(A0f, al, omT, pnew, B.Ap, B.x, rold, rnew, L0.x, L0.t, i, j0, act, lane);
         });
         L0.b = rnew;
         block_sum<1>(accB, sm);
-        if (threadIdx.x == 0) partB[2 * blockIdx.x] = accB[0];
+        if (threadIdx.x == 0) partB[2 * T.rank] = accB[0];
         SA_SYNC();
         double tB[2];
         sum_partials<2>(partB, G, 2, tB, sm);
         tick(SA_P_UPDATE);
         if (sqrt(tB[0]) <= rTol) { ++it; break; }
         double rzn = 0.0;
-        if (!vcycle(rzn, false)) return;
+        if (!vcycle(rzn, false)) return false;
         beta = rzn / rz;
         rz = rzn;
     }
@@ -1143,11 +1135,21 @@ __global__ void __launch_bounds__(512, 1) k_pcg_sa(KParams k, Status* st, const 
         pStar[c] = (double)B.x[c];
         if (j == w) pStar[c + 1] = 0.0;
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (T.lead()) {
         st->itersP = it;
         if (rebuild) *H.dirty = 0;
     }
+    return true;
 #undef SA_SYNC
+}
+
+template <typename TV>
+__global__ void __launch_bounds__(512, 1) k_pcg_sa(KParams k, Status* st, const double* dE, const double* dN,
+                                                PcgBufs<TV> B, SaHier<TV> H, double* pStar, double* part,
+                                                unsigned* bar) {
+    if (st->done) return;
+    unsigned target = 0;
+    pcg_sa<TV>(grid_team(bar, &st->err), target, k, st, dE, dN, B, H, pStar, part);
 }
 
 }  // namespace cp

@@ -1892,7 +1892,16 @@ struct cp_batch {
     unsigned* dBar = nullptr;
     int* dErr = nullptr;
     int* dAllDone = nullptr;
-    int* hFlags = nullptr;       // pinned: allDone, err
+    unsigned long long* dProf = nullptr;   // per-phase timers when CP_BATCH_PROFILE is set
+    // team mode (every field runs smoothed aggregation): k_batch_team
+    bool teamMode = false;
+    int team = 4, nTeams = 0;    // CTAs per team, teams
+    size_t teamSmem = 0;         // dynamic shared memory (the largest field's k_pcg_sa staging)
+    int* dOrder = nullptr;       // queue order, largest field first
+    unsigned* dTbar = nullptr;   // [grid * kTeamStride] team barrier counters
+    int* dQueue = nullptr;       // [1 + 2 grid]
+    int* dRunning = nullptr;     // fields still running after a launch
+    int* hFlags = nullptr;       // pinned: allDone (team mode: fields running), err
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaGraphExec_t graph = nullptr;
@@ -1907,6 +1916,9 @@ constexpr int kBatchChunk = 64;   // outer iterations per launch
 constexpr int kBatchTiles[][2] = {{16, 64}, {8, 128}, {32, 32}, {4, 256}, {8, 64}, {16, 32},
                                   {16, 128}, {32, 64}, {8, 256}};
 constexpr size_t kBatchDynSmem = kMgDenseSmem;
+// team sizes the autotuner tries in team mode (CTAs per team)
+constexpr int kBatchTeams[] = {2, 3, 4, 6, 8, 12, 16};
+constexpr int kBatchTeamDefault = 4;
 
 size_t batch_tiles0(const cp_batch* b, int R, int C) {
     size_t t = 0;
@@ -1954,6 +1966,53 @@ BField<TC> batch_field(cp_ctx* c) {
     return bf;
 }
 
+template <typename TC>
+BFieldSa<TC> batch_field_sa(cp_ctx* c) {
+    BFieldSa<TC> bf;
+    memset(&bf, 0, sizeof(bf));
+    bf.k = c->k;
+    bf.st = c->st;
+    bf.u = c->u; bf.v = c->v; bf.p = c->p; bf.uStar = c->uStar; bf.vStar = c->vStar; bf.pStar = c->pStar;
+    bf.dE = c->dE; bf.dN = c->dN; bf.alpha = c->alpha; bf.gamma = c->gamma;
+    bf.U = mom_sys<TC>(c, 0);
+    bf.V = mom_sys<TC>(c, 1);
+    bf.xU0 = (TC*)c->xb[0]; bf.xU1 = (TC*)c->xb[1]; bf.xV0 = (TC*)c->xb[2]; bf.xV1 = (TC*)c->xb[3];
+    bf.B = pcg_bufs<TC>(c);
+    bf.H = sa_hier<TC>(c);
+    bf.H.prof = nullptr;
+    bf.partJ = c->partJ; bf.partM = c->partM; bf.partP = c->partP;
+    bf.hist = c->hist; bf.histCap = c->histCap; bf.dpWin = c->dpWin;
+    return bf;
+}
+
+cp_status batch_set_team(cp_batch* b, int ctas) {
+    if (ctas < 1 || ctas > b->grid) return fail(CP_ERR_BAD_PARAM, "team of %d CTAs (1..%d)", ctas, b->grid);
+    b->team = ctas;
+    b->nTeams = b->grid / ctas;
+    if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; }
+    return CP_OK;
+}
+
+template <typename TC, bool Mixed>
+cp_status batch_launch_team(cp_batch* b, int nOuter) {
+    TeamArgs a{};
+    a.nf = (int)b->f.size();
+    a.team = b->team;
+    a.nTeams = b->nTeams;
+    a.nOuter = nOuter;
+    a.order = b->dOrder;
+    a.tbar = b->dTbar;
+    a.queue = b->dQueue;
+    a.err = b->dErr;
+    a.running = b->dRunning;
+    CK(cudaMemsetAsync(b->dTbar, 0, (size_t)b->grid * kTeamStride * sizeof(unsigned), b->stream));
+    CK(cudaMemsetAsync(b->dQueue, 0, (size_t)(1 + 2 * b->grid) * sizeof(int), b->stream));
+    CK(cudaMemsetAsync(b->dRunning, 0, sizeof(int), b->stream));
+    CK(launch_coop_cfg(k_batch_team<TC, Mixed>, b->grid, kBatchThreads, b->teamSmem, b->stream, a,
+                       (const BFieldSa<TC>*)b->dF));
+    return CP_OK;
+}
+
 cp_status batch_balloc(cp_batch* b, void** p, size_t bytes) {
     CK(cudaMalloc(p, std::max<size_t>(bytes, 1)));
     b->allocs.push_back(*p);
@@ -1984,6 +2043,7 @@ cp_status batch_launch(cp_batch* b, int nOuter) {
     a.nOuter = nOuter;
     a.toff = b->dToff; a.bs = b->dBs; a.ipart = b->dPart; a.bar = b->dBar; a.err = b->dErr;
     a.allDone = b->dAllDone;
+    a.prof = b->dProf;
     CK(cudaMemsetAsync(b->dBar, 0, sizeof(unsigned), b->stream));
     CK(launch_coop_cfg(k_batch<TC, Mixed>, b->grid, kBatchThreads, kBatchDynSmem, b->stream, a,
                        (const BField<TC>*)b->dF));
@@ -1991,6 +2051,8 @@ cp_status batch_launch(cp_batch* b, int nOuter) {
 }
 
 cp_status batch_launch_any(cp_batch* b, int nOuter) {
+    if (b->teamMode)
+        return b->mixed ? batch_launch_team<float, true>(b, nOuter) : batch_launch_team<double, false>(b, nOuter);
     return b->mixed ? batch_launch<float, true>(b, nOuter) : batch_launch<double, false>(b, nOuter);
 }
 
@@ -2025,9 +2087,22 @@ cp_status batch_graph(cp_batch* b, int nOuter) {
 
 template <typename TC>
 cp_status batch_upload_fields(cp_batch* b) {
-    std::vector<BField<TC>> h;
-    for (cp_ctx* c : b->f) h.push_back(batch_field<TC>(c));
-    CK(cudaMemcpyAsync(b->dF, h.data(), h.size() * sizeof(BField<TC>), cudaMemcpyHostToDevice, b->stream));
+    if (b->teamMode) {
+        std::vector<BFieldSa<TC>> h;
+        for (cp_ctx* c : b->f) h.push_back(batch_field_sa<TC>(c));
+        CK(cudaMemcpyAsync(b->dF, h.data(), h.size() * sizeof(BFieldSa<TC>), cudaMemcpyHostToDevice, b->stream));
+        // queue order: largest field first (cells), so the last fields a team
+        // takes are the short ones
+        std::vector<int> order(b->f.size());
+        for (size_t q = 0; q < order.size(); ++q) order[q] = (int)q;
+        auto cells = [&](int q) { return (long long)(b->f[q]->d.M - 1) * (b->f[q]->d.N - 1); };
+        std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return cells(x) > cells(y); });
+        CK(cudaMemcpyAsync(b->dOrder, order.data(), order.size() * sizeof(int), cudaMemcpyHostToDevice, b->stream));
+    } else {
+        std::vector<BField<TC>> h;
+        for (cp_ctx* c : b->f) h.push_back(batch_field<TC>(c));
+        CK(cudaMemcpyAsync(b->dF, h.data(), h.size() * sizeof(BField<TC>), cudaMemcpyHostToDevice, b->stream));
+    }
     CK(cudaStreamSynchronize(b->stream));
     return CP_OK;
 }
@@ -2056,13 +2131,14 @@ cp_status batch_run(cp_batch* b, int max_outer, cp_batch_report* rep, bool useGr
         else if ((s = batch_launch_any(b, n)) != CP_OK) return s;
         ++launches;
         done += n;
-        CK(cudaMemcpyAsync(b->hFlags, b->dAllDone, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
+        CK(cudaMemcpyAsync(b->hFlags, b->teamMode ? b->dRunning : b->dAllDone, sizeof(int),
+                           cudaMemcpyDeviceToHost, b->stream));
         CK(cudaMemcpyAsync(b->hFlags + 1, b->dErr, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
         CK(cudaStreamSynchronize(b->stream));
         if (b->hFlags[1] != 0)
             return fail((cp_status)b->hFlags[1], "device reported %s in the batch",
                         cp_status_string((cp_status)b->hFlags[1]));
-        all = b->hFlags[0] != 0;
+        all = b->teamMode ? b->hFlags[0] == 0 : b->hFlags[0] != 0;
     }
     CK(cudaEventRecord(b->ev1, b->stream));
     CK(cudaEventSynchronize(b->ev1));
@@ -2072,8 +2148,9 @@ cp_status batch_run(cp_batch* b, int max_outer, cp_batch_report* rep, bool useGr
         cudaEventElapsedTime(&ms, b->ev0, b->ev1);
         rep->device_ms = ms;
         rep->launches = launches;
-        rep->tileRows = b->R;
-        rep->tileCols = b->C;
+        rep->tileRows = b->teamMode ? 0 : b->R;
+        rep->tileCols = b->teamMode ? 0 : b->C;
+        rep->teamCtas = b->teamMode ? b->team : 0;
         int maxIt = 0, nd = 0;
         for (cp_ctx* c : b->f) {
             CK(cudaMemcpy(c->stHost, c->st, sizeof(Status), cudaMemcpyDeviceToHost));
@@ -2082,6 +2159,18 @@ cp_status batch_run(cp_batch* b, int max_outer, cp_batch_report* rep, bool useGr
         }
         rep->outerIterations = maxIt;
         rep->fieldsDone = nd;
+    }
+    if (b->dProf) {
+        // CP_BATCH_PROFILE: device time per phase since the batch was made
+        static const char* names[BP_COUNT] = {"bc", "assemble", "jacobi", "jacobi_sum", "scatter", "bc_star",
+                                              "mass", "mass_sum", "coarsen", "coarsen_cta", "restrict",
+                                              "cycle_cta", "prolong", "cycle_sum", "matvec", "matvec_sum",
+                                              "update", "update_sum", "p_star", "correct", "bc_end", "finalize"};
+        unsigned long long t[BP_COUNT];
+        CK(cudaMemcpy(t, b->dProf, sizeof(t), cudaMemcpyDeviceToHost));
+        fprintf(stderr, "CP_BATCH_PROFILE ms:");
+        for (int q = 0; q < BP_COUNT; ++q) fprintf(stderr, " %s %.3f", names[q], t[q] * 1e-6);
+        fprintf(stderr, "\n");
     }
     return CP_OK;
 }
@@ -2127,9 +2216,26 @@ cp_status cp_batch_create(cp_ctx* const* fields, int n, cp_batch** out) {
         cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess ||
         cudaMallocHost(&b->hFlags, 2 * sizeof(int)) != cudaSuccess)
         return bail(fail(CP_ERR_CUDA, "batch stream / events / pinned flags"));
-    // one block per SM: the kernel must fit with its dense set-up workspace
+    // team mode when every field runs smoothed aggregation (CP_BATCH_TILES=1
+    // keeps the tile kernel, which runs the 2 x 2 cycle for every field)
+    b->teamMode = !getenv("CP_BATCH_TILES");
+    for (cp_ctx* c : b->f) b->teamMode = b->teamMode && c->useSa;
+    // one block per SM: the kernel must fit with its shared-memory workspace
     int nb = 0;
-    if (b->mixed) {
+    if (b->teamMode) {
+        for (cp_ctx* c : b->f) b->teamSmem = std::max(b->teamSmem, c->saSmem);
+        if (b->mixed) {
+            cudaFuncSetAttribute(k_batch_team<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)b->teamSmem);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_batch_team<float, true>, kBatchThreads,
+                                                          b->teamSmem);
+        } else {
+            cudaFuncSetAttribute(k_batch_team<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)b->teamSmem);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_batch_team<double, false>, kBatchThreads,
+                                                          b->teamSmem);
+        }
+    } else if (b->mixed) {
         cudaFuncSetAttribute(k_batch<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBatchDynSmem);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_batch<float, true>, kBatchThreads, kBatchDynSmem);
     } else {
@@ -2141,7 +2247,8 @@ cp_status cp_batch_create(cp_ctx* const* fields, int n, cp_batch** out) {
     b->grid = b->numSMs;
     for (const auto& t : kBatchTiles) b->partCap = std::max(b->partCap, batch_tiles0(b, t[0], t[1]));
     const size_t nt = (size_t)(b->maxLg + 1) * (n + 1);
-    const size_t fbytes = b->mixed ? sizeof(BField<float>) : sizeof(BField<double>);
+    const size_t fbytes = b->teamMode ? (b->mixed ? sizeof(BFieldSa<float>) : sizeof(BFieldSa<double>))
+                                      : (b->mixed ? sizeof(BField<float>) : sizeof(BField<double>));
     if ((s = batch_balloc(b, &b->dF, fbytes * n)) != CP_OK) return bail(s);
     if ((s = batch_balloc(b, (void**)&b->dToff, nt * sizeof(int))) != CP_OK) return bail(s);
     if ((s = batch_balloc(b, (void**)&b->dBs, (size_t)n * sizeof(BState))) != CP_OK) return bail(s);
@@ -2150,9 +2257,21 @@ cp_status cp_batch_create(cp_ctx* const* fields, int n, cp_batch** out) {
     if ((s = batch_balloc(b, (void**)&b->dBar, sizeof(unsigned))) != CP_OK) return bail(s);
     if ((s = batch_balloc(b, (void**)&b->dErr, sizeof(int))) != CP_OK) return bail(s);
     if ((s = batch_balloc(b, (void**)&b->dAllDone, sizeof(int))) != CP_OK) return bail(s);
+    if (getenv("CP_BATCH_PROFILE") &&
+        (s = batch_balloc(b, (void**)&b->dProf, BP_COUNT * sizeof(unsigned long long))) != CP_OK)
+        return bail(s);
+    if (b->teamMode) {
+        if ((s = batch_balloc(b, (void**)&b->dOrder, (size_t)n * sizeof(int))) != CP_OK) return bail(s);
+        if ((s = batch_balloc(b, (void**)&b->dTbar, (size_t)b->grid * kTeamStride * sizeof(unsigned))) != CP_OK)
+            return bail(s);
+        if ((s = batch_balloc(b, (void**)&b->dQueue, (size_t)(1 + 2 * b->grid) * sizeof(int))) != CP_OK)
+            return bail(s);
+        if ((s = batch_balloc(b, (void**)&b->dRunning, sizeof(int))) != CP_OK) return bail(s);
+    }
     s = b->mixed ? batch_upload_fields<float>(b) : batch_upload_fields<double>(b);
     if (s != CP_OK) return bail(s);
     if ((s = batch_set_tile(b, b->R, b->C)) != CP_OK) return bail(s);
+    if (b->teamMode && (s = batch_set_team(b, std::min(kBatchTeamDefault, b->grid))) != CP_OK) return bail(s);
     *out = b;
     return CP_OK;
 }
@@ -2175,6 +2294,12 @@ cp_status cp_batch_set_tile(cp_batch* b, int rows, int cols) {
     return batch_set_tile(b, rows, cols);
 }
 
+cp_status cp_batch_set_team(cp_batch* b, int ctas) {
+    if (!b) return fail(CP_ERR_BAD_PARAM, "batch is NULL");
+    if (!b->teamMode) return fail(CP_ERR_UNSUPPORTED, "the batch runs cell tiles (not every field is type 4)");
+    return batch_set_team(b, ctas);
+}
+
 cp_status cp_batch_run(cp_batch* b, int max_outer, cp_batch_report* rep) {
     if (!b) return fail(CP_ERR_BAD_PARAM, "batch is NULL");
     if (max_outer < 0) return fail(CP_ERR_BAD_PARAM, "max_outer < 0");
@@ -2185,6 +2310,30 @@ cp_status cp_batch_autotune(cp_batch* b, int trial_outer, cp_batch_report* best)
     if (!b) return fail(CP_ERR_BAD_PARAM, "batch is NULL");
     if (trial_outer < 1) return fail(CP_ERR_BAD_PARAM, "trial_outer >= 1 required");
     double bestMs = -1.0;
+    if (b->teamMode) {
+        int bT = b->team;
+        for (int t : kBatchTeams) {
+            if (t > b->grid) continue;
+            cp_status s = batch_set_team(b, t);
+            if (s != CP_OK) return s;
+            for (cp_ctx* c : b->f)
+                if ((s = cp_reset(c)) != CP_OK) return s;
+            cp_batch_report r;
+            if ((s = batch_run(b, trial_outer, &r, false)) != CP_OK) return s;
+            if (bestMs < 0.0 || r.device_ms < bestMs) { bestMs = r.device_ms; bT = t; }
+        }
+        cp_status s = batch_set_team(b, bT);
+        if (s != CP_OK) return s;
+        for (cp_ctx* c : b->f)
+            if ((s = cp_reset(c)) != CP_OK) return s;
+        if (best) {
+            memset(best, 0, sizeof(*best));
+            best->teamCtas = bT;
+            best->device_ms = bestMs;
+            best->outerIterations = trial_outer;
+        }
+        return CP_OK;
+    }
     int bR = b->R, bC = b->C;
     for (const auto& t : kBatchTiles) {
         if (batch_tiles0(b, t[0], t[1]) > b->partCap) continue;

@@ -316,30 +316,43 @@ cp_status cp_kernel_times(cp_ctx* ctx, int n_outer, cp_kernel_timing* out);
  * New (the reference runs one field per process, run_solvers.py:248): many
  * fields, each its own context with its own grid size, geometry and
  * parameters, advanced together by one persistent cooperative kernel per
- * launch.  Every phase of the outer iteration covers the rows x cols cell
- * tiles of all fields still iterating; each field keeps its own stop rules
- * (Jacobi, CG and outer loop), history and status, so cp_get_field,
- * cp_get_history and cp_adjoint_dp_dgamma work on a field's context after a
- * batch run as after cp_step.  Requirements: pressureSolverType 2 or 4, the
- * same precision for every field, contexts on one device.  The contexts must
- * outlive the batch and must not be stepped while a batch call runs. */
+ * launch.  Two schedules:
+ *   - teams (every field pressureSolverType 4): the grid is cut into teams
+ *     of consecutive CTAs; each team takes the next field from a queue
+ *     (largest first) and runs its outer iterations with the single-field
+ *     device code (smoothed-aggregation PCG included) on its own barrier;
+ *     the autotuner picks the team size;
+ *   - cell tiles (otherwise; pressureSolverType 2 or 4, every field on the
+ *     2 x 2 aggregation cycle): every phase covers the rows x cols cell
+ *     tiles of all fields still iterating; the autotuner picks the tile.
+ * Each field keeps its own stop rules (Jacobi, CG and outer loop), history
+ * and status, so cp_get_field, cp_get_history and cp_adjoint_dp_dgamma work
+ * on a field's context after a batch run as after cp_step.  Requirements:
+ * pressureSolverType 2 or 4, the same precision for every field, contexts on
+ * one device.  The contexts must outlive the batch and must not be stepped
+ * while a batch call runs. */
 typedef struct cp_batch cp_batch;
 typedef struct cp_batch_report {
     int outerIterations;   /* largest completed outer iteration count     */
     int fieldsDone;        /* fields whose loop has stopped               */
     int launches;          /* persistent-kernel launches (64 iterations each at most) */
-    int tileRows, tileCols;/* cell tile used                              */
+    int tileRows, tileCols;/* cell tile used (0 in team mode)             */
     double device_ms;      /* device time of the call (CUDA events)       */
+    int teamCtas;          /* CTAs per team (0 in cell-tile mode)         */
 } cp_batch_report;
 cp_status cp_batch_create(cp_ctx* const* fields, int n, cp_batch** out);
 cp_status cp_batch_destroy(cp_batch* batch);
-/* rows x cols in [256, 4096]; the default is 16 x 64 */
+/* rows x cols in [256, 4096]; the default is 16 x 64 (cell-tile mode) */
 cp_status cp_batch_set_tile(cp_batch* batch, int rows, int cols);
+/* CTAs per team in [1, SMs]; the default is 4; CP_ERR_UNSUPPORTED in
+ * cell-tile mode */
+cp_status cp_batch_set_team(cp_batch* batch, int ctas);
 /* Runs until every field has stopped or max_outer iterations, in launches of
  * up to 64 outer iterations replayed from a captured CUDA graph. */
 cp_status cp_batch_run(cp_batch* batch, int max_outer, cp_batch_report* rep);
 /* Times trial_outer iterations from the initial state for each candidate tile
- * shape, keeps the fastest, and resets every field (cp_reset) afterwards. */
+ * shape (team mode: team size), keeps the fastest, and resets every field
+ * (cp_reset) afterwards. */
 cp_status cp_batch_autotune(cp_batch* batch, int trial_outer, cp_batch_report* best);
 
 /* Self-test of the bounded device waits.  The persistent kernels wait on
