@@ -525,8 +525,10 @@ def thermal_leg(Simple, torch, args) -> dict:
     precision, THERMAL_FLOW_ITERS outer iterations, untimed): 1024 x 512 x 12
     cells (8 base-plate + 4 channel layers, cases.THERMAL_3D), hotspot power
     map, the reference's rtol 1e-6; then the p-norm (p = 8) adjoint
-    gradient.  Device times from CUDA events on the solver's stream; e2e
-    through the public calls with host arrays (inputs up, T back)."""
+    gradient, in FP64 and in mixed precision (float V-cycle inside the FP64
+    BiCGStab, restarted until the FP64 residual meets rtol; under "mixed").
+    Device times from CUDA events on the solver's stream; e2e through the
+    public calls with host arrays (inputs up, T back)."""
     from coldplate_b200 import Thermal, cases
     from coldplate_b200.thermal import inputs_from_flow
     Ny, Nx = args.thermal_ny, args.thermal_nx
@@ -541,31 +543,37 @@ def thermal_leg(Simple, torch, args) -> dict:
     levels, a, b = 1, Nx, Ny              # 2 x 2 column aggregates down to one column
     while a > 1 or b > 1:
         a, b, levels = (a + 1) // 2, (b + 1) // 2, levels + 1
-    fwd, adj = [], []
-    with Thermal(**prm) as th:
-        th.set_inputs(q0=q0, **fl)
-        for k in range(args.warmup + args.thermal_steps):
-            flush_l2(torch)
-            torch.cuda.synchronize()
-            r = th.solve()
-            flush_l2(torch)
-            torch.cuda.synchronize()
-            J, g, ra = th.pnorm_gradient(THERMAL_P)
-            if k >= args.warmup:
-                fwd.append(r)
-                adj.append(ra)
-        tb_max, _ = th.objective(THERMAL_P)
-        # end to end: host inputs up, solve, T and the objective back
-        e2e = []
-        for k in range(1 + args.thermal_steps):
-            flush_l2(torch)
-            t0 = time.perf_counter()
+    def timed(precision):
+        """warm-up + timed forward and adjoint solves of one precision"""
+        fwd, adj = [], []
+        with Thermal(precision=precision, **prm) as th:
             th.set_inputs(q0=q0, **fl)
-            th.solve()
-            T = th.T
-            th.objective(THERMAL_P)
-            if k >= 1:
-                e2e.append(time.perf_counter() - t0)
+            for k in range(args.warmup + args.thermal_steps):
+                flush_l2(torch)
+                torch.cuda.synchronize()
+                r = th.solve()
+                flush_l2(torch)
+                torch.cuda.synchronize()
+                J, g, ra = th.pnorm_gradient(THERMAL_P)
+                if k >= args.warmup:
+                    fwd.append(r)
+                    adj.append(ra)
+            tb_max, _ = th.objective(THERMAL_P)
+            # end to end: host inputs up, solve, T and the objective back
+            e2e = []
+            for k in range(1 + args.thermal_steps):
+                flush_l2(torch)
+                t0 = time.perf_counter()
+                th.set_inputs(q0=q0, **fl)
+                th.solve()
+                T = th.T
+                th.objective(THERMAL_P)
+                if k >= 1:
+                    e2e.append(time.perf_counter() - t0)
+        return fwd, adj, J, g, tb_max, T, e2e
+
+    fwd_m, adj_m, J_m, g_m, _, _, e2e_m = timed(1)
+    fwd, adj, J, g, tb_max, T, e2e = timed(0)
     t_f = max(r["device_ms"] for r in fwd) / 1e3
     t_a = max(r["device_ms"] for r in adj) / 1e3
     its_f = max(r["iterations"] for r in fwd)
@@ -584,6 +592,26 @@ def thermal_leg(Simple, torch, args) -> dict:
         pass
     peak = float(peaks.get("hbm_gbs", 6650.0))
     achieved = bytes_iter * its_f / t_f / 1e9
+    # the mixed form's bytes per cell and iteration: the V-cycle's levels,
+    # factors and iterates in float, the Krylov vectors it reads (p, s) and
+    # the operator of the FP64 matvecs in double: level 0 482 B (update +
+    # pre-smoothing 48 and 40, restrictions 41 each, prolongation + post-
+    # smoothing 52 each, operator applications 76 each, solution update 56),
+    # the coarse levels 74.8 (the FP64 18.7 words in float)
+    bytes_iter_m = 557 * n
+    t_fm = max(r["device_ms"] for r in fwd_m) / 1e3
+    t_am = max(r["device_ms"] for r in adj_m) / 1e3
+    its_fm = max(r["iterations"] for r in fwd_m)
+    achieved_m = bytes_iter_m * its_fm / t_fm / 1e9
+    mixed = {"t_forward_s": t_fm, "forward_iterations": its_fm, "t_adjoint_s": t_am,
+             "adjoint_iterations": max(r["iterations"] for r in adj_m), "forward_over_fp64": t_fm / t_f,
+             "adjoint_over_fp64": t_am / t_a, "residual_forward": max(r["residual"] for r in fwd_m),
+             "Tb_pnorm_rel_diff_vs_fp64": abs(J_m - J) / abs(J),
+             "dJ_dgamma_max_diff_vs_fp64": float(np.abs(g_m - g).max() / np.abs(g).max()),
+             "e2e_s": float(np.mean(e2e_m)),
+             "roofline": {"bound": "hbm", "achieved": achieved_m, "peak": peak, "unit": "GB/s",
+                          "frac": achieved_m / peak, "kernel": "k_th_bicgstab<false, float>",
+                          "algorithmic_bytes": bytes_iter_m * its_fm}}
     return {"workload": f"density flow {Nx}x{Ny} seed {args.seed} ({THERMAL_FLOW_ITERS} mixed SIMPLE iterations) "
                         f"-> {Nx}x{Ny}x12 CHT (8 plate + 4 channel layers), hotspot power map, rtol 1e-6, "
                         f"p-norm p={THERMAL_P:g}",
@@ -592,7 +620,7 @@ def thermal_leg(Simple, torch, args) -> dict:
             "Tb_max_C": tb_max, "Tb_pnorm_C": J, "max_abs_dJ_dgamma": float(np.abs(g).max()),
             "residual_forward": max(r["residual"] for r in fwd),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "kernel": "k_th_bicgstab<false> (assembly and factorisation inside the time)",
+                         "kernel": "k_th_bicgstab<false, double> (assembly and factorisation inside the time)",
                          "traffic": THERMAL_CAPTURE_BYTES_PER_CELL_ITER * n * its_f,
                          "algorithmic_bytes": bytes_iter * its_f,
                          "traffic_source": "ncu capture at 512x256x12 (78 iterations), scaled by cells x iterations; "
@@ -603,6 +631,7 @@ def thermal_leg(Simple, torch, args) -> dict:
             # launches: assembly, fill, a Galerkin coarsening per coarse level, a
             # z-factorisation per level, the persistent solver; the adjoint adds
             # the p-norm, its right-hand side and the sensitivity
+            "mixed": mixed,
             "multigrid_levels": levels,
             "gpu_launches_per_forward": 2 + (levels - 1) + levels + 1,
             "gpu_launches_per_adjoint": 2 + levels + 1 + 1}

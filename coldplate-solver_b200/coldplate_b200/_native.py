@@ -93,7 +93,7 @@ class CpThermalParams(ctypes.Structure):
     """struct cp_thermal_params (include/cp_thermal.h)."""
     _fields_ = [("Nx", _I), ("Ny", _I), ("nz_solid", _I), ("nz_fluid", _I), ("dx", _D), ("dy", _D),
                 ("H_b", _D), ("H_t", _D), ("k_s", _D), ("k_f", _D), ("rho", _D), ("Cp", _D), ("T_inlet", _D),
-                ("rtol", _D), ("maxiter", _I), ("k_interp_mode", _I), ("qk", _D)]
+                ("rtol", _D), ("maxiter", _I), ("k_interp_mode", _I), ("qk", _D), ("precision", _I)]
 
 
 class CpThermalReport(ctypes.Structure):

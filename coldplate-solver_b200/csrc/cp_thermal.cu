@@ -79,6 +79,7 @@ constexpr double kThOmega = 0.8;          // z-line Jacobi damping
 constexpr double kThScale0 = 1.4;         // coarse-correction factor into level 0
 constexpr double kThScale = 1.4;          // ... into the deeper levels (1.2 / 1.1: 95 / more iterations
                                           // at 1024 x 512 x 12, against 84)
+constexpr int kThRefineRounds = 4;        // mixed precision: BiCGStab launches per solve at most
 
 }  // namespace
 
@@ -90,9 +91,14 @@ struct ThK {
     double dx, dy, dzS, dzF, Ht, kS, kF, rhoCp, Tin, qk;
 };
 
-struct ThSys {
-    double *aP, *aW, *aE, *aS, *aN, *aB, *aT, *b;
+// The seven coefficient arrays of a 7-point system and its right-hand side
+// (T = double: the assembled system and its Galerkin levels; T = float: the
+// preconditioner's copies in the mixed-precision solve)
+template <typename T>
+struct ThSysT {
+    T *aP, *aW, *aE, *aS, *aN, *aB, *aT, *b;
 };
+using ThSys = ThSysT<double>;
 
 struct ThStatus {
     int iterations, converged, err, pad;
@@ -232,50 +238,52 @@ __global__ void k_th_assemble(ThK k, const double* gamma, const double* u_xy, co
 // One level of the hierarchy (level 0: the assembled system).  x holds the
 // pre-smoothed iterate, b the restricted residual and y the post-smoothed
 // iterate of a coarse level.
-struct ThLevel {
+template <typename T>
+struct ThLevelT {
     int nx, ny;
     long long ncol, n;
-    ThSys S;
-    double *lc, *linv;
-    double *b, *x, *y;
+    ThSysT<T> S;
+    T *lc, *linv;
+    T *b, *x, *y;
 };
+using ThLevel = ThLevelT<double>;
 
 // Entries of row q of A (Tr = false) or of A^T (Tr = true) towards the
 // west, east, south, north, lower and upper neighbour.  Row q of A^T holds
 // column q of A: its west entry is the east coefficient of the west cell.
-template <bool Tr>
-__device__ __forceinline__ double th_cW(const ThSys& S, long long q) { return __ldg(Tr ? S.aE + (q - 1) : S.aW + q); }
-template <bool Tr>
-__device__ __forceinline__ double th_cE(const ThSys& S, long long q) { return __ldg(Tr ? S.aW + (q + 1) : S.aE + q); }
-template <bool Tr>
-__device__ __forceinline__ double th_cS(const ThSys& S, long long q, int nx) {
+template <bool Tr, typename T>
+__device__ __forceinline__ T th_cW(const ThSysT<T>& S, long long q) { return __ldg(Tr ? S.aE + (q - 1) : S.aW + q); }
+template <bool Tr, typename T>
+__device__ __forceinline__ T th_cE(const ThSysT<T>& S, long long q) { return __ldg(Tr ? S.aW + (q + 1) : S.aE + q); }
+template <bool Tr, typename T>
+__device__ __forceinline__ T th_cS(const ThSysT<T>& S, long long q, int nx) {
     return __ldg(Tr ? S.aN + (q - nx) : S.aS + q);
 }
-template <bool Tr>
-__device__ __forceinline__ double th_cN(const ThSys& S, long long q, int nx) {
+template <bool Tr, typename T>
+__device__ __forceinline__ T th_cN(const ThSysT<T>& S, long long q, int nx) {
     return __ldg(Tr ? S.aS + (q + nx) : S.aN + q);
 }
-template <bool Tr>
-__device__ __forceinline__ double th_sub(const ThSys& S, long long q, long long L) {
+template <bool Tr, typename T>
+__device__ __forceinline__ T th_sub(const ThSysT<T>& S, long long q, long long L) {
     return __ldg(Tr ? S.aT + (q - L) : S.aB + q);
 }
-template <bool Tr>
-__device__ __forceinline__ double th_sup(const ThSys& S, long long q, long long L) {
+template <bool Tr, typename T>
+__device__ __forceinline__ T th_sup(const ThSysT<T>& S, long long q, long long L) {
     return __ldg(Tr ? S.aB + (q + L) : S.aT + q);
 }
 
-// (op x)_q on a level, op = A or A^T
-template <bool Tr>
-__device__ __forceinline__ double th_ax(const ThLevel& F, int Nz, const double* x, long long q, int i, int j,
-                                        int kk) {
+// (op x)_q on a level, op = A or A^T, in the level's arithmetic T (x may be
+// stored narrower: the FP64 matvec of a float preconditioner output)
+template <bool Tr, typename T, typename X>
+__device__ __forceinline__ T th_ax(const ThLevelT<T>& F, int Nz, const X* x, long long q, int i, int j, int kk) {
     const long long L = F.ncol;
-    double s = __ldg(F.S.aP + q) * x[q];
-    if (i > 0) s += th_cW<Tr>(F.S, q) * x[q - 1];
-    if (i < F.nx - 1) s += th_cE<Tr>(F.S, q) * x[q + 1];
-    if (j > 0) s += th_cS<Tr>(F.S, q, F.nx) * x[q - F.nx];
-    if (j < F.ny - 1) s += th_cN<Tr>(F.S, q, F.nx) * x[q + F.nx];
-    if (kk > 0) s += th_sub<Tr>(F.S, q, L) * x[q - L];
-    if (kk < Nz - 1) s += th_sup<Tr>(F.S, q, L) * x[q + L];
+    T s = __ldg(F.S.aP + q) * T(x[q]);
+    if (i > 0) s += th_cW<Tr>(F.S, q) * T(x[q - 1]);
+    if (i < F.nx - 1) s += th_cE<Tr>(F.S, q) * T(x[q + 1]);
+    if (j > 0) s += th_cS<Tr>(F.S, q, F.nx) * T(x[q - F.nx]);
+    if (j < F.ny - 1) s += th_cN<Tr>(F.S, q, F.nx) * T(x[q + F.nx]);
+    if (kk > 0) s += th_sub<Tr>(F.S, q, L) * T(x[q - L]);
+    if (kk < Nz - 1) s += th_sup<Tr>(F.S, q, L) * T(x[q + L]);
     return s;
 }
 
@@ -310,6 +318,12 @@ __global__ void k_th_coarsen(int Nz, ThLevel F, ThLevel C) {
     }
 }
 
+// float copy of a level array (the mixed-precision preconditioner's levels)
+__global__ void k_th_narrow(const double* __restrict__ src, float* __restrict__ dst, long long n) {
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+        dst[q] = (float)src[q];
+}
+
 // Thomas factors of each column's tridiagonal z-block of a level:
 // inv_k = 1 / (d_k - sub_k c_{k-1}), c_k = sup_k inv_k
 template <bool Tr>
@@ -337,62 +351,70 @@ __global__ void k_th_lu(int Nz, ThLevel F) {
 struct ThSm {
     double* ys;
     double* st;
-    __device__ __forceinline__ double& y(int kk) const { return ys[kk * blockDim.x + threadIdx.x]; }
-    __device__ __forceinline__ double& s(int a, int u) const {
-        return st[(a * kThStage + u) * blockDim.x + threadIdx.x];
+    // a slot holds one value of type S (double or float) in its first bytes
+    template <typename S = double>
+    __device__ __forceinline__ S& y(int kk) const {
+        return *reinterpret_cast<S*>(ys + kk * blockDim.x + threadIdx.x);
+    }
+    template <typename S = double>
+    __device__ __forceinline__ S& s(int a, int u) const {
+        return *reinterpret_cast<S*>(st + (a * kThStage + u) * blockDim.x + threadIdx.x);
     }
 };
 
-__device__ __forceinline__ void th_stage(double* dst, const double* src) { __pipeline_memcpy_async(dst, src, 8); }
+template <typename S>
+__device__ __forceinline__ void th_stage(S* dst, const S* src) { __pipeline_memcpy_async(dst, src, sizeof(S)); }
 
 // Pre-smoothing from zero over the columns of a level: b = A0 + c1 A1 +
 // c2 A2 (A1, A2 optional; stored to bout when set), x = omega Mz^-1 b.  The
 // inputs of kThStage layers are copied to shared memory asynchronously, all
 // in flight together, and the Thomas recurrence runs from shared memory.
-template <bool Tr>
-__device__ __forceinline__ void th_presmooth(const ThLevel& F, int Nz, const double* A0, const double* A1, double c1,
-                                             const double* A2, double c2, double* bout, double* x, double omega,
-                                             long long t0, long long nt, const ThSm& sm) {
+// T is the level's type, B the type of the right-hand side's terms (double
+// at level 0, where b is a Krylov vector; T on the coarse levels).
+template <bool Tr, typename T, typename B>
+__device__ __forceinline__ void th_presmooth(const ThLevelT<T>& F, int Nz, const B* A0, const B* A1, double c1,
+                                             const B* A2, double c2, B* bout, T* x, double omega, long long t0,
+                                             long long nt, const ThSm& sm) {
     const long long L = F.ncol;
     for (long long col = t0; col < F.ncol; col += nt) {
-        double yprev = 0.0;
+        T yprev = T(0);
         for (int k0 = 0; k0 < Nz; k0 += kThStage) {
             const int nu = min(kThStage, Nz - k0);
             for (int u = 0; u < nu; ++u) {
                 const int kk = k0 + u;
                 const long long q = kk * L + col;
-                th_stage(&sm.s(0, u), A0 + q);
-                if (A1) th_stage(&sm.s(1, u), A1 + q);
-                if (A2) th_stage(&sm.s(2, u), A2 + q);
-                if (kk > 0) th_stage(&sm.s(3, u), Tr ? F.S.aT + (q - L) : F.S.aB + q);
-                th_stage(&sm.s(4, u), F.linv + q);
+                th_stage(&sm.s<B>(0, u), A0 + q);
+                if (A1) th_stage(&sm.s<B>(1, u), A1 + q);
+                if (A2) th_stage(&sm.s<B>(2, u), A2 + q);
+                if (kk > 0) th_stage(&sm.s<T>(3, u), Tr ? F.S.aT + (q - L) : F.S.aB + q);
+                th_stage(&sm.s<T>(4, u), F.linv + q);
             }
             __pipeline_commit();
             __pipeline_wait_prior(0);
             for (int u = 0; u < nu; ++u) {
                 const int kk = k0 + u;
-                double b = sm.s(0, u);
-                if (A1) b += c1 * sm.s(1, u);
-                if (A2) b += c2 * sm.s(2, u);
+                B b = sm.s<B>(0, u);
+                if (A1) b += c1 * sm.s<B>(1, u);
+                if (A2) b += c2 * sm.s<B>(2, u);
                 if (bout) bout[kk * L + col] = b;
-                const double sub = kk > 0 ? sm.s(3, u) : 0.0;
-                yprev = (b - sub * yprev) * sm.s(4, u);
-                sm.y(kk) = yprev;
+                const T sub = kk > 0 ? sm.s<T>(3, u) : T(0);
+                yprev = (T(b) - sub * yprev) * sm.s<T>(4, u);
+                sm.y<T>(kk) = yprev;
             }
         }
-        double xn = 0.0;
+        T xn = T(0);
         for (int k0 = ((Nz - 1) / kThStage) * kThStage; k0 >= 0; k0 -= kThStage) {
             const int nu = min(kThStage, Nz - k0);
             for (int u = 0; u < nu; ++u) {
                 const int kk = k0 + u;
-                if (kk < Nz - 1) th_stage(&sm.s(0, u), F.lc + (kk * L + col));
+                if (kk < Nz - 1) th_stage(&sm.s<T>(0, u), F.lc + (kk * L + col));
             }
             __pipeline_commit();
             __pipeline_wait_prior(0);
             for (int u = nu - 1; u >= 0; --u) {
                 const int kk = k0 + u;
-                const double xv = sm.y(kk) - (kk < Nz - 1 ? sm.s(0, u) * xn : 0.0);
-                x[kk * L + col] = omega * xv;
+                const T xv = sm.y<T>(kk) - (kk < Nz - 1 ? sm.s<T>(0, u) * xn : T(0));
+                x[kk * L + col] = T(omega) * xv;
                 xn = xv;
             }
         }
@@ -402,20 +424,20 @@ __device__ __forceinline__ void th_presmooth(const ThLevel& F, int Nz, const dou
 // Residual restriction: bC = sum over the 2 x 2 aggregate of (bF - op xF).
 // The four fine residuals are independent, so their loads are in flight
 // together; index math in 32 bits (levels hold fewer than 2^31 cells).
-template <bool Tr>
-__device__ __forceinline__ void th_restrict(const ThLevel& F, const ThLevel& C, int Nz, const double* bF,
-                                            const double* xF, double* bC, long long t0, long long nt) {
+template <bool Tr, typename T, typename B>
+__device__ __forceinline__ void th_restrict(const ThLevelT<T>& F, const ThLevelT<T>& C, int Nz, const B* bF,
+                                            const T* xF, T* bC, long long t0, long long nt) {
     const unsigned LC = (unsigned)C.ncol, cnx = (unsigned)C.nx, LF = (unsigned)F.ncol;
     for (unsigned qc = (unsigned)t0; qc < (unsigned)C.n; qc += (unsigned)nt) {
         const unsigned kk = qc / LC, rem = qc - kk * LC, J = rem / cnx, I = rem - J * cnx;
-        double r[4];
+        T r[4];
 #pragma unroll
         for (int d = 0; d < 4; ++d) {
             const int i = 2 * (int)I + (d & 1), j = 2 * (int)J + (d >> 1);
-            r[d] = 0.0;
+            r[d] = T(0);
             if (i < F.nx && j < F.ny) {
                 const long long q = (long long)kk * LF + (long long)j * F.nx + i;
-                r[d] = bF[q] - th_ax<Tr>(F, Nz, xF, q, i, j, (int)kk);
+                r[d] = T(bF[q]) - th_ax<Tr>(F, Nz, xF, q, i, j, (int)kk);
             }
         }
         bC[qc] = ((r[0] + r[1]) + r[2]) + r[3];
@@ -426,14 +448,14 @@ __device__ __forceinline__ void th_restrict(const ThLevel& F, const ThLevel& C, 
 // iterate xp = xF + scale P xC formed on the fly at every stencil point.
 // Two cells a thread per step (their loads in flight together), 32-bit
 // index math.
-template <bool Tr>
-__device__ __forceinline__ double th_post_res1(const ThLevel& F, const ThLevel& C, int Nz, const double* bF,
-                                               const double* xF, const double* xC, double scale, unsigned q) {
+template <bool Tr, typename T, typename B>
+__device__ __forceinline__ T th_post_res1(const ThLevelT<T>& F, const ThLevelT<T>& C, int Nz, const B* bF,
+                                          const T* xF, const T* xC, T scale, unsigned q) {
     const unsigned L = (unsigned)F.ncol, LC = (unsigned)C.ncol, nx = (unsigned)F.nx, cnx = (unsigned)C.nx;
     const unsigned kk = q / L, col = q - kk * L, ju = col / nx, iu = col - ju * nx;
     const int i = (int)iu, j = (int)ju;
     const unsigned kc = kk * LC, cj = (ju >> 1) * cnx;
-    double ax = __ldg(F.S.aP + q) * (xF[q] + scale * xC[kc + cj + (iu >> 1)]);
+    T ax = __ldg(F.S.aP + q) * (xF[q] + scale * xC[kc + cj + (iu >> 1)]);
     if (i > 0) ax += th_cW<Tr>(F.S, q) * (xF[q - 1] + scale * xC[kc + cj + ((iu - 1) >> 1)]);
     if (i < F.nx - 1) ax += th_cE<Tr>(F.S, q) * (xF[q + 1] + scale * xC[kc + cj + ((iu + 1) >> 1)]);
     if (j > 0) ax += th_cS<Tr>(F.S, q, F.nx) * (xF[q - nx] + scale * xC[kc + ((ju - 1) >> 1) * cnx + (iu >> 1)]);
@@ -441,81 +463,86 @@ __device__ __forceinline__ double th_post_res1(const ThLevel& F, const ThLevel& 
         ax += th_cN<Tr>(F.S, q, F.nx) * (xF[q + nx] + scale * xC[kc + ((ju + 1) >> 1) * cnx + (iu >> 1)]);
     if (kk > 0) ax += th_sub<Tr>(F.S, q, L) * (xF[q - L] + scale * xC[kc - LC + cj + (iu >> 1)]);
     if ((int)kk < Nz - 1) ax += th_sup<Tr>(F.S, q, L) * (xF[q + L] + scale * xC[kc + LC + cj + (iu >> 1)]);
-    return bF[q] - ax;
+    return T(bF[q]) - ax;
 }
 
-template <bool Tr>
-__device__ __forceinline__ void th_post_resid(const ThLevel& F, const ThLevel& C, int Nz, const double* bF,
-                                              const double* xF, const double* xC, double scale, double* out,
-                                              long long t0, long long nt) {
+template <bool Tr, typename T, typename B>
+__device__ __forceinline__ void th_post_resid(const ThLevelT<T>& F, const ThLevelT<T>& C, int Nz, const B* bF,
+                                              const T* xF, const T* xC, double scale, T* out, long long t0,
+                                              long long nt) {
     const unsigned n = (unsigned)F.n, st = (unsigned)nt;
+    const T sc = T(scale);
     unsigned q = (unsigned)t0;
     for (; q + st < n; q += 2 * st) {
-        const double r0 = th_post_res1<Tr>(F, C, Nz, bF, xF, xC, scale, q);
-        const double r1 = th_post_res1<Tr>(F, C, Nz, bF, xF, xC, scale, q + st);
+        const T r0 = th_post_res1<Tr>(F, C, Nz, bF, xF, xC, sc, q);
+        const T r1 = th_post_res1<Tr>(F, C, Nz, bF, xF, xC, sc, q + st);
         out[q] = r0;
         out[q + st] = r1;
     }
-    if (q < n) out[q] = th_post_res1<Tr>(F, C, Nz, bF, xF, xC, scale, q);
+    if (q < n) out[q] = th_post_res1<Tr>(F, C, Nz, bF, xF, xC, sc, q);
 }
 
 // Post-smoothing, second half (columns): out = xp + omega Mz^-1 out, in
 // place (each column reads its residual before writing the result)
-template <bool Tr>
-__device__ __forceinline__ void th_post_cols(const ThLevel& F, const ThLevel& C, int Nz, const double* xF,
-                                             const double* xC, double scale, double omega, double* out,
-                                             long long t0, long long nt, const ThSm& sm) {
+template <bool Tr, typename T>
+__device__ __forceinline__ void th_post_cols(const ThLevelT<T>& F, const ThLevelT<T>& C, int Nz, const T* xF,
+                                             const T* xC, double scale, double omega, T* out, long long t0,
+                                             long long nt, const ThSm& sm) {
     const long long L = F.ncol, LC = C.ncol;
     for (long long col = t0; col < F.ncol; col += nt) {
         const int i = (int)(col % F.nx), j = (int)(col / F.nx);
         const long long c0 = (long long)(j >> 1) * C.nx + (i >> 1);
-        double yprev = 0.0;
+        T yprev = T(0);
         for (int k0 = 0; k0 < Nz; k0 += kThStage) {
             const int nu = min(kThStage, Nz - k0);
             for (int u = 0; u < nu; ++u) {
                 const int kk = k0 + u;
                 const long long q = kk * L + col;
-                th_stage(&sm.s(0, u), out + q);
-                if (kk > 0) th_stage(&sm.s(1, u), Tr ? F.S.aT + (q - L) : F.S.aB + q);
-                th_stage(&sm.s(2, u), F.linv + q);
+                th_stage(&sm.s<T>(0, u), out + q);
+                if (kk > 0) th_stage(&sm.s<T>(1, u), Tr ? F.S.aT + (q - L) : F.S.aB + q);
+                th_stage(&sm.s<T>(2, u), F.linv + q);
             }
             __pipeline_commit();
             __pipeline_wait_prior(0);
             for (int u = 0; u < nu; ++u) {
                 const int kk = k0 + u;
-                const double sub = kk > 0 ? sm.s(1, u) : 0.0;
-                yprev = (sm.s(0, u) - sub * yprev) * sm.s(2, u);
-                sm.y(kk) = yprev;
+                const T sub = kk > 0 ? sm.s<T>(1, u) : T(0);
+                yprev = (sm.s<T>(0, u) - sub * yprev) * sm.s<T>(2, u);
+                sm.y<T>(kk) = yprev;
             }
         }
-        double cnext = 0.0;
+        T cnext = T(0);
         for (int k0 = ((Nz - 1) / kThStage) * kThStage; k0 >= 0; k0 -= kThStage) {
             const int nu = min(kThStage, Nz - k0);
             for (int u = 0; u < nu; ++u) {
                 const int kk = k0 + u;
                 const long long q = kk * L + col;
-                if (kk < Nz - 1) th_stage(&sm.s(0, u), F.lc + q);
-                th_stage(&sm.s(1, u), xF + q);
-                th_stage(&sm.s(2, u), xC + (kk * LC + c0));
+                if (kk < Nz - 1) th_stage(&sm.s<T>(0, u), F.lc + q);
+                th_stage(&sm.s<T>(1, u), xF + q);
+                th_stage(&sm.s<T>(2, u), xC + (kk * LC + c0));
             }
             __pipeline_commit();
             __pipeline_wait_prior(0);
             for (int u = nu - 1; u >= 0; --u) {
                 const int kk = k0 + u;
-                const double corr = sm.y(kk) - (kk < Nz - 1 ? sm.s(0, u) * cnext : 0.0);
-                out[kk * L + col] = sm.s(1, u) + scale * sm.s(2, u) + omega * corr;
+                const T corr = sm.y<T>(kk) - (kk < Nz - 1 ? sm.s<T>(0, u) * cnext : T(0));
+                out[kk * L + col] = sm.s<T>(1, u) + T(scale) * sm.s<T>(2, u) + T(omega) * corr;
                 cnext = corr;
             }
         }
     }
 }
 
-struct ThHier {
+// The preconditioner's hierarchy in type T (level 0's arrays: copies of the
+// assembled system when T is float)
+template <typename T>
+struct ThHierT {
     int L, cta;             // levels; first level run by block 0 alone (L: none)
     double omega, scale0, scale;   // coarse-correction factor into level 0, into the deeper levels
-    const ThLevel* lv;      // device array of L levels
+    const ThLevelT<T>* lv;  // device array of L levels
     unsigned long long* prof;  // per-phase nanoseconds (CP_TH_PROFILE), or null
 };
+using ThHier = ThHierT<double>;
 
 // phase slots of the profile: the BiCGStab phases, then 16 slots per
 // V-cycle phase kind indexed by level
@@ -525,17 +552,24 @@ enum ThProfSlot {
     TH_P_COUNT = 80
 };
 
-struct ThVecs {
-    double *x, *r, *rh, *p, *v, *s, *t, *ph, *sh;
+// BiCGStab's vectors, FP64; the preconditioned directions ph = M^-1 p and
+// sh = M^-1 s are stored in the preconditioner's type T
+template <typename T>
+struct ThVecsT {
+    double *x, *r, *rh, *p, *v, *s, *t;
+    T *ph, *sh;
 };
+using ThVecs = ThVecsT<double>;
 
 // BiCGStab (van der Vorst), right-preconditioned by one V-cycle, for
 // A x = rhs (Tr = false) or A^T x = rhs (Tr = true), from the x in V.x.
-// Dynamic shared memory: kThSmemBytes (the column sweeps' staging).
-template <bool Tr>
-__global__ void __launch_bounds__(kThThreads, 2) k_th_bicgstab(ThK k, ThHier H, const double* rhs, ThVecs V,
-                                                              double* part, unsigned* bar, ThStatus* st, int maxiter,
-                                                              double rtol) {
+// F0 is the FP64 system (matvecs, residuals, dot products); the V-cycle runs
+// on H in type T (T = float: the mixed-precision form; T = double: H.lv[0]
+// is F0).  Dynamic shared memory: kThSmemBytes (the column sweeps' staging).
+template <bool Tr, typename T>
+__global__ void __launch_bounds__(kThThreads, 2) k_th_bicgstab(ThK k, ThLevel F0, ThHierT<T> H, const double* rhs,
+                                                              ThVecsT<T> V, double* part, unsigned* bar, ThStatus* st,
+                                                              int maxiter, double rtol) {
     __shared__ double sm[96];
     extern __shared__ double th_dyn[];
     const ThSm cs{th_dyn, th_dyn + kThZ * blockDim.x};
@@ -545,7 +579,6 @@ __global__ void __launch_bounds__(kThThreads, 2) k_th_bicgstab(ThK k, ThHier H, 
     double* pA = part;             // [G][2]
     double* pB = part + 2 * G;     // [G][2]
     double* pC = part + 4 * G;     // [G][2]
-    const ThLevel& F0 = H.lv[0];
     unsigned long long tprev = (H.prof && blockIdx.x == 0 && threadIdx.x == 0) ? globaltimer_ns() : 0ull;
     // grid barrier; with the profile on, block 0 books the time since the
     // previous barrier to the phase slot
@@ -584,28 +617,34 @@ __global__ void __launch_bounds__(kThThreads, 2) k_th_bicgstab(ThK k, ThHier H, 
         }
         if (q < n) commit((long long)q, at(q));
     };
-    // The V-cycle after the level-0 pre-smoothing (F0.x = omega Mz^-1 b0):
+    // The V-cycle after the level-0 pre-smoothing (H.lv[0].x = omega Mz^-1 b0):
     // out0 = M^-1 b0.  Ends with a grid barrier.
-    auto vcycle = [&](const double* b0, double* out0) -> bool {
+    auto vcycle = [&](const double* b0, T* out0) __attribute__((always_inline)) -> bool {
         const int L = H.L;
+        // residual restriction from level l (its right-hand side: b0 at level 0)
+        auto restrict_from = [&](int l) __attribute__((always_inline)) {
+            const ThLevelT<T> &F = H.lv[l], &C = H.lv[l + 1];
+            if (l == 0) th_restrict<Tr>(F, C, Nz, b0, F.x, C.b, tid, nth);
+            else th_restrict<Tr>(F, C, Nz, F.b, F.x, C.b, tid, nth);
+        };
         int l = 0;
         for (; l + 1 < L && l + 1 < H.cta; ++l) {
-            const ThLevel &F = H.lv[l], &C = H.lv[l + 1];
-            th_restrict<Tr>(F, C, Nz, l == 0 ? b0 : F.b, F.x, C.b, tid, nth);
+            const ThLevelT<T>& C = H.lv[l + 1];
+            restrict_from(l);
             if (!sync(TH_P_RESTRICT + l)) return false;
-            th_presmooth<Tr>(C, Nz, C.b, nullptr, 0.0, nullptr, 0.0, nullptr, C.x, l + 2 == L ? 1.0 : H.omega, tid,
-                             nth, cs);
+            th_presmooth<Tr>(C, Nz, C.b, (const T*)nullptr, 0.0, (const T*)nullptr, 0.0, (T*)nullptr, C.x,
+                             l + 2 == L ? 1.0 : H.omega, tid, nth, cs);
             if (!sync(TH_P_PRESMOOTH + l + 1)) return false;
         }
         if (l + 1 < L) {
             // levels l+1 .. L-1 are small: restrict to l+1 grid-wide, then block 0
-            th_restrict<Tr>(H.lv[l], H.lv[l + 1], Nz, l == 0 ? b0 : H.lv[l].b, H.lv[l].x, H.lv[l + 1].b, tid, nth);
+            restrict_from(l);
             if (!sync(TH_P_RESTRICT + l)) return false;
             if (blockIdx.x == 0) {
                 const long long bt = threadIdx.x, bn = blockDim.x;
                 for (int m = l + 1;; ++m) {
-                    const ThLevel& C = H.lv[m];
-                    th_presmooth<Tr>(C, Nz, C.b, nullptr, 0.0, nullptr, 0.0, nullptr, C.x,
+                    const ThLevelT<T>& C = H.lv[m];
+                    th_presmooth<Tr>(C, Nz, C.b, (const T*)nullptr, 0.0, (const T*)nullptr, 0.0, (T*)nullptr, C.x,
                                      m + 1 == L ? 1.0 : H.omega, bt, bn, cs);
                     __syncthreads();
                     if (m + 1 == L) break;
@@ -613,8 +652,8 @@ __global__ void __launch_bounds__(kThThreads, 2) k_th_bicgstab(ThK k, ThHier H, 
                     __syncthreads();
                 }
                 for (int m = L - 2; m >= l + 1; --m) {
-                    const ThLevel &F = H.lv[m], &C = H.lv[m + 1];
-                    const double* xc = m + 2 == L ? C.x : C.y;
+                    const ThLevelT<T> &F = H.lv[m], &C = H.lv[m + 1];
+                    const T* xc = m + 2 == L ? C.x : C.y;
                     th_post_resid<Tr>(F, C, Nz, F.b, F.x, xc, H.scale, F.y, bt, bn);
                     __syncthreads();
                     th_post_cols<Tr>(F, C, Nz, F.x, xc, H.scale, H.omega, F.y, bt, bn, cs);   // m >= 1
@@ -626,11 +665,12 @@ __global__ void __launch_bounds__(kThThreads, 2) k_th_bicgstab(ThK k, ThHier H, 
             l = L - 2;   // every level grid-wide: the ascent starts above the bottom
         }
         for (int m = l; m >= 0; --m) {
-            const ThLevel &F = H.lv[m], &C = H.lv[m + 1];
-            const double* xc = m + 2 == L ? C.x : C.y;
-            double* out = m == 0 ? out0 : F.y;
+            const ThLevelT<T> &F = H.lv[m], &C = H.lv[m + 1];
+            const T* xc = m + 2 == L ? C.x : C.y;
+            T* out = m == 0 ? out0 : F.y;
             const double sc = m == 0 ? H.scale0 : H.scale;
-            th_post_resid<Tr>(F, C, Nz, m == 0 ? b0 : F.b, F.x, xc, sc, out, tid, nth);
+            if (m == 0) th_post_resid<Tr>(F, C, Nz, b0, F.x, xc, sc, out, tid, nth);
+            else th_post_resid<Tr>(F, C, Nz, F.b, F.x, xc, sc, out, tid, nth);
             if (!sync(TH_P_POSTRES + m)) return false;
             th_post_cols<Tr>(F, C, Nz, F.x, xc, sc, H.omega, out, tid, nth, cs);
             if (!sync(TH_P_POSTCOL + m)) return false;
@@ -664,7 +704,8 @@ __global__ void __launch_bounds__(kThThreads, 2) k_th_bicgstab(ThK k, ThHier H, 
         if (rho1 == 0.0) break;
         const double beta = (rho1 / rho) * (alpha / omega);
         // ---- p = r + beta p - beta omega v, fused with the level-0 pre-smoothing; ph = M^-1 p
-        th_presmooth<Tr>(F0, Nz, V.r, V.p, beta, V.v, -beta * omega, V.p, F0.x, H.omega, tid, nth, cs);
+        th_presmooth<Tr>(H.lv[0], Nz, (const double*)V.r, (const double*)V.p, beta, (const double*)V.v,
+                         -beta * omega, V.p, H.lv[0].x, H.omega, tid, nth, cs);
         if (!sync(TH_P_PRE_P)) return;
         if (!vcycle(V.p, V.ph)) return;
         // ---- v = op ph; (rh, v)
@@ -685,7 +726,8 @@ __global__ void __launch_bounds__(kThThreads, 2) k_th_bicgstab(ThK k, ThHier H, 
         if (rv[0] == 0.0) break;
         alpha = rho1 / rv[0];
         // ---- s = r - alpha v, fused with the level-0 pre-smoothing; sh = M^-1 s
-        th_presmooth<Tr>(F0, Nz, V.r, V.v, -alpha, nullptr, 0.0, V.s, F0.x, H.omega, tid, nth, cs);
+        th_presmooth<Tr>(H.lv[0], Nz, (const double*)V.r, (const double*)V.v, -alpha, (const double*)nullptr, 0.0,
+                         V.s, H.lv[0].x, H.omega, tid, nth, cs);
         if (!sync(TH_P_PRE_S)) return;
         if (!vcycle(V.s, V.sh)) return;
         // ---- t = op sh; (t, s), (t, t)
@@ -709,7 +751,8 @@ __global__ void __launch_bounds__(kThThreads, 2) k_th_bicgstab(ThK k, ThHier H, 
         {
             double acc[2] = {0.0, 0.0};
             cells2([&](long long q, int, int, int) {
-                return make_double3(V.x[q] + alpha * V.ph[q] + omega * V.sh[q], V.s[q] - omega * V.t[q], V.rh[q]);
+                return make_double3(V.x[q] + alpha * double(V.ph[q]) + omega * double(V.sh[q]), V.s[q] - omega * V.t[q],
+                                    V.rh[q]);
             }, [&](long long q, double3 a) {
                 V.x[q] = a.x;
                 V.r[q] = a.y;
@@ -855,6 +898,13 @@ struct cp_thermal {
     std::vector<ThLevel> lv;          // the hierarchy (level 0: S, lc, linv, z0)
     ThLevel* dlv = nullptr;           // its device copy
     ThHier H{};
+    // CP_PREC_MIXED: float copies of every level for the V-cycle, and the
+    // preconditioned directions in float
+    bool mixed = false;
+    std::vector<ThLevelT<float>> lvf;
+    ThLevelT<float>* dlvf = nullptr;
+    ThHierT<float> Hf{};
+    float *phf = nullptr, *shf = nullptr;
     double* part = nullptr;
     unsigned* bar = nullptr;
     ThStatus* st = nullptr;
@@ -864,13 +914,63 @@ struct cp_thermal {
 
 namespace {
 
-cp_status th_alloc(cp_thermal* t, double** p, size_t n) {
+template <typename T>
+cp_status th_alloc(cp_thermal* t, T** p, size_t n) {
     void* q = nullptr;
-    TCK(cudaMalloc(&q, std::max<size_t>(n, 1) * sizeof(double)));
+    TCK(cudaMalloc(&q, std::max<size_t>(n, 1) * sizeof(T)));
     t->allocs.push_back(q);
-    TCK(cudaMemsetAsync(q, 0, std::max<size_t>(n, 1) * sizeof(double), t->stream));
-    *p = static_cast<double*>(q);
+    TCK(cudaMemsetAsync(q, 0, std::max<size_t>(n, 1) * sizeof(T), t->stream));
+    *p = static_cast<T*>(q);
     return CP_OK;
+}
+
+// float copy of a level array (mixed precision)
+cp_status th_narrow(cp_thermal* t, const double* src, float* dst, long long n) {
+    const int g = (int)std::min<long long>(t->gElem, (n + kThThreads - 1) / kThThreads);
+    k_th_narrow<<<std::max(g, 1), kThThreads, 0, t->stream>>>(src, dst, n);
+    TCK(cudaGetLastError());
+    return CP_OK;
+}
+
+// The float levels of the mixed-precision V-cycle, shaped like the FP64
+// hierarchy.  Level 0 needs no b (its right-hand side is a Krylov vector)
+// and no y (its output is ph or sh).
+cp_status th_build_float_hierarchy(cp_thermal* t) {
+    const int L = (int)t->lv.size();
+    t->lvf.assign(L, ThLevelT<float>{});
+    for (int l = 0; l < L; ++l) {
+        const ThLevel& F = t->lv[l];
+        ThLevelT<float>& G = t->lvf[l];
+        G.nx = F.nx;
+        G.ny = F.ny;
+        G.ncol = F.ncol;
+        G.n = F.n;
+        std::vector<float**> arr = {&G.S.aP, &G.S.aW, &G.S.aE, &G.S.aS, &G.S.aN, &G.S.aB, &G.S.aT,
+                                    &G.lc,   &G.linv, &G.x};
+        if (l > 0) {
+            arr.push_back(&G.b);
+            arr.push_back(&G.y);
+        }
+        for (float** q : arr) {
+            cp_status s = th_alloc(t, q, (size_t)G.n);
+            if (s != CP_OK) return s;
+        }
+    }
+    void* q = nullptr;
+    TCK(cudaMalloc(&q, sizeof(ThLevelT<float>) * L));
+    t->allocs.push_back(q);
+    t->dlvf = static_cast<ThLevelT<float>*>(q);
+    TCK(cudaMemcpyAsync(t->dlvf, t->lvf.data(), sizeof(ThLevelT<float>) * L, cudaMemcpyHostToDevice, t->stream));
+    t->Hf.L = t->H.L;
+    t->Hf.cta = t->H.cta;
+    t->Hf.omega = t->H.omega;
+    t->Hf.scale0 = t->H.scale0;
+    t->Hf.scale = t->H.scale;
+    t->Hf.lv = t->dlvf;
+    t->Hf.prof = t->H.prof;
+    cp_status s = th_alloc(t, &t->phf, (size_t)t->k.n);
+    if (s != CP_OK) return s;
+    return th_alloc(t, &t->shf, (size_t)t->k.n);
 }
 
 // Levels of 2 x 2 column aggregates down to a single column, all z-layers
@@ -972,16 +1072,24 @@ cp_status th_objective(cp_thermal* t, double p, double* Tb_max, double* Tb_pnorm
 
 // Column factorisation and the persistent BiCGStab for op x = rhs, op = A or
 // A^T, from V.x; records ev1 after the solve and reads the status back.
+// Mixed precision: the factors are narrowed to the float levels, and the
+// solve is restarted from its iterate while the FP64 residual it computes
+// on entry (b - op x, not the recursive one) is above rtol, for at most
+// kThRefineRounds launches in all; the iterations add up.
 template <bool Tr>
 cp_status th_krylov(cp_thermal* t, const double* rhs, const ThVecs& V, ThStatus* hs) {
     const ThK& k = t->k;
-    for (const ThLevel& F : t->lv) {
+    for (size_t l = 0; l < t->lv.size(); ++l) {
+        const ThLevel& F = t->lv[l];
         const int g = (int)std::min<long long>(t->gElem, (F.ncol + kThThreads - 1) / kThThreads);
         k_th_lu<Tr><<<g, kThThreads, 0, t->stream>>>(k.Nz, F);
         TCK(cudaGetLastError());
+        if (t->mixed) {
+            cp_status s = th_narrow(t, F.lc, t->lvf[l].lc, F.n);
+            if (s == CP_OK) s = th_narrow(t, F.linv, t->lvf[l].linv, F.n);
+            if (s != CP_OK) return s;
+        }
     }
-    TCK(cudaMemsetAsync(t->bar, 0, sizeof(unsigned), t->stream));
-    TCK(cudaMemsetAsync(t->st, 0, sizeof(ThStatus), t->stream));
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(t->grid);
     cfg.blockDim = dim3(kThThreads);
@@ -992,16 +1100,32 @@ cp_status th_krylov(cp_thermal* t, const double* rhs, const ThVecs& V, ThStatus*
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     cfg.dynamicSmemBytes = kThSmemBytes;
-    if (t->H.prof) TCK(cudaMemsetAsync(t->H.prof, 0, sizeof(unsigned long long) * TH_P_COUNT, t->stream));
-    TCK(cudaLaunchKernelEx(&cfg, k_th_bicgstab<Tr>, k, t->H, rhs, V, t->part, t->bar, t->st, t->prm.maxiter,
-                           t->prm.rtol));
-    TCK(cudaEventRecord(t->ev1, t->stream));
-    TCK(cudaMemcpyAsync(hs, t->st, sizeof *hs, cudaMemcpyDeviceToHost, t->stream));
-    TCK(cudaStreamSynchronize(t->stream));
-    if (hs->err)
-        return tfail((cp_status)hs->err, "device reported %s in the thermal %s solve",
-                     cp_status_string((cp_status)hs->err), Tr ? "adjoint" : "forward");
-    if (t->H.prof) th_print_profile(t, Tr, hs->iterations);
+    const ThVecsT<float> Vf{V.x, V.r, V.rh, V.p, V.v, V.s, V.t, t->phf, t->shf};
+    const int rounds = t->mixed ? kThRefineRounds : 1;
+    int total = 0;
+    for (int round = 0; round < rounds; ++round) {
+        TCK(cudaMemsetAsync(t->bar, 0, sizeof(unsigned), t->stream));
+        TCK(cudaMemsetAsync(t->st, 0, sizeof(ThStatus), t->stream));
+        if (t->H.prof) TCK(cudaMemsetAsync(t->H.prof, 0, sizeof(unsigned long long) * TH_P_COUNT, t->stream));
+        const int left = std::max(t->prm.maxiter - total, 0);
+        if (t->mixed)
+            TCK(cudaLaunchKernelEx(&cfg, k_th_bicgstab<Tr, float>, k, t->lv[0], t->Hf, rhs, Vf, t->part, t->bar,
+                                   t->st, left, t->prm.rtol));
+        else
+            TCK(cudaLaunchKernelEx(&cfg, k_th_bicgstab<Tr, double>, k, t->lv[0], t->H, rhs, V, t->part, t->bar,
+                                   t->st, left, t->prm.rtol));
+        TCK(cudaEventRecord(t->ev1, t->stream));
+        TCK(cudaMemcpyAsync(hs, t->st, sizeof *hs, cudaMemcpyDeviceToHost, t->stream));
+        TCK(cudaStreamSynchronize(t->stream));
+        if (hs->err)
+            return tfail((cp_status)hs->err, "device reported %s in the thermal %s solve",
+                         cp_status_string((cp_status)hs->err), Tr ? "adjoint" : "forward");
+        if (t->H.prof) th_print_profile(t, Tr, hs->iterations);
+        total += hs->iterations;
+        // stop once a launch found the true residual at rtol on entry, or did not converge
+        if (!hs->converged || hs->iterations == 0) break;
+    }
+    hs->iterations = total;
     return CP_OK;
 }
 
@@ -1035,6 +1159,7 @@ void cp_thermal_params_default(cp_thermal_params* p) {
     p->maxiter = 1000;
     p->k_interp_mode = 1;
     p->qk = 1.0;
+    p->precision = CP_PREC_FP64;
 }
 
 cp_status cp_thermal_create(const cp_thermal_params* p, cp_thermal** out) {
@@ -1047,8 +1172,9 @@ cp_status cp_thermal_create(const cp_thermal_params* p, cp_thermal** out) {
     for (double x : pos)
         if (!(x > 0.0) || !std::isfinite(x)) return tfail(CP_ERR_BAD_PARAM, "dx, dy, H_b, H_t, k, rho, Cp must be > 0");
     if (!std::isfinite(p->T_inlet) || !(p->rtol >= 0.0) || p->maxiter < 0 || p->k_interp_mode < 0 ||
-        p->k_interp_mode > 2 || !std::isfinite(p->qk))
-        return tfail(CP_ERR_BAD_PARAM, "T_inlet, rtol, maxiter, k_interp_mode or qk out of range");
+        p->k_interp_mode > 2 || !std::isfinite(p->qk) ||
+        (p->precision != CP_PREC_FP64 && p->precision != CP_PREC_MIXED))
+        return tfail(CP_ERR_BAD_PARAM, "T_inlet, rtol, maxiter, k_interp_mode, qk or precision out of range");
     cp_thermal* t = new cp_thermal();
     t->prm = *p;
     auto bail = [&](cp_status s) {
@@ -1088,18 +1214,22 @@ cp_status cp_thermal_create(const cp_thermal_params* p, cp_thermal** out) {
     for (double** q : vols)
         if ((s = th_alloc(t, q, n)) != CP_OK) return bail(s);
     // the forward and the adjoint kernel run on the same grid: every block resident
-    int nb = 0, nbT = 0;
-    if (cudaFuncSetAttribute(k_th_bicgstab<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kThSmemBytes) !=
-            cudaSuccess ||
-        cudaFuncSetAttribute(k_th_bicgstab<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kThSmemBytes) !=
-            cudaSuccess)
-        return bail(tfail(CP_ERR_CUDA, "the thermal solver kernel's shared memory (%zu bytes)", kThSmemBytes));
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_th_bicgstab<false>, kThThreads, kThSmemBytes);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nbT, k_th_bicgstab<true>, kThThreads, kThSmemBytes);
-    nb = std::min(nb, nbT);
+    // (the forward and adjoint kernels of the solve's precision)
+    t->mixed = p->precision == CP_PREC_MIXED;
+    const void* kern[2] = {t->mixed ? (const void*)k_th_bicgstab<false, float> : (const void*)k_th_bicgstab<false, double>,
+                           t->mixed ? (const void*)k_th_bicgstab<true, float> : (const void*)k_th_bicgstab<true, double>};
+    int nb = 1 << 30;
+    for (const void* f : kern) {
+        int b = 0;
+        if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kThSmemBytes) != cudaSuccess)
+            return bail(tfail(CP_ERR_CUDA, "the thermal solver kernel's shared memory (%zu bytes)", kThSmemBytes));
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, f, kThThreads, kThSmemBytes);
+        nb = std::min(nb, b);
+    }
     if (nb < 1) return bail(tfail(CP_ERR_CUDA, "the thermal solver kernel does not fit on an SM"));
     t->grid = t->numSMs * std::min(nb, 4);
     if ((s = th_build_hierarchy(t)) != CP_OK) return bail(s);
+    if (t->mixed && (s = th_build_float_hierarchy(t)) != CP_OK) return bail(s);
     t->gElem = t->numSMs * 4;
     if ((s = th_alloc(t, &t->part, (size_t)6 * kMaxBlocks)) != CP_OK) return bail(s);
     void* q = nullptr;
@@ -1160,6 +1290,18 @@ cp_status cp_thermal_solve(cp_thermal* t, cp_thermal_report* rep) {
         k_th_coarsen<<<g, kThThreads, 0, t->stream>>>(k.Nz, t->lv[l], C);
         TCK(cudaGetLastError());
     }
+    // mixed precision: the V-cycle's float copies of every level's operator
+    if (t->mixed)
+        for (size_t l = 0; l < t->lv.size(); ++l) {
+            const ThSys& A = t->lv[l].S;
+            const ThSysT<float>& B = t->lvf[l].S;
+            const double* src[7] = {A.aP, A.aW, A.aE, A.aS, A.aN, A.aB, A.aT};
+            float* dst[7] = {B.aP, B.aW, B.aE, B.aS, B.aN, B.aB, B.aT};
+            for (int a = 0; a < 7; ++a) {
+                cp_status s = th_narrow(t, src[a], dst[a], t->lv[l].n);
+                if (s != CP_OK) return s;
+            }
+        }
     ThStatus hs;
     cp_status s = th_krylov<false>(t, t->S.b, t->V, &hs);
     if (s != CP_OK) return s;

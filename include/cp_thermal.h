@@ -26,6 +26,10 @@ typedef struct cp_thermal_params {
     int maxiter;
     int k_interp_mode;     /* 0 linear, 1 RAMP, 2 harmonic (thermal_solver.cpp:267-295) */
     double qk;             /* RAMP parameter                                        */
+    int precision;         /* cp_precision: CP_PREC_FP64 (default) or CP_PREC_MIXED,
+                              a float V-cycle inside the FP64 BiCGStab; the solve is
+                              restarted from its iterate while the FP64 residual
+                              b - A T is above rtol (at most 4 launches)           */
 } cp_thermal_params;
 
 typedef struct cp_thermal cp_thermal;
@@ -47,7 +51,9 @@ cp_status cp_thermal_destroy(cp_thermal* th);
 cp_status cp_thermal_set_inputs(cp_thermal* th, const double* gamma, const double* u_xy, const double* v_xy,
                                 const double* q0);
 /* Assembles the system (thermal_solver.cpp:417-520) and solves it from
- * T = T_inlet with BiCGStab preconditioned by exact solves of each z-column. */
+ * T = T_inlet with BiCGStab right-preconditioned by one V-cycle of 2 x 2
+ * column aggregates with z-line smoothing (the reference: AMGCL IDR(8) with
+ * smoothed-aggregation AMG, thermal_solver.cpp:534-553). */
 cp_status cp_thermal_solve(cp_thermal* th, cp_thermal_report* rep);
 /* T: Nz * Ny * Nx doubles (host) */
 cp_status cp_thermal_get_T(cp_thermal* th, double* T);
