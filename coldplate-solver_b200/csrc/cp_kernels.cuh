@@ -228,7 +228,7 @@ __device__ __forceinline__ void assemble_one(const KParams& k, const Fields& f, 
 }
 
 template <typename TC, bool Mixed>
-__global__ void k_assemble(KParams k, const Status* st, Fields f, MomSys<TC> U, MomSys<TC> V, double* dE,
+__global__ void __launch_bounds__(256, 4) k_assemble(KParams k, const Status* st, Fields f, MomSys<TC> U, MomSys<TC> V, double* dE,
                            double* dN, int doU, int doV) {
     if (st->done) return;
     const double maxVel = max_vel(inlet_velocity(k, st->iter));
