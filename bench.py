@@ -58,9 +58,12 @@ ADJ_FD_NOTE = ("not checked at this state; vs central FD (h 1e-4) at converged s
 # ncu captures of the dominant kernels (profiles/): DRAM bytes read + written
 PCG_MG_CAPTURE_BYTES = (762.0 + 1447.7) * 1e6     # k_pcg_mg<float>, one launch (32 x 64 tiles)
 PCG_MG_CAPTURE_ITERS = 30
-PCG_SA_CAPTURE_BYTES = (1780.3 + 1050.5) * 1e6    # k_pcg_sa<float>, one launch of 16 CG iterations
-PCG_SA_CAPTURE_ITERS = 16
-THERMAL_CAPTURE_BYTES_PER_CELL_ITER = 693.0        # k_th_bicgstab, 512 x 256 x 12 capture (78 iterations)
+# k_pcg_sa<float>: four consecutive launches (outer iterations 20-23 of the
+# mixed solve, one of them rebuilding the coarse operators), 58 CG iterations
+PCG_SA_CAPTURE_BYTES = (6459.0 + 3920.0) * 1e6
+PCG_SA_CAPTURE_ITERS = 58
+THERMAL_CAPTURE_BYTES_PER_CELL_ITER = 693.0        # k_th_bicgstab<false, double>, 512 x 256 x 12 (78 iterations)
+THERMAL_MIXED_CAPTURE_BYTES_PER_CELL_ITER = 406.0  # k_th_bicgstab<false, float>, the same case (85 iterations)
 
 
 def parse():
@@ -611,6 +614,7 @@ def thermal_leg(Simple, torch, args) -> dict:
              "e2e_s": float(np.mean(e2e_m)),
              "roofline": {"bound": "hbm", "achieved": achieved_m, "peak": peak, "unit": "GB/s",
                           "frac": achieved_m / peak, "kernel": "k_th_bicgstab<false, float>",
+                          "traffic": THERMAL_MIXED_CAPTURE_BYTES_PER_CELL_ITER * n * its_fm,
                           "algorithmic_bytes": bytes_iter_m * its_fm}}
     return {"workload": f"density flow {Nx}x{Ny} seed {args.seed} ({THERMAL_FLOW_ITERS} mixed SIMPLE iterations) "
                         f"-> {Nx}x{Ny}x12 CHT (8 plate + 4 channel layers), hotspot power map, rtol 1e-6, "
@@ -747,7 +751,8 @@ def main():
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": traffic, "algorithmic_bytes": pcg_bytes, "kernel": kname,
                 "bytes_per_unknown_per_cg_iteration": words * w_mix,
-                "traffic_source": (f"ncu capture (2048x1024, {cap_iters} CG iterations) scaled by CG iterations"
+                "traffic_source": (f"ncu capture (2048x1024, {cap_iters} CG iterations in consecutive launches, "
+                                   f"coarse-operator rebuilds included) scaled by CG iterations"
                                    if cap_bytes else "no capture of this kernel yet"),
                 "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"}
 
