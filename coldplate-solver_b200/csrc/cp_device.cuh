@@ -159,8 +159,12 @@ __device__ __forceinline__ bool grid_barrier(unsigned* counter, unsigned target,
     __syncthreads();
     if (threadIdx.x == 0) {
         int ok = 1;
-        __threadfence();
-        atomicAdd(counter, 1u);
+        // release pattern: the acq_rel fence orders the block's writes (made
+        // before the __syncthreads above) ahead of the relaxed arrival; the
+        // acquire loads below order the reads after it, and the closing
+        // __syncthreads extends both to the whole block
+        asm volatile("fence.acq_rel.gpu;" ::: "memory");
+        asm volatile("red.relaxed.gpu.global.add.u32 [%0], 1;" ::"l"(counter) : "memory");
         unsigned long long t0 = 0;
         unsigned spins = 0;
         while (ld_acquire_u32(counter) < target) {
@@ -175,7 +179,6 @@ __device__ __forceinline__ bool grid_barrier(unsigned* counter, unsigned target,
             }
             if (*(volatile int*)err != 0) { ok = 0; break; }
         }
-        __threadfence();
         s_ok = ok;
     }
     __syncthreads();
