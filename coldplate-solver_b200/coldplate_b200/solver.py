@@ -104,9 +104,16 @@ class Simple:
                 "vStar": (M, N + 1), "pStar": (M + 1, N + 1), "dE": (M + 1, N), "dN": (M, N + 1),
                 "gamma": (M, N), "alpha": (M, N), "cellType": (M, N)}[name]
 
-    def get(self, name: str) -> np.ndarray:
+    def get(self, name: str, out: np.ndarray | None = None) -> np.ndarray:
+        """The field as a float64 array of shape(name).  With `out` (a
+        C-contiguous float64 array of that shape, e.g. a view of pinned host
+        memory, which the copy then reaches by DMA) the field is written
+        there and `out` is returned."""
         r, c = self.shape(name)
-        out = np.empty((r, c), dtype=np.float64)
+        if out is None:
+            out = np.empty((r, c), dtype=np.float64)
+        elif out.dtype != np.float64 or out.shape != (r, c) or not out.flags.c_contiguous:
+            raise ValueError(f"{name}: out must be a C-contiguous float64 array of shape {(r, c)}")
         nat.check(self._lib.cp_get_field(self._h, nat.FIELDS[name], _dptr(out), r, c, c, 1))
         return out
 

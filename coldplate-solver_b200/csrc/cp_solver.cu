@@ -76,6 +76,7 @@ struct cp_ctx {
     double *u = nullptr, *v = nullptr, *p = nullptr, *uStar = nullptr, *vStar = nullptr, *pStar = nullptr;
     double *dE = nullptr, *dN = nullptr, *gamma = nullptr, *alpha = nullptr;
     std::vector<double> cellTypeHost;  // M x N padded, as the reference keeps it
+    double* gammaStage = nullptr;      // pinned M x N staging of gamma (first set_cell_type / set_gamma)
     // inner systems (double or float)
     void* mom[12] = {};
     void* xb[4] = {};
@@ -234,9 +235,8 @@ void fill_kparams(cp_ctx* c) {
 
 // density -> gamma (1 - clamp(cellType)) with the padded row/column copied,
 // alpha by RAMP (SIMPLE.cpp:667-676, 707-729, 766-772); all M x N, double.
-void build_density(const cp_ctx* c, const std::vector<double>& cellTypePadded, std::vector<double>& gamma) {
+void build_density(const cp_ctx* c, const std::vector<double>& cellTypePadded, double* gamma) {
     const int M = c->d.M, N = c->d.N, pr = M - 1, pc = N - 1;
-    gamma.assign((size_t)M * N, 1.0);
     for (int i = 0; i < pr; ++i)
         for (int j = 0; j < pc; ++j) {
             const double val = cellTypePadded[(size_t)i * N + j];
@@ -267,9 +267,10 @@ cp_status mark_sa_stale(cp_ctx* c) {
     return CP_OK;
 }
 
-cp_status upload_cells(cp_ctx* c, const std::vector<double>& g) {
+// gamma (M x N, host) to the device, alpha from it; returns after the copy
+cp_status upload_cells(cp_ctx* c, const double* g) {
     const int M = c->d.M, N = c->d.N;
-    CK(cudaMemcpy2DAsync(c->gamma, (size_t)c->d.P * 8, g.data(), (size_t)N * 8, (size_t)N * 8, M,
+    CK(cudaMemcpy2DAsync(c->gamma, (size_t)c->d.P * 8, g, (size_t)N * 8, (size_t)N * 8, M,
                          cudaMemcpyHostToDevice, c->stream));
     const double amax = c->prm.eta / std::max(c->prm.brinkmanKMin, 1e-20);
     k_alpha<<<c->gElem, kThreads, 0, c->stream>>>(c->gamma, c->alpha, M, N, c->d.P, amax, c->prm.brinkmanQ);
@@ -955,9 +956,9 @@ cp_status cp_create(const cp_params* prm, cp_ctx** out) {
     memset(c->stHost, 0, sizeof(Status));
     // all fluid until a geometry is set (SIMPLE.cpp:267-269)
     c->cellTypeHost.assign((size_t)M * N, 0.0);
-    std::vector<double> g;
-    build_density(c, c->cellTypeHost, g);
-    if ((s = upload_cells(c, g)) != CP_OK) return bail(s);
+    std::vector<double> g((size_t)M * N);
+    build_density(c, c->cellTypeHost, g.data());
+    if ((s = upload_cells(c, g.data())) != CP_OK) return bail(s);
     if (cudaStreamSynchronize(c->stream) != cudaSuccess) return bail(fail(CP_ERR_CUDA, "initialisation failed"));
     *out = c;
     return CP_OK;
@@ -981,6 +982,7 @@ cp_status cp_destroy(cp_ctx* c) {
     if (c->graph) cudaGraphExecDestroy(c->graph);
     for (void* q : c->allocs) cudaFree(q);
     if (c->stHost) cudaFreeHost(c->stHost);
+    if (c->gammaStage) cudaFreeHost(c->gammaStage);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -997,22 +999,27 @@ static cp_status set_cells(cp_ctx* c, const double* src, long rows, long cols, l
     if (!src) return fail(CP_ERR_BAD_PARAM, "host pointer is NULL");
     const int M = c->d.M, N = c->d.N, pr = M - 1, pc = N - 1;
     if (rows != pr || cols != pc) return fail(CP_ERR_BAD_PARAM, "shape %ld x %ld, expected %d x %d", rows, cols, pr, pc);
-    std::vector<double> P((size_t)M * N, 0.0);
+    // checked first, so that a rejected input leaves the geometry as it was
+    for (long i = 0; i < rows; ++i)
+        for (long j = 0; j < cols; ++j)
+            if (!std::isfinite(src[i * rs + j * cs])) return fail(CP_ERR_NONFINITE, "non-finite input at (%ld, %ld)", i, j);
+    // gamma goes up from a pinned staging array the context keeps (DMA; no
+    // fresh host pages per call)
+    if (!c->gammaStage && cudaMallocHost(&c->gammaStage, (size_t)M * N * sizeof(double)) != cudaSuccess) {
+        c->gammaStage = nullptr;
+        cudaGetLastError();
+        return fail(CP_ERR_CUDA, "cudaMallocHost of the gamma staging array failed");
+    }
+    std::vector<double>& P = c->cellTypeHost;   // M x N padded; every entry is rewritten
     for (long i = 0; i < rows; ++i) {
         const double* row = src + i * rs;
         double* out = P.data() + (size_t)i * N;
-        for (long j = 0; j < cols; ++j) {
-            const double x = row[j * cs];
-            if (!std::isfinite(x)) return fail(CP_ERR_NONFINITE, "non-finite input at (%ld, %ld)", i, j);
-            out[j] = fromGamma ? 1.0 - x : x;
-        }
+        for (long j = 0; j < cols; ++j) out[j] = fromGamma ? 1.0 - row[j * cs] : row[j * cs];
     }
     for (int i = 0; i < pr; ++i) P[(size_t)i * N + pc] = P[(size_t)i * N + pc - 1];
     for (int j = 0; j < N; ++j) P[(size_t)pr * N + j] = P[(size_t)(pr - 1) * N + std::min(j, pc - 1)];
-    c->cellTypeHost.swap(P);
-    std::vector<double> g;
-    build_density(c, c->cellTypeHost, g);
-    return upload_cells(c, g);
+    build_density(c, P, c->gammaStage);
+    return upload_cells(c, c->gammaStage);
 }
 
 cp_status cp_set_cell_type(cp_ctx* c, const double* ct, long rows, long cols, long rs, long cs) {
