@@ -112,7 +112,8 @@ class Simple:
         r, c = self.shape(name)
         if out is None:
             out = np.empty((r, c), dtype=np.float64)
-        elif out.dtype != np.float64 or out.shape != (r, c) or not out.flags.c_contiguous:
+        elif (out.dtype != np.float64 or out.shape != (r, c) or not out.flags.c_contiguous
+              or not out.flags.writeable):
             raise ValueError(f"{name}: out must be a C-contiguous float64 array of shape {(r, c)}")
         nat.check(self._lib.cp_get_field(self._h, nat.FIELDS[name], _dptr(out), r, c, c, 1))
         return out

@@ -176,7 +176,10 @@ cp_status cp_destroy(cp_ctx* ctx);
 
 /* Geometry.  cellType: Ny x Nx, 0 fluid .. 1 solid (geometry_fluid.txt,
  * SIMPLE.cpp:633-690, converted as SIMPLE.cpp:695-777).  gamma: Ny x Nx
- * density, 1 fluid .. 0 solid (set directly, e.g. by an optimiser). */
+ * density, 1 fluid .. 0 solid (set directly, e.g. by an optimiser).  A
+ * non-finite entry returns CP_ERR_NONFINITE and leaves the geometry as it
+ * was.  The first call allocates a pinned (M x N doubles) staging array that
+ * the context keeps for later calls and frees in cp_destroy. */
 cp_status cp_set_cell_type(cp_ctx* ctx, const double* cellType, long rows, long cols,
                            long row_stride, long col_stride);
 cp_status cp_set_gamma(cp_ctx* ctx, const double* gamma, long rows, long cols,
