@@ -10,7 +10,7 @@ def test_defaults_are_the_reference_defaults(built_lib):
     from coldplate_b200.thermal import default_thermal_params
     p = default_thermal_params()
     expect = dict(nz_solid=2, nz_fluid=7, H_b=5e-4, H_t=4e-3, k_s=400.0, k_f=0.6, rho=998.0, Cp=4180.0,
-                  T_inlet=30.0, rtol=1e-6, maxiter=1000, k_interp_mode=1, qk=1.0)
+                  T_inlet=30.0, rtol=1e-6, maxiter=1000, k_interp_mode=1, qk=1.0, precision=0)
     for k, v in expect.items():
         assert getattr(p, k) == pytest.approx(v), k
 
@@ -18,7 +18,8 @@ def test_defaults_are_the_reference_defaults(built_lib):
 @pytest.mark.parametrize("over", [dict(Nx=1), dict(Ny=0), dict(nz_solid=0), dict(nz_fluid=70),
                                   dict(nz_solid=8, nz_fluid=9), dict(dx=0.0),
                                   dict(k_f=-1.0), dict(k_interp_mode=3), dict(maxiter=-1),
-                                  dict(rtol=float("nan")), dict(T_inlet=float("inf"))])
+                                  dict(rtol=float("nan")), dict(T_inlet=float("inf")), dict(precision=2),
+                                  dict(precision=-1)])
 def test_bad_parameters_are_rejected_before_any_device_work(built_lib, over):
     from coldplate_b200 import CpError, Thermal
     kw = dict(Nx=8, Ny=6, dx=1e-5, dy=1e-5)
