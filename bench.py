@@ -705,9 +705,13 @@ def main():
                                                  adjoint=not args.no_adjoint)
         t_64, dp_64_k, _ = timed_solves("fp64", k64, 1, 1)
     clocks = clk.summary()
-    t_mixed = max(t_mix)
+    # every figure of the line is the slowest rank's (the same all-reduces on
+    # every rank, in this order)
+    t_mixed = max_over_ranks(max(t_mix), dist, "cuda")
+    t_64 = [max_over_ranks(max(t_64), dist, "cuda")]
     t_adj = max(r["device_ms"] for r in adj_reps) / 1e3 if adj_reps else None
-    t_mixed = max_over_ranks(t_mixed, dist, "cuda")
+    if adj_reps:
+        t_adj = max_over_ranks(t_adj, dist, "cuda")
 
     # ---- per-kernel device times and the roofline of the dominant kernel
     prm = case.params(precision="mixed", maxIterations=100000, epsilon=1e-30, historyCapacity=100000)
@@ -791,6 +795,7 @@ def main():
                 e2e_t.append(t1 - t0)
     h2d = gamma_host.nbytes
     d2h = p.nbytes + u.nbytes + v.nbytes + 8
+    e2e_mean = max_over_ranks(float(np.mean(e2e_t)), dist, "cuda")
 
     # ---- errors against the FP64 oracle (rank 0; CPU work outside every timed region)
     parity = None
@@ -824,7 +829,7 @@ def main():
             "vs_oracle": parity,
             "roofline": roofline,
             "cpu_baseline": cb,
-            "e2e": {"value": float(np.mean(e2e_t)), "unit": "s", "h2d_bytes_per_step": int(h2d),
+            "e2e": {"value": e2e_mean, "unit": "s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
             "clocks": clocks,
             "dp_star_pa": dp_star,
