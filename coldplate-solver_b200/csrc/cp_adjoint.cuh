@@ -740,17 +740,9 @@ __global__ void k_adj_update(KParams k, const double* zu, const double* zv, cons
 constexpr int kKryMaxDots = 32;
 
 // part[b * 32 + q] = block b's share of <w, B_q>, q < nv, B_q = B + q L
-__global__ void __launch_bounds__(256) k_kry_mdot(const double* __restrict__ w, const double* __restrict__ B,
-                                                  size_t L, int nv, double* part) {
-    double acc[kKryMaxDots];
-#pragma unroll
-    for (int q = 0; q < kKryMaxDots; ++q) acc[q] = 0.0;
-    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < L; t += (size_t)gridDim.x * blockDim.x) {
-        const double wt = w[t];
-#pragma unroll
-        for (int q = 0; q < kKryMaxDots; ++q)
-            if (q < nv) acc[q] += B[q * L + t] * wt;
-    }
+// a block's partial sums of the nv per-thread accumulators (warp shuffles,
+// then warps in order) into part[block * 32 + q]
+__device__ __forceinline__ void kry_block_partials(const double (&acc)[kKryMaxDots], int nv, double* part) {
     __shared__ double sm[8][kKryMaxDots];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
@@ -767,6 +759,48 @@ __global__ void __launch_bounds__(256) k_kry_mdot(const double* __restrict__ w, 
         for (int q = 0; q < (int)(blockDim.x >> 5); ++q) v += sm[q][threadIdx.x];
         part[(size_t)blockIdx.x * kKryMaxDots + threadIdx.x] = v;
     }
+}
+
+__global__ void __launch_bounds__(256) k_kry_mdot(const double* __restrict__ w, const double* __restrict__ B,
+                                                  size_t L, int nv, double* part) {
+    double acc[kKryMaxDots];
+#pragma unroll
+    for (int q = 0; q < kKryMaxDots; ++q) acc[q] = 0.0;
+    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < L; t += (size_t)gridDim.x * blockDim.x) {
+        const double wt = w[t];
+#pragma unroll
+        for (int q = 0; q < kKryMaxDots; ++q)
+            if (q < nv) acc[q] += B[q * L + t] * wt;
+    }
+    kry_block_partials(acc, nv, part);
+}
+
+// w += sign * sum_q h[q] B_q (k_kry_axpy), then the partials of the updated
+// w against B_0 .. B_nd-1, or (selfDot) of its squared norm (k_kry_mdot on
+// the new w): one pass over B and w instead of two, with the per-thread
+// element order and the block reduction of the two kernels it replaces.
+__global__ void __launch_bounds__(256) k_kry_axpy_mdot(double* __restrict__ w, const double* __restrict__ B,
+                                                       size_t L, int nv, const double* __restrict__ h, double sign,
+                                                       int nd, int selfDot, double* part) {
+    __shared__ double hs[kKryMaxDots];
+    if (threadIdx.x < nv) hs[threadIdx.x] = sign * h[threadIdx.x];
+    __syncthreads();
+    double acc[kKryMaxDots];
+#pragma unroll
+    for (int q = 0; q < kKryMaxDots; ++q) acc[q] = 0.0;
+    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < L; t += (size_t)gridDim.x * blockDim.x) {
+        double a = w[t];
+        for (int q = 0; q < nv; ++q) a += hs[q] * B[q * L + t];
+        w[t] = a;
+        if (selfDot) {
+            acc[0] += a * a;
+        } else {
+#pragma unroll
+            for (int q = 0; q < kKryMaxDots; ++q)
+                if (q < nd) acc[q] += B[q * L + t] * a;
+        }
+    }
+    kry_block_partials(acc, selfDot ? 1 : nd, part);
 }
 
 // out[q] = sum over blocks of part[b * 32 + q]; one block of 32 warps, warp q

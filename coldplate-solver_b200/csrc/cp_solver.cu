@@ -1575,13 +1575,16 @@ static cp_status adjoint_impl(cp_ctx* c, double* grad, long rows, long cols, lon
             double* h1 = c->adjH;
             double* h2 = c->adjH + kKryMaxDots;
             double* nr = c->adjH + 2 * kKryMaxDots;
+            // (each projection fused with the dot products that follow it)
             if ((s = mdot(W, Vq(0), j + 1, h1)) != CP_OK) return s;
-            k_kry_axpy<<<nb, 256, 0, c->stream>>>(W, Vq(0), L, j + 1, h1, -1.0);
+            k_kry_axpy_mdot<<<nb, 256, 0, c->stream>>>(W, Vq(0), L, j + 1, h1, -1.0, j + 1, 0, c->adjKryPart);
             CK(cudaGetLastError());
-            if ((s = mdot(W, Vq(0), j + 1, h2)) != CP_OK) return s;
-            k_kry_axpy<<<nb, 256, 0, c->stream>>>(W, Vq(0), L, j + 1, h2, -1.0);
+            k_kry_sum<<<1, 1024, 0, c->stream>>>(c->adjKryPart, nb, j + 1, h2);
             CK(cudaGetLastError());
-            if ((s = mdot(W, W, 1, nr)) != CP_OK) return s;
+            k_kry_axpy_mdot<<<nb, 256, 0, c->stream>>>(W, Vq(0), L, j + 1, h2, -1.0, 1, 1, c->adjKryPart);
+            CK(cudaGetLastError());
+            k_kry_sum<<<1, 1024, 0, c->stream>>>(c->adjKryPart, nb, 1, nr);
+            CK(cudaGetLastError());
             CK(cudaMemcpyAsync(hh.data(), c->adjH, hh.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
             CK(cudaStreamSynchronize(c->stream));
             for (int i = 0; i <= j; ++i) Hij(i, j) = hh[i] + hh[kKryMaxDots + i];
